@@ -1,0 +1,225 @@
+"""ctypes binding of libddsolve_b200.so (the C ABI in include/ddsolve_b200.h).
+
+The shared library is built in-tree by dp3_b200/build.py. Loading fails loudly
+when it is missing: there is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libddsolve_b200.so")
+
+DDSOLVE_OK = 0
+ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "call out of order",
+          4: "unsupported", 5: "device wait timed out"}
+
+# Every symbol declared in include/ddsolve_b200.h.
+EXPORTED_SYMBOLS = (
+    "ddsolve_create", "ddsolve_destroy", "ddsolve_last_error",
+    "ddsolve_default_settings", "ddsolve_set_settings",
+    "ddsolve_set_channel_block", "ddsolve_set_channel_block_regular",
+    "ddsolve_solve", "ddsolve_perform_iteration", "ddsolve_stream",
+    "ddsolve_set_tuning", "ddsolve_time_stream_kernel",
+    "ddsolve_last_launch_count",
+)
+
+
+class Dims(ctypes.Structure):
+    _fields_ = [("n_antennas", ctypes.c_uint32),
+                ("n_directions", ctypes.c_uint32),
+                ("n_channel_blocks", ctypes.c_uint32),
+                ("n_correlations", ctypes.c_uint32),
+                ("n_solution_polarizations", ctypes.c_uint32),
+                ("n_solutions_per_direction", ctypes.POINTER(ctypes.c_uint32))]
+
+
+class Settings(ctypes.Structure):
+    _fields_ = [("max_iterations", ctypes.c_uint32),
+                ("min_iterations", ctypes.c_uint32),
+                ("accuracy", ctypes.c_double),
+                ("constraint_accuracy", ctypes.c_double),
+                ("step_size", ctypes.c_double),
+                ("detect_stalling", ctypes.c_int32),
+                ("step_diff_sigma", ctypes.c_double),
+                ("phase_only", ctypes.c_int32)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_uint32),
+                ("constraint_iterations", ctypes.c_uint32),
+                ("has_converged", ctypes.c_int32),
+                ("has_stalled", ctypes.c_int32)]
+
+
+_lib = None
+
+
+def lib():
+    """Loads the solver library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python dp3_b200/build.py`"
+                " (the solver has no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, u32, u64, i32 = (ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64,
+                             ctypes.c_int)
+        L.ddsolve_create.argtypes = [ctypes.POINTER(Dims), i32,
+                                     ctypes.POINTER(vp)]
+        L.ddsolve_destroy.argtypes = [vp]
+        L.ddsolve_last_error.argtypes = [vp]
+        L.ddsolve_last_error.restype = ctypes.c_char_p
+        L.ddsolve_default_settings.argtypes = [ctypes.POINTER(Settings)]
+        L.ddsolve_default_settings.restype = None
+        L.ddsolve_set_settings.argtypes = [vp, ctypes.POINTER(Settings)]
+        L.ddsolve_set_channel_block.argtypes = [vp, u32, u64, vp, vp, vp, vp]
+        L.ddsolve_set_channel_block_regular.argtypes = [vp, u32, u32, u32, u32,
+                                                        vp, vp, vp, vp]
+        L.ddsolve_solve.argtypes = [vp, vp, ctypes.POINTER(Result), vp]
+        L.ddsolve_perform_iteration.argtypes = [vp, vp, vp]
+        L.ddsolve_stream.argtypes = [vp]
+        L.ddsolve_stream.restype = vp
+        L.ddsolve_set_tuning.argtypes = [vp, u32, u32]
+        L.ddsolve_time_stream_kernel.argtypes = [vp, u32,
+                                                 ctypes.POINTER(ctypes.c_float)]
+        L.ddsolve_last_launch_count.argtypes = [vp]
+        L.ddsolve_last_launch_count.restype = u64
+        _lib = L
+    return _lib
+
+
+def default_settings():
+    s = Settings()
+    lib().ddsolve_default_settings(ctypes.byref(s))
+    return s
+
+
+def _addr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+class Context:
+    """Owns one ddsolve_ctx (one CUDA stream on one device)."""
+
+    def __init__(self, n_antennas, n_solutions_per_direction, n_channel_blocks,
+                 n_correlations, n_pol, device=0):
+        self._nspd = np.ascontiguousarray(n_solutions_per_direction,
+                                          dtype=np.uint32)
+        self.n_antennas = int(n_antennas)
+        self.n_directions = len(self._nspd)
+        self.n_channel_blocks = int(n_channel_blocks)
+        self.n_correlations = int(n_correlations)
+        self.n_pol = int(n_pol)
+        self.n_sub = int(self._nspd.sum())
+        dims = Dims(self.n_antennas, self.n_directions, self.n_channel_blocks,
+                    self.n_correlations, self.n_pol,
+                    self._nspd.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)))
+        h = ctypes.c_void_p()
+        rc = lib().ddsolve_create(ctypes.byref(dims), int(device),
+                                  ctypes.byref(h))
+        if rc != DDSOLVE_OK:
+            raise RuntimeError("ddsolve_create: "
+                               + lib().ddsolve_last_error(None).decode())
+        self._h = h
+        self._keep = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ddsolve_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != DDSOLVE_OK:
+            msg = lib().ddsolve_last_error(self._h).decode()
+            raise RuntimeError(f"{what}: {ERRORS.get(rc, rc)}: {msg}")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def stream_ptr(self):
+        return lib().ddsolve_stream(self._h)
+
+    def set_settings(self, settings):
+        self._check(lib().ddsolve_set_settings(self._h, ctypes.byref(settings)),
+                    "ddsolve_set_settings")
+
+    def set_tuning(self, direction_groups=0, max_slab_times=0):
+        self._check(lib().ddsolve_set_tuning(self._h, direction_groups,
+                                             max_slab_times), "ddsolve_set_tuning")
+
+    def set_channel_block(self, cb, data, model, antenna_pairs, solution_map):
+        data = np.ascontiguousarray(data, dtype=np.float32)
+        model = np.ascontiguousarray(model, dtype=np.float32)
+        ap = np.ascontiguousarray(antenna_pairs, dtype=np.uint32)
+        sm = np.ascontiguousarray(solution_map, dtype=np.uint32)
+        n_vis = data.shape[0] if data.ndim else 0
+        self._check(lib().ddsolve_set_channel_block(
+            self._h, cb, n_vis, _addr(data), _addr(model), _addr(ap), _addr(sm)),
+            "ddsolve_set_channel_block")
+
+    def set_channel_block_regular(self, cb, n_times, n_baselines, n_channels,
+                                  data, model, antenna1, antenna2):
+        # Arrays must stay valid until the copy is done: the call synchronises
+        # implicitly for pageable memory; pinned arrays are kept alive here.
+        a1 = np.ascontiguousarray(antenna1, dtype=np.uint32)
+        a2 = np.ascontiguousarray(antenna2, dtype=np.uint32)
+        data = _host_buffer(data)
+        model = _host_buffer(model)
+        self._keep[cb] = (data, model)
+        self._check(lib().ddsolve_set_channel_block_regular(
+            self._h, cb, n_times, n_baselines, n_channels, _ptr_any(data),
+            _ptr_any(model), _addr(a1), _addr(a2)),
+            "ddsolve_set_channel_block_regular")
+
+    def solve(self, solutions, step_magnitudes=None):
+        """solutions: complex128 [n_cb, n_ant, n_sub, n_pol], updated in place."""
+        assert solutions.dtype == np.complex128 and solutions.flags.c_contiguous
+        res = Result()
+        self._check(lib().ddsolve_solve(self._h, _addr(solutions),
+                                        ctypes.byref(res),
+                                        _addr(step_magnitudes)), "ddsolve_solve")
+        return res
+
+    def perform_iteration(self, solutions):
+        solutions = np.ascontiguousarray(solutions, dtype=np.complex128)
+        nxt = np.empty_like(solutions)
+        self._check(lib().ddsolve_perform_iteration(self._h, _addr(solutions),
+                                                    _addr(nxt)),
+                    "ddsolve_perform_iteration")
+        return nxt
+
+    def time_stream_kernel(self, n_launches=10):
+        ms = ctypes.c_float()
+        self._check(lib().ddsolve_time_stream_kernel(self._h, n_launches,
+                                                     ctypes.byref(ms)),
+                    "ddsolve_time_stream_kernel")
+        return ms.value
+
+    def last_launch_count(self):
+        return int(lib().ddsolve_last_launch_count(self._h))
+
+
+def _host_buffer(a):
+    """A contiguous float32 host buffer: numpy array or CPU torch tensor
+    (pinned tensors make the upload asynchronous)."""
+    if hasattr(a, "data_ptr"):
+        assert a.is_contiguous() and not a.is_cuda
+        return a
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _ptr_any(a):
+    """Address of a contiguous numpy array or CPU torch tensor."""
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr())
+    return ctypes.c_void_p(a.ctypes.data)

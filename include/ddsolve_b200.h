@@ -1,0 +1,188 @@
+/*
+ * ddsolve_b200 -- C ABI of the B200 direction-iterative gain solver.
+ *
+ * This is the drop-in boundary for DP3's DDECal direction-iterative solvers.
+ * A DP3-side adapter class derived from dp3::ddecal::SolverBase (see
+ * INTEGRATION.md) binds these entry points; every entry point below names the
+ * reference interface it replaces.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only. No exception crosses the ABI: every
+ *    function returns 0 on success or a nonzero DDSOLVE_E_* code, and
+ *    ddsolve_last_error() gives the message (thread-local for failures that
+ *    have no context yet).
+ *  - Visibility layout per channel block is the reference SolveData layout
+ *    (ddecal/gain_solvers/SolveData.h:28-194):
+ *      data          float32 [n_vis][n_correlations][re,im]
+ *      model         float32 [n_directions][n_vis][n_correlations][re,im]
+ *      antenna_pairs uint32  [n_vis][2]
+ *      solution_map  uint32  [n_directions][n_vis]  (absolute sub-solution)
+ *    n_correlations: 1 = complex<float> (UniSolveData), 2 = XX/YY
+ *    (aocommon::MC2x2FDiag, DuoSolveData), 4 = full 2x2 row-major
+ *    (aocommon::MC2x2F, FullSolveData).
+ *  - Solutions: float64 complex [n_channel_blocks][n_antennas][n_sub][n_pol]
+ *    ([re,im] interleaved), i.e. the concatenation of the reference's
+ *    std::vector<std::vector<std::complex<double>>> solutions
+ *    (ddecal/gain_solvers/SolverBase.h:205-227).
+ *  - One context = one CUDA stream on one device. Contexts are not re-entrant;
+ *    distinct contexts may be used from distinct threads.
+ *  - The library never falls back to the CPU: without a usable sm_100 device
+ *    ddsolve_create() fails with DDSOLVE_E_CUDA.
+ */
+#ifndef DDSOLVE_B200_H
+#define DDSOLVE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DDSOLVE_API __attribute__((visibility("default")))
+#else
+#define DDSOLVE_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DDSOLVE_OK 0
+#define DDSOLVE_E_INVALID 1     /* bad argument / dimension */
+#define DDSOLVE_E_CUDA 2        /* CUDA runtime error */
+#define DDSOLVE_E_STATE 3       /* call out of order (e.g. solve before data) */
+#define DDSOLVE_E_UNSUPPORTED 4 /* valid but not supported combination */
+#define DDSOLVE_E_TIMEOUT 5     /* a device-side bounded wait gave up */
+
+typedef struct ddsolve_ctx ddsolve_ctx;
+
+/* Dimensions; replaces SolverBase::Initialize(n_antennas,
+ * n_solutions_per_direction, n_channel_blocks)
+ * (ddecal/gain_solvers/SolverBase.h:76-78, SolverBase.cc:41-61) plus the
+ * solver choice made by SolverFactory::CreateDiagonalSolver /
+ * CreateScalarSolver (ddecal/SolverFactory.cc:49-146). */
+typedef struct {
+  uint32_t n_antennas;
+  uint32_t n_directions;
+  uint32_t n_channel_blocks;
+  uint32_t n_correlations;           /* 1, 2 or 4, see above */
+  uint32_t n_solution_polarizations; /* 2 = IterativeDiagonalSolver,
+                                        1 = IterativeScalarSolver */
+  const uint32_t* n_solutions_per_direction; /* [n_directions], >= 1 */
+} ddsolve_dims;
+
+/* Solver settings; replaces the SolverBase setters SetMaxIterations,
+ * SetMinIterations, SetAccuracy, SetConstraintAccuracy, SetStepSize,
+ * SetDetectStalling and SetPhaseOnly (ddecal/gain_solvers/SolverBase.h:89-177)
+ * with the defaults of SolverBase::SolverBase (SolverBase.cc:27-39). */
+typedef struct {
+  uint32_t max_iterations;
+  uint32_t min_iterations;
+  double accuracy;
+  double constraint_accuracy;
+  double step_size;
+  int32_t detect_stalling;
+  double step_diff_sigma;
+  int32_t phase_only;
+} ddsolve_settings;
+
+/* Replaces SolverBase::SolveResult (ddecal/gain_solvers/SolverBase.h:61-65):
+ * iterations follows SolverBase::MakeResult (SolverBase.cc:192-213). */
+typedef struct {
+  uint32_t iterations;
+  uint32_t constraint_iterations;
+  int32_t has_converged;
+  int32_t has_stalled;
+} ddsolve_result;
+
+/* Creates a solver on CUDA device `device` (ordinal). Replaces constructing
+ * IterativeDiagonalSolver<V> / IterativeScalarSolver<V> and calling
+ * SolverBase::Initialize (ddecal/gain_solvers/SolverBase.cc:41-61): the same
+ * dimension checks apply. */
+DDSOLVE_API int ddsolve_create(const ddsolve_dims* dims, int device, ddsolve_ctx** out);
+
+/* Frees all device memory of the context. NULL is accepted. */
+DDSOLVE_API int ddsolve_destroy(ddsolve_ctx* ctx);
+
+/* Message of the last failure on this context (or of the last failed create
+ * on this thread when ctx == NULL). Never NULL. */
+DDSOLVE_API const char* ddsolve_last_error(const ddsolve_ctx* ctx);
+
+/* Default settings of SolverBase::SolverBase (SolverBase.cc:27-39). */
+DDSOLVE_API void ddsolve_default_settings(ddsolve_settings* settings);
+
+/* Replaces the SolverBase setters (SolverBase.h:89-177). */
+DDSOLVE_API int ddsolve_set_settings(ddsolve_ctx* ctx, const ddsolve_settings* settings);
+
+/* Uploads one channel block of a SolveData, in the reference layout above
+ * (replaces reading SolveData<V>::ChannelBlockData, SolveData.h:31-133, inside
+ * IterativeDiagonalSolver::Solve). Any visibility order and antenna/solution
+ * assignment is accepted (regular and BDA data); consecutive visibilities
+ * that share antennas and solution indices are solved together. Host pointers;
+ * pinned memory makes the copy asynchronous. Replaces any previous data of
+ * that channel block. */
+DDSOLVE_API int ddsolve_set_channel_block(ddsolve_ctx* ctx, uint32_t channel_block,
+                              uint64_t n_vis, const float* data,
+                              const float* model,
+                              const uint32_t* antenna_pairs,
+                              const uint32_t* solution_map);
+
+/* Same as ddsolve_set_channel_block for data packed by the regular SolveData
+ * constructor (ddecal/gain_solvers/SolveData.cc:77-188): visibility index
+ * ((t * n_baselines) + b) * n_channels + c, baseline b between antenna1[b] and
+ * antenna2[b] (autocorrelations already removed), solution index of direction
+ * d at time t = t * min(n_sol[d], n_times) / n_times + first solution of d.
+ * No per-visibility antenna / solution arrays are read. */
+DDSOLVE_API int ddsolve_set_channel_block_regular(ddsolve_ctx* ctx, uint32_t channel_block,
+                                      uint32_t n_times, uint32_t n_baselines,
+                                      uint32_t n_channels, const float* data,
+                                      const float* model,
+                                      const uint32_t* antenna1,
+                                      const uint32_t* antenna2);
+
+/* Full iterate-until-converged solve on the device with no host constraints:
+ * replaces IterativeDiagonalSolver<V>::Solve
+ * (ddecal/gain_solvers/IterativeDiagonalSolver.cc:38-97) and
+ * IterativeScalarSolver<V>::Solve (IterativeScalarSolver.cc:30-89) for a
+ * solver without constraints. `solutions` (host) holds the initial values on
+ * entry and the result on return, like the reference's in/out argument.
+ * step_magnitudes (optional, host, [max_iterations]) receives the step
+ * magnitude of every iteration (the statistics stream of the reference's
+ * stat_stream overload). */
+DDSOLVE_API int ddsolve_solve(ddsolve_ctx* ctx, double* solutions, ddsolve_result* result,
+                  double* step_magnitudes);
+
+/* One direction-iterative pass over every channel block:
+ * next_solutions = sum(num) / sum(den) per antenna, sub-solution and
+ * polarization, NaN where the denominator is zero -- exactly the
+ * next_solutions tensor that IterativeDiagonalSolver::PerformIteration
+ * (IterativeDiagonalSolver.cc:100-222) / IterativeScalarSolver
+ * (IterativeScalarSolver.cc:91-195) fill before SolverBase::Step. Use it to
+ * run the iteration loop on the host when host constraints
+ * (SolverBase::ApplyConstraints, SolverBase.cc:166-190) are present. Host
+ * pointers, layout as `solutions`. */
+DDSOLVE_API int ddsolve_perform_iteration(ddsolve_ctx* ctx, const double* solutions,
+                              double* next_solutions);
+
+/* The CUDA stream of the context (a cudaStream_t), so that callers can order
+ * their own work or CUDA events against the solver. */
+DDSOLVE_API void* ddsolve_stream(ddsolve_ctx* ctx);
+
+/* Tuning of the streaming kernel: directions per thread group (0 = auto) and
+ * the maximum number of time steps folded into one slab (0 = all). Replaces
+ * nothing in the reference (its thread count is SolverBase::NSubThreads). */
+DDSOLVE_API int ddsolve_set_tuning(ddsolve_ctx* ctx, uint32_t direction_groups,
+                       uint32_t max_slab_times);
+
+/* Device time of the streaming kernel: launches it n_launches times on the
+ * context stream with the current solutions and returns the mean duration in
+ * milliseconds, measured with CUDA events. Solutions are not modified. */
+DDSOLVE_API int ddsolve_time_stream_kernel(ddsolve_ctx* ctx, uint32_t n_launches,
+                               float* mean_ms);
+
+/* Number of kernel launches issued by the last ddsolve_solve call. */
+DDSOLVE_API uint64_t ddsolve_last_launch_count(const ddsolve_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
