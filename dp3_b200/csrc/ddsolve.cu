@@ -727,15 +727,18 @@ struct DevBuf {
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), bytes(o.bytes) {
+  DevBuf(DevBuf&& o) noexcept
+      : ptr(o.ptr), bytes(o.bytes), realloc_flag(o.realloc_flag) {
     o.ptr = nullptr;
     o.bytes = 0;
   }
   ~DevBuf() {
     if (ptr) cudaFree(ptr);
   }
+  bool realloc_flag = false;  // set when Reserve() moved the buffer
   cudaError_t Reserve(size_t n) {
     if (n <= bytes && ptr) return cudaSuccess;
+    realloc_flag = true;
     if (ptr) cudaFree(ptr);
     ptr = nullptr;
     bytes = 0;
@@ -757,6 +760,16 @@ struct HostSlab {
   std::vector<uint32_t> sol;  // [n_dir]
 };
 
+bool SameLayout(const std::vector<HostSlab>& a, const std::vector<HostSlab>& b) {
+  if (a.size() != b.size()) return false;
+  for (size_t i = 0; i < a.size(); ++i)
+    if (a[i].T != b[i].T || a[i].L != b[i].L || a[i].R != b[i].R ||
+        a[i].elem_off != b[i].elem_off || a[i].run_off != b[i].run_off ||
+        a[i].sol != b[i].sol)
+      return false;
+  return true;
+}
+
 struct ChannelBlockStore {
   bool set = false;
   uint64_t n_vis = 0;
@@ -764,6 +777,10 @@ struct ChannelBlockStore {
   std::vector<HostSlab> slabs;
   std::vector<uint32_t> run_ant, run_src, run_len;
   DevBuf data, model, run_ant_dev;
+  // Layout of the previous upload; an upload with the same layout into the
+  // same buffers keeps the streaming plan (and its CUDA graph) valid.
+  std::vector<HostSlab> prev_slabs;
+  std::vector<uint32_t> prev_run_ant;
 };
 
 using StreamFn = void (*)(StreamParams);
@@ -882,6 +899,7 @@ int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const float* data,
   const size_t E = ctx->elem_bytes;
   const size_t src_bytes = size_t(cb.n_vis) * E * (1 + ctx->n_dir);
   DDS_CHECK_CUDA(ctx, ctx->staging.Reserve(src_bytes));
+  cb.data.realloc_flag = cb.model.realloc_flag = cb.run_ant_dev.realloc_flag = false;
   DDS_CHECK_CUDA(ctx, cb.data.Reserve(cb.n_elems * E));
   DDS_CHECK_CUDA(ctx, cb.model.Reserve(cb.n_elems * E * ctx->n_dir));
   DDS_CHECK_CUDA(ctx, cb.run_ant_dev.Reserve(cb.run_ant.size() * 4));
@@ -937,8 +955,15 @@ int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const float* data,
   }
   // The staging and run arrays are reused by the next upload: keep the
   // stream order (a later upload's copies follow these kernels).
+  const bool moved =
+      cb.data.realloc_flag || cb.model.realloc_flag || cb.run_ant_dev.realloc_flag;
+  if (!cb.set || moved || !SameLayout(cb.slabs, cb.prev_slabs) ||
+      cb.run_ant != cb.prev_run_ant) {
+    ctx->plan_dirty = true;
+    cb.prev_slabs = cb.slabs;
+    cb.prev_run_ant = cb.run_ant;
+  }
   cb.set = true;
-  ctx->plan_dirty = true;
   return DDSOLVE_OK;
 }
 
