@@ -47,6 +47,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <type_traits>
@@ -1643,3 +1644,306 @@ int ddsolve_time_stream_kernel(ddsolve_ctx* ctx, uint32_t n_launches, float* mea
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point: one direction-iterative pass over regular
+// data that the caller already holds in device memory, with the per-antenna
+// accumulators in a fixed-size array that lives in the library's own device
+// image. Some callers cannot let a library allocate device memory: code that
+// runs while a CUDA graph is being captured (cudaMalloc is not allowed
+// during capture), frameworks that hand all device memory out of their own
+// pool or arena, and hosts whose device memory is already fully budgeted.
+// This variant only uses that static array; it never calls cudaMalloc,
+// cudaFree or an allocating library routine.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocScratchFloats = size_t(1) << 20;  // 4 MiB
+constexpr uint32_t kNoAllocMaxChannelBlocks = 256;
+constexpr uint32_t kNoAllocMaxDirections = 64;
+constexpr uint32_t kNoAllocMaxChannels = 16;  // channels per block
+constexpr int kNoAllocThreads = 128;
+
+// Per-antenna accumulators [cb][ant][sub][pol][num.re, num.im, den]. Every
+// GPU that loads this library holds these 4 MiB until the process exits.
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocScratchFloats];
+
+struct NoAllocParams {
+  const float* data;
+  const float* model;
+  const uint32_t* antenna1;
+  const uint32_t* antenna2;
+  const double2* solutions;
+  double2* next;
+  float* acc;
+  uint32_t n_ant, n_dir, n_sub, n_cb, n_times, n_bl;
+  uint32_t cb_channels[kNoAllocMaxChannelBlocks];
+  uint64_t cb_vis_offset[kNoAllocMaxChannelBlocks];  // first visibility of cb
+  uint32_t n_sol[kNoAllocMaxDirections];             // min(n_sol, n_times)
+  uint32_t sol_start[kNoAllocMaxDirections];
+};
+
+// One thread per (channel block, time step, baseline): residual over the
+// block's channels, then per direction P = sum R conj(M), Q = sum |M|^2 and
+// the antenna contributions added atomically into the scratch accumulators.
+template <int NCORR, int NPOL>
+__global__ void __launch_bounds__(kNoAllocThreads)
+    noalloc_accumulate_kernel(const NoAllocParams p) {
+  const uint32_t bl = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t t = blockIdx.y;
+  const uint32_t cb = blockIdx.z;
+  if (bl >= p.n_bl) return;
+  const uint32_t a1 = p.antenna1[bl];
+  const uint32_t a2 = p.antenna2[bl];
+  if (a1 >= p.n_ant || a2 >= p.n_ant) return;  // invalid pairs are ignored
+  const uint32_t L = p.cb_channels[cb];
+  const uint64_t n_vis_cb = uint64_t(p.n_times) * p.n_bl * L;
+  const uint64_t v0 = (uint64_t(t) * p.n_bl + bl) * L;
+  const float* data = p.data + p.cb_vis_offset[cb] * NCORR * 2;
+  const float* model = p.model + p.cb_vis_offset[cb] * p.n_dir * NCORR * 2;
+
+  float2 R[kNoAllocMaxChannels][NCORR];
+#pragma unroll
+  for (uint32_t ch = 0; ch < kNoAllocMaxChannels; ++ch)
+    if (ch < L) LoadVis<NCORR>(data, v0 + ch, R[ch]);
+
+  auto gain = [&](uint32_t ant, uint32_t s, int q) {
+    const double2 g = p.solutions[(size_t(cb * p.n_ant + ant) * p.n_sub + s) * NPOL + q];
+    return make_float2(float(g.x), float(g.y));
+  };
+  auto sol_of = [&](uint32_t d) {
+    return uint32_t(uint64_t(t) * p.n_sol[d] / p.n_times) + p.sol_start[d];
+  };
+  // Residual: R = D - sum_d G_d M_d
+  for (uint32_t d = 0; d < p.n_dir; ++d) {
+    const uint32_t s = sol_of(d);
+    float2 ga[NPOL], gb[NPOL];
+#pragma unroll
+    for (int q = 0; q < NPOL; ++q) {
+      ga[q] = gain(a1, s, q);
+      gb[q] = gain(a2, s, q);
+    }
+#pragma unroll
+    for (uint32_t ch = 0; ch < kNoAllocMaxChannels; ++ch) {
+      if (ch >= L) break;
+      float2 M[NCORR];
+      LoadVis<NCORR>(model, d * n_vis_cb + v0 + ch, M);
+#pragma unroll
+      for (int c = 0; c < NCORR; ++c) {
+        const float2 G = cmul_conj(ga[RowPol<NCORR, NPOL>(c)], gb[ColPol<NCORR, NPOL>(c)]);
+        const float2 gm = cmul(G, M[c]);
+        R[ch][c].x -= gm.x;
+        R[ch][c].y -= gm.y;
+      }
+    }
+  }
+  // Normal equations of every direction.
+  for (uint32_t d = 0; d < p.n_dir; ++d) {
+    const uint32_t s = sol_of(d);
+    float2 P[NCORR];
+    float Q[NCORR];
+#pragma unroll
+    for (int c = 0; c < NCORR; ++c) {
+      P[c] = make_float2(0.f, 0.f);
+      Q[c] = 0.f;
+    }
+#pragma unroll
+    for (uint32_t ch = 0; ch < kNoAllocMaxChannels; ++ch) {
+      if (ch >= L) break;
+      float2 M[NCORR];
+      LoadVis<NCORR>(model, d * n_vis_cb + v0 + ch, M);
+#pragma unroll
+      for (int c = 0; c < NCORR; ++c) {
+        const float2 rm = cmul_conj(R[ch][c], M[c]);
+        P[c].x += rm.x;
+        P[c].y += rm.y;
+        Q[c] += cnorm(M[c]);
+      }
+    }
+    float2 ga[NPOL], gb[NPOL];
+#pragma unroll
+    for (int q = 0; q < NPOL; ++q) {
+      ga[q] = gain(a1, s, q);
+      gb[q] = gain(a2, s, q);
+    }
+#pragma unroll
+    for (int q = 0; q < NPOL; ++q) {
+      float2 n1 = make_float2(0.f, 0.f), n2 = make_float2(0.f, 0.f);
+      float d1 = 0.f, d2 = 0.f;
+#pragma unroll
+      for (int c = 0; c < NCORR; ++c) {
+        const int rp = RowPol<NCORR, NPOL>(c);
+        const int cp = ColPol<NCORR, NPOL>(c);
+        if (rp == q) {
+          const float2 t1 = cmul(gb[cp], P[c]);
+          n1.x += t1.x;
+          n1.y += t1.y;
+          d1 += cnorm(gb[cp]) * Q[c];
+        }
+        if (cp == q) {
+          const float2 t2 = cmul(ga[rp], cconj(P[c]));
+          n2.x += t2.x;
+          n2.y += t2.y;
+          d2 += cnorm(ga[rp]) * Q[c];
+        }
+      }
+      float* acc1 = p.acc + ((size_t(cb * p.n_ant + a1) * p.n_sub + s) * NPOL + q) * 3;
+      float* acc2 = p.acc + ((size_t(cb * p.n_ant + a2) * p.n_sub + s) * NPOL + q) * 3;
+      atomicAdd(acc1 + 0, n1.x);
+      atomicAdd(acc1 + 1, n1.y);
+      atomicAdd(acc1 + 2, d1);
+      atomicAdd(acc2 + 0, n2.x);
+      atomicAdd(acc2 + 1, n2.y);
+      atomicAdd(acc2 + 2, d2);
+    }
+  }
+}
+
+// next = g_a + num / den per (cb, ant, sub, pol); NaN where den == 0.
+template <int NPOL>
+__global__ void __launch_bounds__(kThreads)
+    noalloc_finalize_kernel(const float* __restrict__ acc,
+                            const double2* __restrict__ solutions,
+                            double2* __restrict__ next, uint32_t n_items) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_items) return;
+#pragma unroll
+  for (int q = 0; q < NPOL; ++q) {
+    const size_t e = size_t(i) * NPOL + q;
+    const float den = acc[e * 3 + 2];
+    if (den == 0.f) {
+      next[e] = make_double2(nan(""), 0.0);
+    } else {
+      const double2 g = solutions[e];
+      next[e] = make_double2(double(float(g.x)) + double(acc[e * 3]) / double(den),
+                             double(float(g.y)) + double(acc[e * 3 + 1]) / double(den));
+    }
+  }
+}
+
+// Device address of g_noalloc_scratch, looked up once per device (with that
+// device current) and cached.
+int NoAllocScratchAddress(int device, float** out) {
+  static std::mutex mu;
+  static std::map<int, float*> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(device);
+  if (it != cache.end()) {
+    *out = it->second;
+    return DDSOLVE_OK;
+  }
+  float* ptr = nullptr;
+  const cudaError_t e =
+      cudaGetSymbolAddress(reinterpret_cast<void**>(&ptr), g_noalloc_scratch);
+  if (e != cudaSuccess || !ptr) {
+    g_last_error = std::string("ddsolve_perform_iteration_noalloc: "
+                               "cudaGetSymbolAddress failed: ") +
+                   cudaGetErrorString(e);
+    return DDSOLVE_E_CUDA;
+  }
+  cache[device] = ptr;
+  *out = ptr;
+  return DDSOLVE_OK;
+}
+
+template <int NCORR, int NPOL>
+void LaunchNoAlloc(const NoAllocParams& p, uint32_t n_items, cudaStream_t s) {
+  const dim3 grid((p.n_bl + kNoAllocThreads - 1) / kNoAllocThreads, p.n_times, p.n_cb);
+  noalloc_accumulate_kernel<NCORR, NPOL><<<grid, kNoAllocThreads, 0, s>>>(p);
+  noalloc_finalize_kernel<NPOL><<<(n_items + kThreads - 1) / kThreads, kThreads, 0, s>>>(
+      p.acc, p.solutions, p.next, n_items);
+}
+
+}  // namespace
+
+extern "C" int ddsolve_perform_iteration_noalloc(
+    const ddsolve_dims* dims, uint32_t n_times, uint32_t n_baselines,
+    const uint32_t* cb_channels, const float* data, const float* model,
+    const uint32_t* antenna1, const uint32_t* antenna2, const double* solutions,
+    double* next_solutions, void* stream) {
+  const char* who = "ddsolve_perform_iteration_noalloc: ";
+  const int dc = CheckDims(dims);
+  if (dc != DDSOLVE_OK) {
+    g_last_error = std::string(who) + "invalid or unsupported dimensions";
+    return dc;
+  }
+  if (!cb_channels || !data || !model || !antenna1 || !antenna2 || !solutions ||
+      !next_solutions || n_times == 0 || n_baselines == 0) {
+    g_last_error = std::string(who) + "NULL pointer or empty interval";
+    return DDSOLVE_E_INVALID;
+  }
+  const uint32_t n_cb = dims->n_channel_blocks, n_dir = dims->n_directions;
+  const uint32_t n_ant = dims->n_antennas, n_pol = dims->n_solution_polarizations;
+  uint32_t n_sub = 0;
+  for (uint32_t d = 0; d < n_dir; ++d) n_sub += dims->n_solutions_per_direction[d];
+  if (n_cb > kNoAllocMaxChannelBlocks || n_dir > kNoAllocMaxDirections) {
+    g_last_error = std::string(who) + "more than 256 channel blocks or 64 directions";
+    return DDSOLVE_E_UNSUPPORTED;
+  }
+  const uint64_t acc_floats = uint64_t(n_cb) * n_ant * n_sub * n_pol * 3;
+  if (acc_floats > kNoAllocScratchFloats) {
+    g_last_error = std::string(who) + "channel blocks x antennas x sub-solutions x "
+                   "polarizations x 3 = " + std::to_string(acc_floats) +
+                   " exceeds the static scratch of " +
+                   std::to_string(kNoAllocScratchFloats) + " floats";
+    return DDSOLVE_E_UNSUPPORTED;
+  }
+  NoAllocParams p;
+  p.data = data;
+  p.model = model;
+  p.antenna1 = antenna1;
+  p.antenna2 = antenna2;
+  p.solutions = reinterpret_cast<const double2*>(solutions);
+  p.next = reinterpret_cast<double2*>(next_solutions);
+  p.n_ant = n_ant;
+  p.n_dir = n_dir;
+  p.n_sub = n_sub;
+  p.n_cb = n_cb;
+  p.n_times = n_times;
+  p.n_bl = n_baselines;
+  uint64_t off = 0;
+  for (uint32_t c = 0; c < n_cb; ++c) {
+    if (cb_channels[c] == 0 || cb_channels[c] > kNoAllocMaxChannels) {
+      g_last_error = std::string(who) + "channels per block must be 1..16";
+      return DDSOLVE_E_UNSUPPORTED;
+    }
+    p.cb_channels[c] = cb_channels[c];
+    p.cb_vis_offset[c] = off;
+    off += uint64_t(n_times) * n_baselines * cb_channels[c];
+  }
+  uint32_t start = 0;
+  for (uint32_t d = 0; d < n_dir; ++d) {
+    p.n_sol[d] = std::min(dims->n_solutions_per_direction[d], n_times);
+    p.sol_start[d] = start;
+    start += p.n_sol[d];
+  }
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) {
+    g_last_error = std::string(who) + cudaGetErrorString(e);
+    return DDSOLVE_E_CUDA;
+  }
+  float* scratch = nullptr;
+  const int rc = NoAllocScratchAddress(device, &scratch);
+  if (rc != DDSOLVE_OK) return rc;
+  p.acc = scratch;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  e = cudaMemsetAsync(scratch, 0, acc_floats * sizeof(float), s);
+  if (e != cudaSuccess) {
+    g_last_error = std::string(who) + cudaGetErrorString(e);
+    return DDSOLVE_E_CUDA;
+  }
+  const uint32_t n_items = n_cb * n_ant * n_sub;
+  const uint32_t nc = dims->n_correlations;
+  if (nc == 2 && n_pol == 2) LaunchNoAlloc<2, 2>(p, n_items, s);
+  else if (nc == 4 && n_pol == 2) LaunchNoAlloc<4, 2>(p, n_items, s);
+  else if (nc == 1 && n_pol == 1) LaunchNoAlloc<1, 1>(p, n_items, s);
+  else if (nc == 2 && n_pol == 1) LaunchNoAlloc<2, 1>(p, n_items, s);
+  else LaunchNoAlloc<4, 1>(p, n_items, s);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    g_last_error = std::string(who) + cudaGetErrorString(e);
+    return DDSOLVE_E_CUDA;
+  }
+  return DDSOLVE_OK;
+}

@@ -22,7 +22,7 @@ EXPORTED_SYMBOLS = (
     "ddsolve_set_channel_block", "ddsolve_set_channel_block_regular",
     "ddsolve_solve", "ddsolve_perform_iteration", "ddsolve_stream",
     "ddsolve_set_tuning", "ddsolve_time_stream_kernel",
-    "ddsolve_last_launch_count",
+    "ddsolve_last_launch_count", "ddsolve_perform_iteration_noalloc",
 )
 
 

@@ -178,6 +178,45 @@ DDSOLVE_API int ddsolve_set_tuning(ddsolve_ctx* ctx, uint32_t direction_groups,
 DDSOLVE_API int ddsolve_time_stream_kernel(ddsolve_ctx* ctx, uint32_t n_launches,
                                float* mean_ms);
 
+/* Allocation-free direction-iterative pass (no counterpart in the reference:
+ * DP3's solvers always own their buffers).
+ *
+ * Some callers cannot let a library allocate device memory: code running
+ * while a CUDA graph is being captured (cudaMalloc is not permitted during
+ * capture), frameworks that serve all device memory from their own pool or
+ * arena, and processes whose device memory is budgeted in advance. This
+ * entry point computes the same next_solutions as ddsolve_perform_iteration
+ * without a context and without calling cudaMalloc, cudaFree or any
+ * allocating library routine. Its per-antenna accumulators live in one fixed
+ * 4 MiB array compiled into this library; every GPU that loads the library
+ * holds that array until the process exits.
+ *
+ * Inputs and outputs are DEVICE pointers the caller owns, for regular data
+ * in the layout of ddsolve_set_channel_block_regular, with the channel blocks
+ * concatenated: data = cb 0's [n_times*n_baselines*cb_channels[0]][n_corr][2]
+ * floats, then cb 1's, ...; model = cb 0's [n_dir][n_vis_cb0][n_corr][2],
+ * then cb 1's, ...; antenna1 / antenna2 [n_baselines]; solutions and
+ * next_solutions [n_cb][n_ant][n_sub][n_pol] complex double. dims and
+ * cb_channels are host pointers. Baselines with an antenna index
+ * >= n_antennas are skipped.
+ *
+ * Limits (DDSOLVE_E_UNSUPPORTED with a message beyond them): at most 256
+ * channel blocks, 64 directions and 16 channels per block, and
+ * n_cb * n_ant * n_sub * n_pol * 3 <= 1048576 accumulators.
+ *
+ * Work is queued on `stream` (a cudaStream_t; NULL = the legacy default
+ * stream) and the call returns without waiting. The first call on a device
+ * looks up the array's device address with that device current; make that
+ * first call before any stream capture. Every call reuses the same array and
+ * clears the part it needs at its start, so calls that overlap on the GPU
+ * (different streams or devices sharing a context) race: order them on one
+ * stream or synchronise between them. */
+DDSOLVE_API int ddsolve_perform_iteration_noalloc(
+    const ddsolve_dims* dims, uint32_t n_times, uint32_t n_baselines,
+    const uint32_t* cb_channels, const float* data, const float* model,
+    const uint32_t* antenna1, const uint32_t* antenna2,
+    const double* solutions, double* next_solutions, void* stream);
+
 /* Number of kernel launches issued by the last ddsolve_solve call. */
 DDSOLVE_API uint64_t ddsolve_last_launch_count(const ddsolve_ctx* ctx);
 
