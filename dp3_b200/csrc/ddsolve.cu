@@ -44,6 +44,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -68,8 +69,16 @@ struct SlabDesc {
   const uint32_t* run_ant;  // [R] antenna1 | antenna2 << 16
   uint32_t cb, T, L, R;
   uint32_t sol_off;  // first of n_dir entries in slab_sol
-  uint32_t pad;
+  uint32_t table;    // gain table of the slab (pipe_kernel)
 };
+
+// pipe_kernel work item: rows [row_lo, row_hi) of the (t, channel) rows of
+// the tile of runs [r0, r0 + n_runs) of a slab; fragments of one CTA that
+// share a slab form a visit (one partial slot).
+struct Frag {
+  uint32_t slab, r0, n_runs, flags, row_lo, row_hi, visit, pad;
+};
+constexpr uint32_t kFragDirect = 1u;  // distinct antennas on both sides
 
 struct Visit {
   uint32_t slab, run_lo, run_hi, pad;
@@ -179,8 +188,15 @@ __device__ __forceinline__ void LoadVis(const void* base, size_t idx,
 // ---------------------------------------------------------------------------
 // Pack kernel: reference SolveData layout -> slab layout.
 // dst element (t, ch, r) of a slab <- source visibility
-//   src_base + t * tstride + run_src[r] + ch   (zero if ch >= run_len[r])
+//   src_base + t * tstride + run_src[r] + ch   (zero if ch >= run length)
+// A run whose length carries kRunFlipped stores the baseline with its
+// antennas swapped: visibility and model are Hermitian-transposed
+// (conjugated, with XY and YX exchanged for full 2x2 data), which leaves the
+// solver's normal equations unchanged (the contribution of antenna 1 of the
+// flipped run is that of antenna 2 of the original one, and vice versa).
 // ---------------------------------------------------------------------------
+constexpr uint32_t kRunFlipped = 0x80000000u;
+
 struct PackSlab {
   uint64_t dst_elem_off;  // into the cb's packed data buffer
   uint64_t src_base;
@@ -188,46 +204,54 @@ struct PackSlab {
   uint32_t T, L, R, run_off;
 };
 
-template <int E>  // element size in bytes (8, 16, 32)
+template <int NCORR>
+__device__ __forceinline__ void CopyVis(const float2* __restrict__ src, float2* __restrict__ dst,
+                                        bool valid, bool flip) {
+  float2 v[NCORR];
+#pragma unroll
+  for (int c = 0; c < NCORR; ++c) v[c] = valid ? src[c] : make_float2(0.f, 0.f);
+  if (flip) {
+#pragma unroll
+    for (int c = 0; c < NCORR; ++c) v[c].y = -v[c].y;
+    if constexpr (NCORR == 4) {
+      const float2 t = v[1];
+      v[1] = v[2];
+      v[2] = t;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < NCORR; ++c) dst[c] = v[c];
+}
+
+template <int NCORR>
 __global__ void pack_kernel(const PackSlab* __restrict__ slabs, uint32_t slab,
                             const uint32_t* __restrict__ run_src,
                             const uint32_t* __restrict__ run_len,
-                            const char* __restrict__ src_data,
-                            const char* __restrict__ src_model, uint64_t n_vis,
-                            uint32_t n_dir, uint64_t n_elems_cb,
-                            char* __restrict__ dst_data,
-                            char* __restrict__ dst_model) {
+                            const float2* __restrict__ src_data,
+                            const float2* __restrict__ src_model, uint64_t n_vis,
+                            uint32_t n_dir, float2* __restrict__ dst_data,
+                            float2* __restrict__ dst_model) {
   const PackSlab s = slabs[slab];
   const uint64_t tlr = uint64_t(s.T) * s.L * s.R;
-  using Word = typename std::conditional<E == 8, float2, float4>::type;
-  constexpr int kWords = E / int(sizeof(Word));
   for (uint64_t e = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; e < tlr;
        e += uint64_t(gridDim.x) * blockDim.x) {
     const uint32_t r = uint32_t(e % s.R);
     const uint64_t tl = e / s.R;
     const uint32_t ch = uint32_t(tl % s.L);
     const uint32_t t = uint32_t(tl / s.L);
-    const bool valid = ch < run_len[s.run_off + r];
-    const uint64_t v = s.src_base + t * s.tstride + run_src[s.run_off + r] + ch;
+    const uint32_t len = run_len[s.run_off + r];
+    const bool flip = (len & kRunFlipped) != 0;
+    const bool valid = ch < (len & ~kRunFlipped);
+    const uint64_t v = valid ? s.src_base + t * s.tstride + run_src[s.run_off + r] + ch : 0;
     const uint64_t dst = s.dst_elem_off + e;
-    Word zero;
-    memset(&zero, 0, sizeof(zero));
-    for (int w = 0; w < kWords; ++w) {
-      reinterpret_cast<Word*>(dst_data)[dst * kWords + w] =
-          valid ? reinterpret_cast<const Word*>(src_data)[v * kWords + w] : zero;
-    }
+    CopyVis<NCORR>(src_data + v * NCORR, dst_data + dst * NCORR, valid, flip);
     // model block of the slab: [n_dir][T][L][R] starting at n_dir * dst_elem_off
     for (uint32_t d = 0; d < n_dir; ++d) {
       const uint64_t md = uint64_t(n_dir) * s.dst_elem_off + d * tlr + e;
-      const uint64_t ms = d * n_vis + v;
-      for (int w = 0; w < kWords; ++w) {
-        reinterpret_cast<Word*>(dst_model)[md * kWords + w] =
-            valid ? reinterpret_cast<const Word*>(src_model)[ms * kWords + w]
-                  : zero;
-      }
+      CopyVis<NCORR>(src_model + (d * n_vis + v) * NCORR, dst_model + md * NCORR,
+                     valid, flip);
     }
   }
-  (void)n_elems_cb;
 }
 
 // ---------------------------------------------------------------------------
@@ -709,6 +733,840 @@ __global__ void __launch_bounds__(kThreads) finalize_kernel(const FinParams p) {
 }
 
 // ---------------------------------------------------------------------------
+// pipe_kernel: the Blackwell streaming path. Per CTA one producer warp moves
+// the (time, channel) rows of each tile (224 runs) from HBM into a ring of
+// shared-memory stages with 1-D bulk copies (cp.async.bulk, completion on an
+// mbarrier, no multicast); seven consumer warps (one run per lane) compute
+// the residual and the per-direction P/Q sums from shared memory. Runs are
+// stored in baseline-diagonal order, so within a warp the 32 first antennas
+// are distinct and so are the 32 second antennas: every shared-memory atomic
+// of the antenna reduction is conflict-free and no warp shuffles are needed.
+// The accumulator and gain tables use an odd per-antenna stride, so the 32
+// lanes of one atomic hit 32 different banks.
+//
+// The finalisation is fused: the CTA that flushes the last partial slot of a
+// channel block finalises that block (merge, FP64 update, step, norm,
+// non-finite detection for the lazy MakeSolutionsFinite), and the CTA that
+// finalises the last channel block runs the iteration control. One launch per
+// iteration. Every wait is bounded by a 4 s device timer; a timeout sets an
+// error flag that the host reports as DDSOLVE_E_TIMEOUT, and all later waits
+// of that CTA return at once so that the kernel still ends.
+// ---------------------------------------------------------------------------
+constexpr int kPipeConsumerWarps = 7;
+constexpr int kPipeRuns = kPipeConsumerWarps * 32;  // runs per tile
+constexpr int kPipeThreads = kPipeRuns + 32;         // + one producer warp
+constexpr int kPipeMaxStages = 8;
+static_assert(kPipeRuns <= 256 && kPipeRuns % 32 == 0, "tree reductions assume <= 256 consumers");
+constexpr uint64_t kWaitBudgetNs = 4000000000ull;
+
+struct PipeParams {
+  const SlabDesc* slabs;
+  const Frag* frags;
+  const uint32_t* cta_frag_off;
+  const uint32_t* slab_sol;
+  double2* solutions;
+  float* partials;
+  float2* tables;         // gain tables [n_tables][table_f2]
+  uint32_t table_f2;      // float2 per table (n_ant * gain_stride, even)
+  const uint32_t* tab_off;  // finalisation: (cb, s) -> [tab_off, tab_off+1)
+  const uint32_t* tab_ent;  //   entries table * 256 + direction
+  uint32_t n_ant, n_dir, n_sub, n_cb;
+  uint32_t acc_stride;    // floats per antenna in the accumulator table (odd)
+  uint32_t gain_stride;   // float2 per antenna in a gain table (odd)
+  uint32_t stages;
+  uint32_t acc_floats;    // n_ant * acc_stride = one partial slot
+  uint32_t owner_groups;  // direction groups per antenna in the sorted reduction
+  // shared-memory layout (byte offsets)
+  uint32_t off_acc, off_gtab, off_stg, off_cnt, off_off, off_pair, off_ent,
+      off_wsum, off_stages;
+  const uint32_t* fin_off;
+  const uint32_t* fin_visits;
+  const uint32_t* dir_of_sub;
+  uint32_t* cb_flag;     // channel block holds non-finite solutions
+  double* cb_avg;        // replacement value for them (MakeSolutionsFinite)
+  uint32_t* cb_newflag;  // set during the finalisation that produced them
+  double* block_sum;     // per-CTA norm partials
+  uint32_t* block_cnt;
+  uint32_t* counters;    // [0] CTAs finalised, [1] error flag, [2] grid barrier
+  double2* next_out;
+  int32_t host_mode;
+  const DevSettings* settings;
+  LoopState* state;
+  double* step_magnitudes;
+  cudaGraphConditionalHandle handle;
+  int32_t use_handle;
+};
+
+__device__ __forceinline__ uint32_t SmemAddr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void MbarInit(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(SmemAddr(bar)),
+               "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void MbarArriveExpectTx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                   SmemAddr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void MbarArrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(SmemAddr(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool MbarTryWait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n"
+      " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(SmemAddr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void BulkCopyG2S(void* dst, const void* src,
+                                            uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1], %2, [%3];" ::"r"(SmemAddr(dst)),
+      "l"(src), "r"(bytes), "r"(SmemAddr(bar))
+      : "memory");
+}
+__device__ __forceinline__ uint64_t GlobalTimerNs() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void ConsumerBarrier() {
+  asm volatile("bar.sync 1, %0;" ::"n"(kPipeRuns) : "memory");
+}
+
+// Bounded wait on an mbarrier phase. Returns false on timeout (or when the CTA
+// is already in error), after recording the error.
+__device__ __forceinline__ bool PipeWait(uint64_t* bar, uint32_t parity,
+                                      volatile int* s_err, uint32_t* g_err) {
+  if (MbarTryWait(bar, parity)) return true;
+  const uint64_t t0 = GlobalTimerNs();
+  for (uint32_t n = 1;; ++n) {
+    if (*s_err) return false;
+    if (MbarTryWait(bar, parity)) return true;
+    if ((n & 63u) == 0 && GlobalTimerNs() - t0 > kWaitBudgetNs) {
+      *s_err = 1;
+      atomicExch(g_err, 1u);
+      return false;
+    }
+  }
+}
+
+template <int NCORR>
+__device__ __forceinline__ void LoadVisShared(const char* base, uint32_t idx,
+                                              float2 (&v)[NCORR]) {
+  if constexpr (NCORR == 2) {
+    const float4 x = reinterpret_cast<const float4*>(base)[idx];
+    v[0] = make_float2(x.x, x.y);
+    v[1] = make_float2(x.z, x.w);
+  } else {
+    const float4 x = reinterpret_cast<const float4*>(base)[2 * idx];
+    const float4 y = reinterpret_cast<const float4*>(base)[2 * idx + 1];
+    v[0] = make_float2(x.x, x.y);
+    v[1] = make_float2(x.z, x.w);
+    v[2] = make_float2(y.x, y.y);
+    v[3] = make_float2(y.z, y.w);
+  }
+}
+
+// Writes the FP32 gain-table entries of solution (cb, ant, s): one entry per
+// gain table of that channel block whose slab uses sub-solution s.
+template <int NPOL>
+__device__ __forceinline__ void WriteTables(const PipeParams& p, uint32_t cb,
+                                            uint32_t ant, uint32_t s,
+                                            const double2 (&v)[NPOL]) {
+  const uint32_t k0 = p.tab_off[cb * p.n_sub + s];
+  const uint32_t k1 = p.tab_off[cb * p.n_sub + s + 1];
+  for (uint32_t k = k0; k < k1; ++k) {
+    const uint32_t e = p.tab_ent[k];
+    float2* t = p.tables + size_t(e >> 8) * p.table_f2 + size_t(ant) * p.gain_stride +
+                (e & 255u) * NPOL;
+#pragma unroll
+    for (int q = 0; q < NPOL; ++q) t[q] = make_float2(float(v[q].x), float(v[q].y));
+  }
+}
+
+// Grid-wide finalisation of pipe_kernel, after the grid barrier: the
+// consumer threads of all CTAs take (channel block, antenna, sub-solution)
+// items in a grid-stride loop: fixed-order compensated merge of the item's
+// partial slots, FP64 add-back and division (IterativeDiagonalSolver.cc:206-221,
+// IterativeScalarSolver.cc:184-194), SolverBase::Step (SolverBase.cc:88-158),
+// the AssignSolutions norm (SolverBase.cc:234-285), and the FP32 gain tables
+// of the next iteration. The last CTA to finish sums the per-CTA norms in CTA
+// order, runs ReachedStoppingCriterion / DetectStall (SolverBase.h:274-285,
+// SolverBase.cc:63-86), and prepares the next iteration's
+// MakeSolutionsFinite{1,2}Pol (SolverBase.cc:316-371) for channel blocks that
+// got non-finite solutions.
+template <int NPOL>
+__device__ __noinline__ void FinalizeDistributed(const PipeParams& p, int ctid,
+                                                 double* s_sum, uint32_t* s_cnt,
+                                                 uint32_t* s_last) {
+  const DevSettings st = *p.settings;
+  const uint32_t n_items_cb = p.n_ant * p.n_sub;
+  const uint32_t n_items = p.n_cb * n_items_cb;
+  double nsum = 0.0;
+  uint32_t ncnt = 0;
+  for (uint32_t item = blockIdx.x * kPipeRuns + ctid; item < n_items;
+       item += gridDim.x * kPipeRuns) {
+    const uint32_t cb = item / n_items_cb;
+    const uint32_t it = item - cb * n_items_cb;
+    const uint32_t ant = it / p.n_sub;
+    const uint32_t s = it - ant * p.n_sub;
+    const uint32_t d = p.dir_of_sub[s];
+    NeumaierSum nr[NPOL], ni[NPOL], dn[NPOL];
+    const uint32_t j0 = p.fin_off[cb * p.n_sub + s];
+    const uint32_t j1 = p.fin_off[cb * p.n_sub + s + 1];
+    const size_t off = size_t(ant) * p.acc_stride + d * NPOL * 3;
+    uint32_t j = j0;
+    for (; j + 4 <= j1; j += 4) {  // four slots in flight
+      float v[4][NPOL * 3];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const float* a = p.partials + size_t(p.fin_visits[j + u]) * p.acc_floats + off;
+#pragma unroll
+        for (int e = 0; e < NPOL * 3; ++e) v[u][e] = __ldcg(a + e);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int q = 0; q < NPOL; ++q) {
+          nr[q].Add(v[u][q * 3 + 0]);
+          ni[q].Add(v[u][q * 3 + 1]);
+          dn[q].Add(v[u][q * 3 + 2]);
+        }
+    }
+    for (; j < j1; ++j) {
+      const float* a = p.partials + size_t(p.fin_visits[j]) * p.acc_floats + off;
+#pragma unroll
+      for (int q = 0; q < NPOL; ++q) {
+        nr[q].Add(__ldcg(a + q * 3 + 0));
+        ni[q].Add(__ldcg(a + q * 3 + 1));
+        dn[q].Add(__ldcg(a + q * 3 + 2));
+      }
+    }
+    double2* sol = p.solutions + size_t(item) * NPOL;
+    double2 old[NPOL], nxt[NPOL];
+    bool pair_ok = true;
+#pragma unroll
+    for (int q = 0; q < NPOL; ++q) {
+      old[q] = sol[q];
+      pair_ok = pair_ok && dfinite(old[q]);
+    }
+    if (!pair_ok && p.cb_flag[cb]) {
+      const double rv = p.cb_avg[cb];
+#pragma unroll
+      for (int q = 0; q < NPOL; ++q) old[q] = make_double2(rv, 0.0);
+    }
+#pragma unroll
+    for (int q = 0; q < NPOL; ++q) {
+      const float den = dn[q].Value();
+      if (den == 0.f) {
+        nxt[q] = make_double2(nan(""), 0.0);
+      } else {
+        nxt[q] = make_double2(
+            double(float(old[q].x)) + double(nr[q].Value()) / double(den),
+            double(float(old[q].y)) + double(ni[q].Value()) / double(den));
+      }
+    }
+    if (p.host_mode) {
+      double2* out = p.next_out + size_t(item) * NPOL;
+#pragma unroll
+      for (int q = 0; q < NPOL; ++q) out[q] = nxt[q];
+      continue;
+    }
+#pragma unroll
+    for (int q = 0; q < NPOL; ++q) {
+      if (!st.phase_only) {
+        nxt[q] = make_double2(old[q].x * (1.0 - st.step_size) + nxt[q].x * st.step_size,
+                              old[q].y * (1.0 - st.step_size) + nxt[q].y * st.step_size);
+      } else {
+        const double from = atan2(old[q].y, old[q].x);
+        double dist = atan2(nxt[q].y, nxt[q].x) - from;
+        if (dist > M_PI)
+          dist -= 2.0 * M_PI;
+        else if (dist < -M_PI)
+          dist += 2.0 * M_PI;
+        double sn, cs;
+        sincos(from + st.step_size * dist, &sn, &cs);
+        nxt[q] = make_double2(cs, sn);
+      }
+    }
+    if (NPOL == 1) {
+      if (old[0].x != 0.0 || old[0].y != 0.0) {
+        const double2 diff = dmul(
+            make_double2(nxt[0].x - old[0].x, nxt[0].y - old[0].y), dinv(old[0]));
+        const double a = hypot(diff.x, diff.y);
+        if (isfinite(a)) {
+          nsum += a;
+          ncnt += 1;
+        }
+      }
+    } else {
+      const double2 inv0 = dinv(old[0]);
+      const double2 inv1 = dinv(old[NPOL - 1]);
+      if (dfinite(inv0) && dfinite(inv1)) {
+        const double2 d0 =
+            dmul(make_double2(nxt[0].x - old[0].x, nxt[0].y - old[0].y), inv0);
+        const double2 d1 = dmul(make_double2(nxt[NPOL - 1].x - old[NPOL - 1].x,
+                                             nxt[NPOL - 1].y - old[NPOL - 1].y),
+                                inv1);
+        const double sumabs = hypot(d0.x, d0.y) + hypot(d1.x, d1.y);
+        if (isfinite(sumabs)) {
+          nsum += sumabs;
+          ncnt += 2;
+        }
+      }
+    }
+    bool all_finite = true;
+#pragma unroll
+    for (int q = 0; q < NPOL; ++q) {
+      sol[q] = nxt[q];
+      all_finite = all_finite && dfinite(nxt[q]);
+    }
+    WriteTables<NPOL>(p, cb, ant, s, nxt);
+    if (!all_finite) p.cb_newflag[cb] = 1u;
+  }
+  // Per-CTA norm partial, then the last CTA finishes the iteration.
+  s_sum[ctid] = nsum;
+  s_cnt[ctid] = ncnt;
+  ConsumerBarrier();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (ctid < w && ctid + w < kPipeRuns) {
+      s_sum[ctid] += s_sum[ctid + w];
+      s_cnt[ctid] += s_cnt[ctid + w];
+    }
+    ConsumerBarrier();
+  }
+  if (ctid == 0) {
+    p.block_sum[blockIdx.x] = s_sum[0];
+    p.block_cnt[blockIdx.x] = s_cnt[0];
+    __threadfence();
+    const uint32_t prev = atomicAdd(&p.counters[0], 1u);
+    *s_last = (prev == gridDim.x - 1) ? 1u : 0u;
+  }
+  ConsumerBarrier();
+  if (!*s_last) return;
+  __threadfence();
+  if (!p.host_mode) {
+    // Replacement values for channel blocks with new non-finite solutions:
+    // mean |pol 0| over finite pairs; the gain tables take the replacement
+    // now, the solutions when the next finalisation reads them.
+    for (uint32_t cb = 0; cb < p.n_cb; ++cb) {
+      const bool bad = reinterpret_cast<volatile uint32_t*>(p.cb_newflag)[cb] != 0;
+      if (!bad) {
+        if (ctid == 0) p.cb_flag[cb] = 0u;
+        continue;
+      }
+      double asum = 0.0;
+      uint32_t acnt = 0;
+      for (uint32_t it = ctid; it < n_items_cb; it += kPipeRuns) {
+        const double2* sol = p.solutions + (size_t(cb) * n_items_cb + it) * NPOL;
+        bool ok = true;
+        double2 v[NPOL];
+#pragma unroll
+        for (int q = 0; q < NPOL; ++q) {
+          v[q] = __ldcg(sol + q);
+          ok = ok && dfinite(v[q]);
+        }
+        if (ok) {
+          asum += hypot(v[0].x, v[0].y);
+          ++acnt;
+        }
+      }
+      s_sum[ctid] = asum;
+      s_cnt[ctid] = acnt;
+      ConsumerBarrier();
+      for (int w = 128; w > 0; w >>= 1) {
+        if (ctid < w && ctid + w < kPipeRuns) {
+          s_sum[ctid] += s_sum[ctid + w];
+          s_cnt[ctid] += s_cnt[ctid + w];
+        }
+        ConsumerBarrier();
+      }
+      const double avg = s_cnt[0] == 0 ? 1.0 : s_sum[0] / double(s_cnt[0]);
+      for (uint32_t it = ctid; it < n_items_cb; it += kPipeRuns) {
+        const double2* sol = p.solutions + (size_t(cb) * n_items_cb + it) * NPOL;
+        bool ok = true;
+#pragma unroll
+        for (int q = 0; q < NPOL; ++q) ok = ok && dfinite(__ldcg(sol + q));
+        if (!ok) {
+          double2 r[NPOL];
+#pragma unroll
+          for (int q = 0; q < NPOL; ++q) r[q] = make_double2(avg, 0.0);
+          WriteTables<NPOL>(p, cb, it / p.n_sub, it % p.n_sub, r);
+        }
+      }
+      ConsumerBarrier();
+      if (ctid == 0) {
+        p.cb_avg[cb] = avg;
+        p.cb_flag[cb] = 1u;
+        p.cb_newflag[cb] = 0u;
+      }
+      ConsumerBarrier();
+    }
+  }
+  if (ctid != 0) return;
+  double sum = 0.0;
+  uint64_t cnt = 0;
+  for (uint32_t b = 0; b < gridDim.x; ++b) {
+    sum += reinterpret_cast<volatile double*>(p.block_sum)[b];
+    cnt += reinterpret_cast<volatile uint32_t*>(p.block_cnt)[b];
+  }
+  p.counters[0] = 0;
+  p.counters[2] = 0;
+  if (p.host_mode) return;
+  LoopState& ls = *p.state;
+  const double mag = cnt == 0 ? 0.0 : sum / st.step_size / double(cnt);
+  const uint32_t itn = ls.iteration + 1;
+  ls.iteration = itn;
+  if (itn <= st.hard_cap) p.step_magnitudes[itn - 1] = mag;
+  const bool converged = mag <= st.accuracy;
+  bool stalled = false;
+  if (st.detect_stalling) {
+    if (itn == 1) {
+      ls.n_var_count = 1;
+      ls.step_mean = mag;
+      ls.step_var = 0.0;
+    } else {
+      ls.n_var_count += 1;
+      const double delta_1 = mag - ls.step_mean;
+      ls.step_mean += delta_1 / double(ls.n_var_count);
+      const double delta_2 = mag - ls.step_mean;
+      ls.step_var += delta_1 * delta_2;
+    }
+    if (itn >= 30)
+      stalled = ls.step_mean <
+                st.step_diff_sigma * sqrt(ls.step_var / double(ls.n_var_count));
+  }
+  const bool ready = itn >= st.max_iterations || converged || stalled;
+  const bool error = p.counters[1] != 0;
+  const bool stop =
+      (itn >= st.min_iterations && ready) || itn >= st.hard_cap || error;
+  ls.has_converged = converged;
+  ls.has_stalled = stalled;
+  ls.done = stop;
+  if (p.use_handle) cudaGraphSetConditional(p.handle, stop ? 0u : 1u);
+}
+
+// Builds the FP32 gain tables from the FP64 solutions: one thread per
+// (table, antenna, direction). tab_cb / tab_sol give each table's channel
+// block and per-direction sub-solution.
+template <int NPOL>
+__global__ void build_tables_kernel(const double2* __restrict__ solutions,
+                                    float2* __restrict__ tables,
+                                    const uint32_t* __restrict__ tab_cb,
+                                    const uint32_t* __restrict__ tab_sol,
+                                    uint32_t n_tables, uint32_t n_ant, uint32_t n_dir,
+                                    uint32_t n_sub, uint32_t gain_stride,
+                                    uint32_t table_f2) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_tables * n_ant * n_dir) return;
+  const uint32_t tab = i / (n_ant * n_dir);
+  const uint32_t rem = i - tab * n_ant * n_dir;
+  const uint32_t ant = rem / n_dir;
+  const uint32_t d = rem - ant * n_dir;
+  const uint32_t s = tab_sol[tab * n_dir + d];
+  const double2* src = solutions + (size_t(tab_cb[tab] * n_ant + ant) * n_sub + s) * NPOL;
+  float2* dst = tables + size_t(tab) * table_f2 + size_t(ant) * gain_stride + d * NPOL;
+#pragma unroll
+  for (int q = 0; q < NPOL; ++q) dst[q] = make_float2(float(src[q].x), float(src[q].y));
+}
+
+// Launched cooperatively (all CTAs co-resident), one CTA per SM.
+template <int NCORR, int NPOL, int DMAX>
+__global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams p) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* empty = full + kPipeMaxStages;
+  uint64_t* gfull = empty + kPipeMaxStages;  // gain table buffer loaded
+  uint64_t* gfree = gfull + 2;               // gain table buffer released
+  int* s_err = reinterpret_cast<int*>(gfree + 2);
+  uint32_t* s_last = reinterpret_cast<uint32_t*>(s_err + 1);
+  double* s_sum = reinterpret_cast<double*>(smem + 256);
+  uint32_t* s_cnt = reinterpret_cast<uint32_t*>(s_sum + kPipeRuns);
+  float* acc = reinterpret_cast<float*>(smem + p.off_acc);
+  float2* gtab_buf = reinterpret_cast<float2*>(smem + p.off_gtab);
+  float* stg = reinterpret_cast<float*>(smem + p.off_stg);
+  uint32_t* a_cnt = reinterpret_cast<uint32_t*>(smem + p.off_cnt);
+  uint32_t* a_off = reinterpret_cast<uint32_t*>(smem + p.off_off);
+  uint32_t* t_pair = reinterpret_cast<uint32_t*>(smem + p.off_pair);
+  uint16_t* ent = reinterpret_cast<uint16_t*>(smem + p.off_ent);
+  uint32_t* s_wsum = reinterpret_cast<uint32_t*>(smem + p.off_wsum);
+  char* stages = reinterpret_cast<char*>(smem + p.off_stages);
+  constexpr uint32_t E = NCORR * 8;  // bytes per visibility
+  const uint32_t acc_n = p.acc_floats;
+  const uint32_t n_dir = p.n_dir;
+  const uint32_t stage_bytes = (1 + n_dir) * kPipeRuns * E;
+  const uint32_t table_bytes = p.table_f2 * 8;
+  const uint32_t S = p.stages;
+
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+  if (tid == 0) {
+    for (uint32_t s = 0; s < S; ++s) {
+      MbarInit(&full[s], 1);
+      MbarInit(&empty[s], kPipeConsumerWarps);
+    }
+    for (int b = 0; b < 2; ++b) {
+      MbarInit(&gfull[b], 1);
+      MbarInit(&gfree[b], kPipeConsumerWarps);
+    }
+    *s_err = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (p.use_handle && blockIdx.x == 0) cudaGraphSetConditional(p.handle, 0);
+  }
+  __syncthreads();
+
+  const uint32_t f_begin = p.cta_frag_off[blockIdx.x];
+  const uint32_t f_end = p.cta_frag_off[blockIdx.x + 1];
+
+  if (warp == kPipeConsumerWarps) {
+    // ---------------- producer warp: one thread issues all bulk copies ----
+    if (lane != 0) return;
+    uint32_t row = 0, nvis = 0, cur_visit = 0xFFFFFFFFu;
+    bool ok = true;
+    for (uint32_t fi = f_begin; fi < f_end && ok; ++fi) {
+      const Frag f = p.frags[fi];
+      const SlabDesc sl = p.slabs[f.slab];
+      if (f.visit != cur_visit) {  // new visit: its gain table first
+        const uint32_t b = nvis & 1u;
+        if (nvis >= 2 &&
+            !PipeWait(&gfree[b], ((nvis - 2) >> 1) & 1u, s_err, &p.counters[1])) {
+          ok = false;
+          break;
+        }
+        MbarArriveExpectTx(&gfull[b], table_bytes);
+        BulkCopyG2S(gtab_buf + size_t(b) * p.table_f2,
+                    p.tables + size_t(sl.table) * p.table_f2, table_bytes, &gfull[b]);
+        cur_visit = f.visit;
+        ++nvis;
+      }
+      const size_t tlr = size_t(sl.T) * sl.L * sl.R;
+      const uint32_t seg = f.n_runs * E;
+      for (uint32_t rr = f.row_lo; rr < f.row_hi; ++rr, ++row) {
+        const uint32_t s = row % S;
+        if (row >= S &&
+            !PipeWait(&empty[s], ((row / S) & 1u) ^ 1u, s_err, &p.counters[1])) {
+          ok = false;
+          break;
+        }
+        MbarArriveExpectTx(&full[s], seg * (1 + n_dir));
+        char* dst = stages + size_t(s) * stage_bytes;
+        const size_t off = size_t(rr) * sl.R + f.r0;
+        BulkCopyG2S(dst, static_cast<const char*>(sl.data) + off * E, seg, &full[s]);
+        for (uint32_t d = 0; d < n_dir; ++d)
+          BulkCopyG2S(dst + size_t(1 + d) * kPipeRuns * E,
+                      static_cast<const char*>(sl.model) + (d * tlr + off) * E, seg,
+                      &full[s]);
+      }
+    }
+    // Wait for the last copies, so none is in flight when the CTA ends.
+    for (uint32_t k = 0; k < S && k < row; ++k) {
+      const uint32_t r = row - 1 - k;
+      PipeWait(&full[r % S], (r / S) & 1u, s_err, &p.counters[1]);
+    }
+    for (uint32_t k = 0; k < 2 && k < nvis; ++k) {
+      const uint32_t v = nvis - 1 - k;
+      PipeWait(&gfull[v & 1u], (v >> 1) & 1u, s_err, &p.counters[1]);
+    }
+    return;
+  }
+
+  // ---------------- consumer warps ----------------
+  const int ctid = tid;  // 0 .. kPipeRuns - 1
+  uint32_t row = 0, nvis = 0, cur_visit = 0xFFFFFFFFu;
+  const float2* gtab = gtab_buf;
+  auto end_visit = [&]() {
+    // all consumers are done with the visit: release its gain table buffer
+    // and flush the accumulators into the visit's partial slot
+    ConsumerBarrier();
+    __syncwarp();
+    if (lane == 0) MbarArrive(&gfree[(nvis - 1) & 1u]);
+    float* out = p.partials + size_t(cur_visit) * acc_n;
+    for (uint32_t i = ctid; i < acc_n; i += kPipeRuns) __stcg(out + i, acc[i]);
+    ConsumerBarrier();
+  };
+  for (uint32_t fi = f_begin; fi < f_end; ++fi) {
+    const Frag f = p.frags[fi];
+    const SlabDesc sl = p.slabs[f.slab];
+    if (f.visit != cur_visit) {
+      if (cur_visit != 0xFFFFFFFFu) end_visit();
+      for (uint32_t i = ctid; i < acc_n; i += kPipeRuns) acc[i] = 0.f;
+      const uint32_t b = nvis & 1u;
+      PipeWait(&gfull[b], (nvis >> 1) & 1u, s_err, &p.counters[1]);
+      gtab = gtab_buf + size_t(b) * p.table_f2;
+      cur_visit = f.visit;
+      ++nvis;
+      ConsumerBarrier();
+    }
+    const uint32_t run = f.r0 + ctid;
+    const bool active = uint32_t(ctid) < f.n_runs;
+    uint32_t a1 = 0, a2 = 0;
+    if (active) {
+      const uint32_t ap = sl.run_ant[run];
+      a1 = ap & 0xFFFFu;
+      a2 = ap >> 16;
+    }
+    float2 G[DMAX][NCORR];
+    float2 P[DMAX][NCORR];
+    float Q[DMAX][NCORR];
+#pragma unroll
+    for (int k = 0; k < DMAX; ++k) {
+      float2 ga[NPOL], gb[NPOL];
+#pragma unroll
+      for (int q = 0; q < NPOL; ++q) {
+        ga[q] = make_float2(0.f, 0.f);
+        gb[q] = make_float2(0.f, 0.f);
+        if (k < int(n_dir)) {
+          ga[q] = gtab[a1 * p.gain_stride + k * NPOL + q];
+          gb[q] = gtab[a2 * p.gain_stride + k * NPOL + q];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < NCORR; ++c) {
+        G[k][c] = cmul_conj(ga[RowPol<NCORR, NPOL>(c)], gb[ColPol<NCORR, NPOL>(c)]);
+        P[k][c] = make_float2(0.f, 0.f);
+        Q[k][c] = 0.f;
+      }
+    }
+    for (uint32_t rr = f.row_lo; rr < f.row_hi; ++rr, ++row) {
+      const uint32_t s = row % S;
+      PipeWait(&full[s], (row / S) & 1u, s_err, &p.counters[1]);
+      const char* base = stages + size_t(s) * stage_bytes;
+      float2 Rv[NCORR];
+      LoadVisShared<NCORR>(base, ctid, Rv);
+      // Residual R = D - sum_d G_d M_d (first read of the model rows) ...
+#pragma unroll
+      for (int k = 0; k < DMAX; ++k) {
+        float2 M[NCORR];
+        if (k < int(n_dir)) {
+          LoadVisShared<NCORR>(base + size_t(1 + k) * kPipeRuns * E, ctid, M);
+        } else {
+#pragma unroll
+          for (int c = 0; c < NCORR; ++c) M[c] = make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int c = 0; c < NCORR; ++c) {
+          Rv[c].x = fmaf(-G[k][c].x, M[c].x, Rv[c].x);
+          Rv[c].x = fmaf(G[k][c].y, M[c].y, Rv[c].x);
+          Rv[c].y = fmaf(-G[k][c].x, M[c].y, Rv[c].y);
+          Rv[c].y = fmaf(-G[k][c].y, M[c].x, Rv[c].y);
+        }
+      }
+      // ... then P_d += R conj(M_d), Q_d += |M_d|^2 (second read, shared).
+#pragma unroll
+      for (int k = 0; k < DMAX; ++k) {
+        float2 M[NCORR];
+        if (k < int(n_dir)) {
+          LoadVisShared<NCORR>(base + size_t(1 + k) * kPipeRuns * E, ctid, M);
+        } else {
+#pragma unroll
+          for (int c = 0; c < NCORR; ++c) M[c] = make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int c = 0; c < NCORR; ++c) {
+          P[k][c].x = fmaf(Rv[c].x, M[c].x, P[k][c].x);
+          P[k][c].x = fmaf(Rv[c].y, M[c].y, P[k][c].x);
+          P[k][c].y = fmaf(Rv[c].y, M[c].x, P[k][c].y);
+          P[k][c].y = fmaf(-Rv[c].x, M[c].y, P[k][c].y);
+          Q[k][c] = fmaf(M[c].x, M[c].x, Q[k][c]);
+          Q[k][c] = fmaf(M[c].y, M[c].y, Q[k][c]);
+        }
+      }
+      __syncwarp();
+      if (lane == 0) MbarArrive(&empty[s]);
+    }
+
+    // ---- tile reduction into the visit's antenna accumulators ----
+    ConsumerBarrier();  // the previous reduction is complete everywhere
+    if (f.flags & kFragDirect) {
+      // The tile's first antennas are distinct, and so are its second
+      // antennas: two conflict-free phases of plain shared-memory updates.
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        if (side == 1) ConsumerBarrier();
+        if (active) {
+          const uint32_t a = side == 0 ? a1 : a2;
+          const uint32_t b = side == 0 ? a2 : a1;
+#pragma unroll
+          for (int k = 0; k < DMAX; ++k) {
+            if (k < int(n_dir)) {
+              float2 gb[NPOL];
+#pragma unroll
+              for (int q = 0; q < NPOL; ++q) gb[q] = gtab[b * p.gain_stride + k * NPOL + q];
+              float* x = acc + a * p.acc_stride + k * NPOL * 3;
+#pragma unroll
+              for (int q = 0; q < NPOL; ++q) {
+                float2 n = make_float2(0.f, 0.f);
+                float dd = 0.f;
+#pragma unroll
+                for (int c = 0; c < NCORR; ++c) {
+                  const int rp = RowPol<NCORR, NPOL>(c);
+                  const int cp = ColPol<NCORR, NPOL>(c);
+                  if (side == 0 && rp == q) {  // num += g_b P, den += |g_b|^2 Q
+                    const float2 t1 = cmul(gb[cp], P[k][c]);
+                    n.x += t1.x;
+                    n.y += t1.y;
+                    dd += cnorm(gb[cp]) * Q[k][c];
+                  }
+                  if (side == 1 && cp == q) {  // num += g_a conj(P), den += |g_a|^2 Q
+                    const float2 t2 = cmul(gb[rp], cconj(P[k][c]));
+                    n.x += t2.x;
+                    n.y += t2.y;
+                    dd += cnorm(gb[rp]) * Q[k][c];
+                  }
+                }
+                x[q * 3 + 0] += n.x;
+                x[q * 3 + 1] += n.y;
+                x[q * 3 + 2] += dd;
+              }
+            }
+          }
+        }
+      }
+      continue;
+    }
+    // Sorted reduction: stage the run's P/Q, counting-sort the (run, side)
+    // pairs by antenna, then (antenna, direction group) owner threads add
+    // them up; each accumulator entry has exactly one writer.
+    constexpr uint32_t NVPD = 3 * NCORR;  // staged values per direction
+#pragma unroll
+    for (int k = 0; k < DMAX; ++k) {
+      if (k < int(n_dir)) {
+#pragma unroll
+        for (int c = 0; c < NCORR; ++c) {
+          float* v = stg + ((k * NCORR + c) * 3) * kPipeRuns + ctid;
+          v[0] = P[k][c].x;
+          v[kPipeRuns] = P[k][c].y;
+          v[2 * kPipeRuns] = Q[k][c];
+        }
+      }
+    }
+    (void)NVPD;
+    t_pair[ctid] = active ? (a1 | (a2 << 16)) : 0xFFFFFFFFu;
+    for (uint32_t i = ctid; i < p.n_ant; i += kPipeRuns) a_cnt[i] = 0;
+    ConsumerBarrier();
+    uint32_t rank1 = 0, rank2 = 0;
+    if (active) {
+      rank1 = atomicAdd(&a_cnt[a1], 1u);
+      rank2 = atomicAdd(&a_cnt[a2], 1u);
+    }
+    ConsumerBarrier();
+    {
+      const uint32_t chunk = (p.n_ant + kPipeRuns - 1) / kPipeRuns;
+      const uint32_t lo = min(p.n_ant, ctid * chunk);
+      const uint32_t hi = min(p.n_ant, lo + chunk);
+      uint32_t local = 0;
+      for (uint32_t i = lo; i < hi; ++i) local += a_cnt[i];
+      uint32_t x = local;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+      }
+      if (lane == 31) s_wsum[warp] = x;
+      ConsumerBarrier();
+      uint32_t base = 0;
+      for (int w = 0; w < warp; ++w) base += s_wsum[w];
+      uint32_t run_off = base + x - local;
+      for (uint32_t i = lo; i < hi; ++i) {
+        a_off[i] = run_off;
+        run_off += a_cnt[i];
+      }
+    }
+    ConsumerBarrier();
+    if (active) {
+      ent[a_off[a1] + rank1] = uint16_t(ctid << 1);
+      ent[a_off[a2] + rank2] = uint16_t((ctid << 1) | 1);
+    }
+    ConsumerBarrier();
+    const uint32_t n_groups = p.owner_groups;
+    for (uint32_t task = ctid; task < p.n_ant * n_groups; task += kPipeRuns) {
+      const uint32_t a = task / n_groups;
+      const uint32_t grp = task - a * n_groups;
+      const uint32_t e0 = a_off[a], e1 = e0 + a_cnt[a];
+      for (uint32_t e = e0; e < e1; ++e) {
+        const uint32_t en = ent[e];
+        const uint32_t j = en >> 1;
+        const bool second = (en & 1u) != 0;  // antenna a is antenna 2 of run j
+        const uint32_t pr = t_pair[j];
+        const uint32_t b = second ? (pr & 0xFFFFu) : (pr >> 16);
+        for (uint32_t k = grp; k < n_dir; k += n_groups) {
+          float2 gb[NPOL];
+#pragma unroll
+          for (int q = 0; q < NPOL; ++q) gb[q] = gtab[b * p.gain_stride + k * NPOL + q];
+          float2 Pc[NCORR];
+          float Qc[NCORR];
+#pragma unroll
+          for (int c = 0; c < NCORR; ++c) {
+            const float* v = stg + ((k * NCORR + c) * 3) * kPipeRuns + j;
+            Pc[c] = make_float2(v[0], v[kPipeRuns]);
+            Qc[c] = v[2 * kPipeRuns];
+          }
+          float* x = acc + a * p.acc_stride + k * NPOL * 3;
+#pragma unroll
+          for (int q = 0; q < NPOL; ++q) {
+            float2 n = make_float2(0.f, 0.f);
+            float dd = 0.f;
+#pragma unroll
+            for (int c = 0; c < NCORR; ++c) {
+              const int rp = RowPol<NCORR, NPOL>(c);
+              const int cp = ColPol<NCORR, NPOL>(c);
+              if (!second && rp == q) {
+                const float2 t1 = cmul(gb[cp], Pc[c]);
+                n.x += t1.x;
+                n.y += t1.y;
+                dd += cnorm(gb[cp]) * Qc[c];
+              }
+              if (second && cp == q) {
+                const float2 t2 = cmul(gb[rp], cconj(Pc[c]));
+                n.x += t2.x;
+                n.y += t2.y;
+                dd += cnorm(gb[rp]) * Qc[c];
+              }
+            }
+            x[q * 3 + 0] += n.x;
+            x[q * 3 + 1] += n.y;
+            x[q * 3 + 2] += dd;
+          }
+        }
+      }
+    }
+  }
+  if (cur_visit != 0xFFFFFFFFu) end_visit();
+  // Grid barrier: every CTA has flushed every partial slot (the launch is
+  // cooperative, so all CTAs are resident). Bounded: a timeout flags an error
+  // and the finalisation goes ahead on whatever is there.
+  __threadfence();
+  ConsumerBarrier();
+  if (ctid == 0) {
+    atomicAdd(&p.counters[2], 1u);
+    volatile uint32_t* arrived = &p.counters[2];
+    if (*arrived < gridDim.x) {
+      const uint64_t t0 = GlobalTimerNs();
+      for (uint32_t n = 1; *arrived < gridDim.x; ++n) {
+        if ((n & 63u) == 0 && GlobalTimerNs() - t0 > kWaitBudgetNs) {
+          atomicExch(&p.counters[1], 1u);
+          break;
+        }
+      }
+    }
+    __threadfence();
+  }
+  ConsumerBarrier();
+  FinalizeDistributed<NPOL>(p, ctid, s_sum, s_cnt, s_last);
+}
+
+// ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
 thread_local std::string g_last_error = "no error";
@@ -808,6 +1666,16 @@ struct ddsolve_ctx {
   uint32_t ng = 1, dmax = 1;
   StreamFn stream_fn = nullptr;
   size_t stream_smem = 0;
+  // pipelined path (pipe_kernel): chosen when eligible
+  bool use_pipe = false;
+  const void* pipe_fn = nullptr;
+  size_t pipe_smem = 0;
+  uint32_t pipe_stages = 0, acc_stride = 0, gain_stride = 0;
+  DevBuf d_cb_done /* new non-finite flags */, d_cb_flag, d_cb_avg, d_counters;
+  DevBuf d_frags, d_cta_frag_off, d_tables, d_tab_cb, d_tab_sol, d_tab_off, d_tab_ent;
+  uint32_t n_tables = 0, table_f2 = 0, owner_groups = 1;
+  uint32_t off_acc = 0, off_gtab = 0, off_stg = 0, off_cnt = 0, off_off = 0,
+           off_pair = 0, off_ent = 0, off_wsum = 0, off_stages = 0;
   uint32_t n_ctas = 0, n_visits = 0, fin_blocks = 0;
   DevBuf d_slabs, d_visits, d_cta_off, d_slab_sol, d_partials, d_fin_off,
       d_fin_visits, d_dir_of_sub, d_block_sum, d_block_cnt;
@@ -874,6 +1742,52 @@ const KernelEntry* FindKernel(int ncorr, int npol, int need) {
   return best;
 }
 
+// Registry of pipelined-kernel instantiations keyed by (ncorr, npol, dmax).
+template <int NC, int NP, int DM>
+constexpr KernelEntry PipeEntry() {
+  return KernelEntry{NC, NP, DM,
+                     reinterpret_cast<const void*>(&pipe_kernel<NC, NP, DM>)};
+}
+
+const std::vector<KernelEntry>& PipeKernels() {
+  static const std::vector<KernelEntry> k = {
+      PipeEntry<2, 2, 2>(), PipeEntry<2, 2, 4>(), PipeEntry<2, 2, 6>(),
+      PipeEntry<2, 2, 8>(), PipeEntry<2, 2, 10>(), PipeEntry<2, 2, 12>(),
+      PipeEntry<2, 1, 2>(), PipeEntry<2, 1, 4>(), PipeEntry<2, 1, 6>(),
+      PipeEntry<2, 1, 8>(), PipeEntry<2, 1, 10>(), PipeEntry<2, 1, 12>(),
+      PipeEntry<4, 2, 2>(), PipeEntry<4, 2, 4>(),
+      PipeEntry<4, 1, 2>(), PipeEntry<4, 1, 4>(),
+  };
+  return k;
+}
+
+const KernelEntry* FindPipeKernel(int ncorr, int npol, int n_dir) {
+  const KernelEntry* best = nullptr;
+  for (const KernelEntry& e : PipeKernels())
+    if (e.ncorr == ncorr && e.npol == npol && e.dmax >= n_dir &&
+        (!best || e.dmax < best->dmax))
+      best = &e;
+  return best;
+}
+
+uint32_t OddAtLeast(uint32_t x) { return x | 1u; }
+
+// Shared memory of pipe_kernel for `stages` stages, with the scratch of the
+// sorted tile reduction (the layout is fixed in BuildPipePlan).
+size_t PipeSmemBytes(const ddsolve_ctx* ctx, uint32_t stages, uint32_t acc_stride,
+                     uint32_t gain_stride) {
+  auto align = [](size_t x, size_t a) { return (x + a - 1) / a * a; };
+  const size_t n_ant4 = align(ctx->n_ant, 4);
+  const size_t table_f2 = (size_t(ctx->n_ant) * gain_stride + 1) & ~size_t(1);
+  size_t off = align(256 + size_t(kPipeRuns) * 12, 16);
+  off += align(size_t(ctx->n_ant) * acc_stride * 4, 16);
+  off += 2 * table_f2 * 8;
+  off += size_t(3) * ctx->n_corr * ctx->n_dir * kPipeRuns * 4 + 2 * n_ant4 * 4 +
+         size_t(kPipeRuns) * 4 + size_t(kPipeRuns) * 4 + 128;
+  off = align(off, 128);
+  return off + size_t(stages) * (1 + ctx->n_dir) * kPipeRuns * ctx->elem_bytes;
+}
+
 int PreferredDirsPerLane(int ncorr) { return ncorr == 4 ? 2 : (ncorr == 2 ? 5 : 8); }
 
 size_t ElemBytes(uint32_t ncorr) { return size_t(ncorr) * 8; }
@@ -937,21 +1851,22 @@ int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const float* data,
     if (tlr == 0) continue;
     const uint32_t blocks =
         uint32_t(std::min<uint64_t>((tlr + 255) / 256, uint64_t(ctx->n_sm) * 8));
+    const float2* src_d = reinterpret_cast<const float2*>(st);
+    const float2* src_m = reinterpret_cast<const float2*>(st + size_t(cb.n_vis) * E);
+    float2* dst_d = cb.data.as<float2>();
+    float2* dst_m = cb.model.as<float2>();
     if (E == 8)
-      pack_kernel<8><<<blocks, 256, 0, ctx->stream>>>(
+      pack_kernel<1><<<blocks, 256, 0, ctx->stream>>>(
           ctx->pack_desc.as<PackSlab>(), uint32_t(i), ctx->run_src_dev.as<uint32_t>(),
-          ctx->run_len_dev.as<uint32_t>(), st, st + size_t(cb.n_vis) * E, cb.n_vis,
-          ctx->n_dir, cb.n_elems, cb.data.as<char>(), cb.model.as<char>());
+          ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir, dst_d, dst_m);
     else if (E == 16)
-      pack_kernel<16><<<blocks, 256, 0, ctx->stream>>>(
+      pack_kernel<2><<<blocks, 256, 0, ctx->stream>>>(
           ctx->pack_desc.as<PackSlab>(), uint32_t(i), ctx->run_src_dev.as<uint32_t>(),
-          ctx->run_len_dev.as<uint32_t>(), st, st + size_t(cb.n_vis) * E, cb.n_vis,
-          ctx->n_dir, cb.n_elems, cb.data.as<char>(), cb.model.as<char>());
+          ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir, dst_d, dst_m);
     else
-      pack_kernel<32><<<blocks, 256, 0, ctx->stream>>>(
+      pack_kernel<4><<<blocks, 256, 0, ctx->stream>>>(
           ctx->pack_desc.as<PackSlab>(), uint32_t(i), ctx->run_src_dev.as<uint32_t>(),
-          ctx->run_len_dev.as<uint32_t>(), st, st + size_t(cb.n_vis) * E, cb.n_vis,
-          ctx->n_dir, cb.n_elems, cb.data.as<char>(), cb.model.as<char>());
+          ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir, dst_d, dst_m);
     DDS_CHECK_CUDA(ctx, cudaGetLastError());
   }
   // The staging and run arrays are reused by the next upload: keep the
@@ -968,6 +1883,219 @@ int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const float* data,
   return DDSOLVE_OK;
 }
 
+// Plan of the pipelined path: tiles of up to kPipeRuns runs (flagged direct
+// when their first antennas are distinct and their second antennas are
+// distinct), split along their (time, channel) rows into fragments so that
+// every CTA streams the same weight of rows; visits (one partial slot each);
+// gain tables (one per channel block and solution-index vector) with the
+// lists the finalisation uses to refresh them; shared-memory layout.
+int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
+                  const std::vector<uint32_t>& slab_sol, int max_optin) {
+  const uint32_t n_dir = ctx->n_dir, n_ant = ctx->n_ant, n_pol = ctx->n_pol;
+  // ---- gain tables ----
+  std::map<std::vector<uint32_t>, uint32_t> table_ids;
+  std::vector<uint32_t> tab_cb, tab_sol;
+  for (SlabDesc& sd : descs) {
+    std::vector<uint32_t> key(1 + n_dir);
+    key[0] = sd.cb;
+    for (uint32_t d = 0; d < n_dir; ++d) key[1 + d] = slab_sol[sd.sol_off + d];
+    auto it = table_ids.find(key);
+    if (it == table_ids.end()) {
+      it = table_ids.emplace(key, uint32_t(tab_cb.size())).first;
+      tab_cb.push_back(sd.cb);
+      tab_sol.insert(tab_sol.end(), key.begin() + 1, key.end());
+    }
+    sd.table = it->second;
+  }
+  const uint32_t n_tables = uint32_t(tab_cb.size());
+  std::vector<std::vector<uint32_t>> tlists(size_t(ctx->n_cb) * ctx->n_sub);
+  for (uint32_t t = 0; t < n_tables; ++t)
+    for (uint32_t d = 0; d < n_dir; ++d)
+      tlists[size_t(tab_cb[t]) * ctx->n_sub + tab_sol[t * n_dir + d]].push_back((t << 8) | d);
+  std::vector<uint32_t> tab_off(tlists.size() + 1, 0), tab_ent;
+  for (size_t i = 0; i < tlists.size(); ++i) {
+    tab_off[i] = uint32_t(tab_ent.size());
+    tab_ent.insert(tab_ent.end(), tlists[i].begin(), tlists[i].end());
+  }
+  tab_off[tlists.size()] = uint32_t(tab_ent.size());
+  const uint32_t table_f2 = (n_ant * ctx->gain_stride + 1u) & ~1u;
+
+  // ---- tiles ----
+  struct Tile {
+    uint32_t slab, r0, n, rows, direct;
+  };
+  std::vector<Tile> tiles;
+  std::vector<uint32_t> stamp1(n_ant, 0xFFFFFFFFu), stamp2(n_ant, 0xFFFFFFFFu);
+  uint32_t tile_id = 0;
+  bool any_sorted = false;
+  for (uint32_t gi = 0; gi < descs.size(); ++gi) {
+    const SlabDesc& sd = descs[gi];
+    const ChannelBlockStore& cbs = ctx->cbs[sd.cb];
+    const uint32_t run_off = uint32_t(sd.run_ant - cbs.run_ant_dev.as<uint32_t>());
+    for (uint32_t r0 = 0; r0 < sd.R; r0 += kPipeRuns, ++tile_id) {
+      const uint32_t n = std::min<uint32_t>(kPipeRuns, sd.R - r0);
+      bool direct = true;
+      for (uint32_t r = r0; r < r0 + n && direct; ++r) {
+        const uint32_t ap = cbs.run_ant[run_off + r];
+        const uint32_t a1 = ap & 0xFFFFu, a2 = ap >> 16;
+        if (stamp1[a1] == tile_id || stamp2[a2] == tile_id) direct = false;
+        stamp1[a1] = tile_id;
+        stamp2[a2] = tile_id;
+      }
+      any_sorted = any_sorted || !direct;
+      tiles.push_back({gi, r0, n, sd.T * sd.L, direct ? 1u : 0u});
+    }
+  }
+  // ---- fragments: rows balanced over the CTAs ----
+  uint64_t total_rows = 0;
+  double total_w = 0.0;
+  for (const Tile& t : tiles) {
+    total_rows += t.rows;
+    total_w += double(t.rows) * double(t.n + 32);
+  }
+  const uint32_t max_ctas = uint32_t(ctx->n_sm);
+  const uint32_t n_ctas = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(max_ctas, total_rows)));
+  std::vector<Frag> frags;
+  std::vector<uint32_t> cta_off(n_ctas + 1, 0);
+  {
+    double cum = 0.0;
+    uint32_t cur_cta = 0;
+    for (const Tile& t : tiles) {
+      const double w = double(t.n + 32);
+      uint32_t lo = 0;
+      while (lo < t.rows) {
+        // last row of this tile that stays on cur_cta
+        uint32_t hi = lo;
+        while (hi < t.rows) {
+          const double mid = cum + (double(hi - lo) + 0.5) * w;
+          uint32_t c = uint32_t(mid * n_ctas / total_w);
+          if (c >= n_ctas) c = n_ctas - 1;
+          if (c != cur_cta) break;
+          ++hi;
+        }
+        if (hi > lo) {
+          frags.push_back({t.slab, t.r0, t.n, t.direct, lo, hi, 0, 0});
+          cum += double(hi - lo) * w;
+          lo = hi;
+        }
+        if (lo < t.rows) {
+          ++cur_cta;
+          cta_off[cur_cta] = uint32_t(frags.size());
+        }
+      }
+    }
+    for (uint32_t c = cur_cta + 1; c <= n_ctas; ++c) cta_off[c] = uint32_t(frags.size());
+    for (uint32_t c = 1; c <= n_ctas; ++c) cta_off[c] = std::max(cta_off[c], cta_off[c - 1]);
+    cta_off[n_ctas] = uint32_t(frags.size());
+  }
+  // ---- visits ----
+  uint32_t n_visits = 0;
+  std::vector<uint32_t> visit_slab;
+  for (uint32_t c = 0; c < n_ctas; ++c) {
+    uint32_t prev_slab = 0xFFFFFFFFu;
+    for (uint32_t i = cta_off[c]; i < cta_off[c + 1]; ++i) {
+      if (frags[i].slab != prev_slab) {
+        prev_slab = frags[i].slab;
+        visit_slab.push_back(prev_slab);
+        ++n_visits;
+      }
+      frags[i].visit = n_visits - 1;
+    }
+  }
+  std::vector<std::vector<uint32_t>> lists(size_t(ctx->n_cb) * ctx->n_sub);
+  for (uint32_t v = 0; v < n_visits; ++v) {
+    const SlabDesc& sd = descs[visit_slab[v]];
+    for (uint32_t d = 0; d < n_dir; ++d) {
+      const uint32_t sub = slab_sol[sd.sol_off + d];
+      if (sub < ctx->n_sub) lists[size_t(sd.cb) * ctx->n_sub + sub].push_back(v);
+    }
+  }
+  std::vector<uint32_t> fin_off(lists.size() + 1, 0), fin_visits;
+  for (size_t i = 0; i < lists.size(); ++i) {
+    fin_off[i] = uint32_t(fin_visits.size());
+    fin_visits.insert(fin_visits.end(), lists[i].begin(), lists[i].end());
+  }
+  fin_off[lists.size()] = uint32_t(fin_visits.size());
+
+  // ---- shared-memory layout ----
+  auto align = [](size_t x, size_t a) { return (x + a - 1) / a * a; };
+  size_t off = 256 + size_t(kPipeRuns) * 12;
+  ctx->off_acc = uint32_t(align(off, 16));
+  off = ctx->off_acc + align(size_t(n_ant) * ctx->acc_stride * 4, 16);
+  ctx->off_gtab = uint32_t(off);
+  off += size_t(2) * table_f2 * 8;
+  const size_t n_ant4 = align(n_ant, 4);
+  ctx->off_stg = uint32_t(off);
+  if (any_sorted) off += size_t(3) * ctx->n_corr * n_dir * kPipeRuns * 4;
+  ctx->off_cnt = uint32_t(off);
+  if (any_sorted) off += n_ant4 * 4;
+  ctx->off_off = uint32_t(off);
+  if (any_sorted) off += n_ant4 * 4;
+  ctx->off_pair = uint32_t(off);
+  if (any_sorted) off += size_t(kPipeRuns) * 4;
+  ctx->off_ent = uint32_t(off);
+  if (any_sorted) off += size_t(kPipeRuns) * 2 * 2;
+  ctx->off_wsum = uint32_t(off);
+  off += 32 * 4;
+  ctx->off_stages = uint32_t(align(off, 128));
+  const size_t stage_bytes = size_t(1 + n_dir) * kPipeRuns * ctx->elem_bytes;
+  const size_t room = size_t(max_optin) > ctx->off_stages ? size_t(max_optin) - ctx->off_stages : 0;
+  const uint32_t stages = uint32_t(std::min<size_t>(kPipeMaxStages, room / stage_bytes));
+  if (stages < 2)
+    return ctx->Fail(DDSOLVE_E_UNSUPPORTED, "pipelined kernel does not fit in shared memory");
+  ctx->pipe_stages = stages;
+  ctx->pipe_smem = ctx->off_stages + stages * stage_bytes;
+  DDS_CHECK_CUDA(ctx, cudaFuncSetAttribute(ctx->pipe_fn,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           int(ctx->pipe_smem)));
+  ctx->n_ctas = n_ctas;
+  ctx->n_visits = n_visits;
+  ctx->n_tables = n_tables;
+  ctx->table_f2 = table_f2;
+  ctx->owner_groups = std::max<uint32_t>(1u, std::min<uint32_t>(n_dir, uint32_t(kPipeRuns) / n_ant));
+  const uint32_t n_items = ctx->n_cb * ctx->n_ant * ctx->n_sub;
+  ctx->fin_blocks = (n_items + kThreads - 1) / kThreads;
+
+  auto upload = [&](DevBuf& b, const void* src, size_t bytes) -> int {
+    DDS_CHECK_CUDA(ctx, b.Reserve(bytes));
+    if (bytes)
+      DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(b.ptr, src, bytes, cudaMemcpyHostToDevice,
+                                          ctx->stream));
+    return DDSOLVE_OK;
+  };
+  int rc;
+  if ((rc = upload(ctx->d_slabs, descs.data(), descs.size() * sizeof(SlabDesc)))) return rc;
+  if ((rc = upload(ctx->d_frags, frags.data(), frags.size() * sizeof(Frag)))) return rc;
+  if ((rc = upload(ctx->d_cta_frag_off, cta_off.data(), cta_off.size() * 4))) return rc;
+  if ((rc = upload(ctx->d_slab_sol, slab_sol.data(), slab_sol.size() * 4))) return rc;
+  if ((rc = upload(ctx->d_fin_off, fin_off.data(), fin_off.size() * 4))) return rc;
+  if ((rc = upload(ctx->d_fin_visits, fin_visits.data(), fin_visits.size() * 4))) return rc;
+  if ((rc = upload(ctx->d_dir_of_sub, ctx->dir_of_sub.data(), ctx->dir_of_sub.size() * 4)))
+    return rc;
+  if ((rc = upload(ctx->d_tab_cb, tab_cb.data(), tab_cb.size() * 4))) return rc;
+  if ((rc = upload(ctx->d_tab_sol, tab_sol.data(), tab_sol.size() * 4))) return rc;
+  if ((rc = upload(ctx->d_tab_off, tab_off.data(), tab_off.size() * 4))) return rc;
+  if ((rc = upload(ctx->d_tab_ent, tab_ent.data(), tab_ent.size() * 4))) return rc;
+  DDS_CHECK_CUDA(ctx, ctx->d_tables.Reserve(size_t(n_tables) * table_f2 * 8));
+  DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_tables.ptr, 0, size_t(n_tables) * table_f2 * 8,
+                                      ctx->stream));
+  DDS_CHECK_CUDA(ctx, ctx->d_partials.Reserve(
+                          std::max<size_t>(1, size_t(n_visits) * n_ant * ctx->acc_stride) * 4));
+  DDS_CHECK_CUDA(ctx, ctx->d_block_sum.Reserve(size_t(std::max(n_ctas, ctx->fin_blocks)) * 8));
+  DDS_CHECK_CUDA(ctx, ctx->d_block_cnt.Reserve(size_t(std::max(n_ctas, ctx->fin_blocks)) * 4));
+  DDS_CHECK_CUDA(ctx, ctx->d_cb_done.Reserve(size_t(ctx->n_cb) * 4));
+  DDS_CHECK_CUDA(ctx, ctx->d_cb_flag.Reserve(size_t(ctx->n_cb) * 4));
+  DDS_CHECK_CUDA(ctx, ctx->d_cb_avg.Reserve(size_t(ctx->n_cb) * 8));
+  DDS_CHECK_CUDA(ctx, ctx->d_counters.Reserve(16));
+  DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_done.ptr, 0, size_t(ctx->n_cb) * 4, ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_flag.ptr, 0, size_t(ctx->n_cb) * 4, ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.ptr, 0, 16, ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->plan_dirty = false;
+  ctx->DestroyGraph();
+  return DDSOLVE_OK;
+}
+
 // Builds the streaming plan: kernel choice, CTA work split, partial slots and
 // the finalisation lists.
 int BuildPlan(ddsolve_ctx* ctx) {
@@ -975,48 +2103,91 @@ int BuildPlan(ddsolve_ctx* ctx) {
     if (!ctx->cbs[c].set)
       return ctx->Fail(DDSOLVE_E_STATE,
                        "channel block " + std::to_string(c) + " has no data");
-  // Kernel choice: ng lanes per run so that each lane handles at most the
-  // preferred number of directions.
-  uint32_t ng = ctx->tune_ng;
-  if (ng == 0) {
-    ng = 1;
-    while (ng < 32 && (ctx->n_dir + ng - 1) / ng >
-                          uint32_t(PreferredDirsPerLane(int(ctx->n_corr))))
-      ng <<= 1;
-  }
-  if (ng == 0 || ng > 32 || (ng & (ng - 1)))
-    return ctx->Fail(DDSOLVE_E_INVALID, "direction groups must be a power of 2 <= 32");
-  const int need = int((ctx->n_dir + ng - 1) / ng);
-  const KernelEntry* ke = FindKernel(int(ctx->n_corr), int(ctx->n_pol), need);
-  while (!ke && ng < 32) {
-    ng <<= 1;
-    ke = FindKernel(int(ctx->n_corr), int(ctx->n_pol),
-                    int((ctx->n_dir + ng - 1) / ng));
-  }
-  if (!ke)
-    return ctx->Fail(DDSOLVE_E_UNSUPPORTED, "too many directions for the kernel set");
-  ctx->ng = ng;
-  ctx->dmax = uint32_t(ke->dmax);
-  ctx->stream_fn = reinterpret_cast<StreamFn>(const_cast<void*>(ke->fn));
-
-  const size_t acc_n = size_t(ctx->n_ant) * ctx->n_dir * ctx->n_pol * 3;
-  const size_t smem = ((acc_n + 3) & ~size_t(3)) * 4 +
-                      size_t(ctx->n_ant) * ctx->n_dir * ctx->n_pol * 8;
   int max_optin = 0;
   DDS_CHECK_CUDA(ctx, cudaDeviceGetAttribute(
                           &max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
                           ctx->device));
-  if (smem > size_t(max_optin))
-    return ctx->Fail(DDSOLVE_E_UNSUPPORTED,
-                     "antenna x direction accumulators exceed shared memory");
-  DDS_CHECK_CUDA(ctx, cudaFuncSetAttribute(ke->fn,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           int(smem)));
-  int occ = 0;
-  DDS_CHECK_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                          &occ, ke->fn, kThreads, smem));
-  if (occ < 1) return ctx->Fail(DDSOLVE_E_UNSUPPORTED, "stream kernel cannot launch");
-  ctx->stream_smem = smem;
+  // Pipelined kernel when the direction count, the correlation layout and the
+  // shared memory allow it (and no lane groups were requested).
+  ctx->use_pipe = false;
+  if (ctx->tune_ng == 0 && (ctx->n_corr == 2 || ctx->n_corr == 4) &&
+      !std::getenv("DDSOLVE_NO_PIPE")) {
+    const KernelEntry* pe =
+        FindPipeKernel(int(ctx->n_corr), int(ctx->n_pol), int(ctx->n_dir));
+    const uint32_t acc_stride = OddAtLeast(ctx->n_dir * ctx->n_pol * 3);
+    const uint32_t gain_stride = OddAtLeast(ctx->n_dir * ctx->n_pol);
+    uint32_t stages = 0;
+    for (uint32_t st = kPipeMaxStages; st >= 2 && pe; --st)
+      if (PipeSmemBytes(ctx, st, acc_stride, gain_stride) <= size_t(max_optin)) {
+        stages = st;
+        break;
+      }
+    if (pe && stages >= 2) {
+      const size_t smem = PipeSmemBytes(ctx, stages, acc_stride, gain_stride);
+      DDS_CHECK_CUDA(ctx, cudaFuncSetAttribute(
+                              pe->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              int(smem)));
+      int occ = 0;
+      DDS_CHECK_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                              &occ, pe->fn, kPipeThreads, smem));
+      if (occ >= 1) {
+        ctx->use_pipe = true;
+        ctx->pipe_fn = pe->fn;
+        ctx->pipe_smem = smem;
+        ctx->pipe_stages = stages;
+        ctx->acc_stride = acc_stride;
+        ctx->gain_stride = gain_stride;
+        ctx->dmax = uint32_t(pe->dmax);
+        ctx->ng = 1;
+      }
+    }
+  }
+  int occ = 1;
+  size_t slot_floats = 0;
+  uint32_t runs_per_block = 0;
+  if (ctx->use_pipe) {
+    runs_per_block = kPipeRuns;
+    slot_floats = size_t(ctx->n_ant) * ctx->acc_stride;
+  } else {
+    // Kernel choice: ng lanes per run so that each lane handles at most the
+    // preferred number of directions.
+    uint32_t ng = ctx->tune_ng;
+    if (ng == 0) {
+      ng = 1;
+      while (ng < 32 && (ctx->n_dir + ng - 1) / ng >
+                            uint32_t(PreferredDirsPerLane(int(ctx->n_corr))))
+        ng <<= 1;
+    }
+    if (ng == 0 || ng > 32 || (ng & (ng - 1)))
+      return ctx->Fail(DDSOLVE_E_INVALID, "direction groups must be a power of 2 <= 32");
+    const int need = int((ctx->n_dir + ng - 1) / ng);
+    const KernelEntry* ke = FindKernel(int(ctx->n_corr), int(ctx->n_pol), need);
+    while (!ke && ng < 32) {
+      ng <<= 1;
+      ke = FindKernel(int(ctx->n_corr), int(ctx->n_pol),
+                      int((ctx->n_dir + ng - 1) / ng));
+    }
+    if (!ke)
+      return ctx->Fail(DDSOLVE_E_UNSUPPORTED, "too many directions for the kernel set");
+    ctx->ng = ng;
+    ctx->dmax = uint32_t(ke->dmax);
+    ctx->stream_fn = reinterpret_cast<StreamFn>(const_cast<void*>(ke->fn));
+    const size_t acc_n = size_t(ctx->n_ant) * ctx->n_dir * ctx->n_pol * 3;
+    const size_t smem = ((acc_n + 3) & ~size_t(3)) * 4 +
+                        size_t(ctx->n_ant) * ctx->n_dir * ctx->n_pol * 8;
+    if (smem > size_t(max_optin))
+      return ctx->Fail(DDSOLVE_E_UNSUPPORTED,
+                       "antenna x direction accumulators exceed shared memory");
+    DDS_CHECK_CUDA(ctx, cudaFuncSetAttribute(ke->fn,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             int(smem)));
+    DDS_CHECK_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                            &occ, ke->fn, kThreads, smem));
+    if (occ < 1) return ctx->Fail(DDSOLVE_E_UNSUPPORTED, "stream kernel cannot launch");
+    ctx->stream_smem = smem;
+    runs_per_block = kThreads / ng;
+    slot_floats = acc_n;
+  }
 
   // Global slab list and steps.
   struct GSlab {
@@ -1025,7 +2196,6 @@ int BuildPlan(ddsolve_ctx* ctx) {
   std::vector<GSlab> gslabs;
   std::vector<SlabDesc> descs;
   std::vector<uint32_t> slab_sol;
-  const uint32_t runs_per_block = kThreads / ng;
   struct Step {
     uint32_t slab, run_lo, run_hi;
     double w;
@@ -1054,6 +2224,7 @@ int BuildPlan(ddsolve_ctx* ctx) {
       }
     }
   }
+  if (ctx->use_pipe) return BuildPipePlan(ctx, descs, slab_sol, max_optin);
   const uint32_t max_ctas = uint32_t(ctx->n_sm) * uint32_t(occ);
   uint32_t n_ctas = std::max<uint32_t>(1, std::min<uint32_t>(max_ctas, uint32_t(steps.size())));
   double total_w = 0;
@@ -1132,9 +2303,20 @@ int BuildPlan(ddsolve_ctx* ctx) {
   if ((rc = upload(ctx->d_fin_visits, fin_visits.data(), fin_visits.size() * 4))) return rc;
   if ((rc = upload(ctx->d_dir_of_sub, ctx->dir_of_sub.data(), ctx->dir_of_sub.size() * 4)))
     return rc;
-  DDS_CHECK_CUDA(ctx, ctx->d_partials.Reserve(size_t(ctx->n_visits) * acc_n * 4));
-  DDS_CHECK_CUDA(ctx, ctx->d_block_sum.Reserve(size_t(ctx->fin_blocks) * 8));
-  DDS_CHECK_CUDA(ctx, ctx->d_block_cnt.Reserve(size_t(ctx->fin_blocks) * 4));
+  DDS_CHECK_CUDA(ctx, ctx->d_cb_done.Reserve(size_t(ctx->n_cb) * 4));
+  DDS_CHECK_CUDA(ctx, ctx->d_cb_flag.Reserve(size_t(ctx->n_cb) * 4));
+  DDS_CHECK_CUDA(ctx, ctx->d_cb_avg.Reserve(size_t(ctx->n_cb) * 8));
+  DDS_CHECK_CUDA(ctx, ctx->d_counters.Reserve(16));
+  DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_done.ptr, 0, size_t(ctx->n_cb) * 4,
+                                      ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_flag.ptr, 0, size_t(ctx->n_cb) * 4,
+                                      ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.ptr, 0, 16, ctx->stream));
+  DDS_CHECK_CUDA(ctx, ctx->d_partials.Reserve(
+                          std::max<size_t>(1, size_t(ctx->n_visits) * slot_floats) * 4));
+  const size_t n_block_partials = std::max<size_t>(ctx->fin_blocks, ctx->n_ctas);
+  DDS_CHECK_CUDA(ctx, ctx->d_block_sum.Reserve(n_block_partials * 8));
+  DDS_CHECK_CUDA(ctx, ctx->d_block_cnt.Reserve(n_block_partials * 4));
   // Plan arrays are small host vectors: wait so they can be released.
   DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   ctx->plan_dirty = false;
@@ -1181,20 +2363,116 @@ FinParams MakeFinParams(ddsolve_ctx* ctx, bool host_mode) {
   return f;
 }
 
-// Launches one iteration's kernels on the context stream.
+PipeParams MakePipeParams(ddsolve_ctx* ctx, bool host_mode, bool use_handle) {
+  PipeParams p;
+  p.slabs = ctx->d_slabs.as<SlabDesc>();
+  p.frags = ctx->d_frags.as<Frag>();
+  p.cta_frag_off = ctx->d_cta_frag_off.as<uint32_t>();
+  p.slab_sol = ctx->d_slab_sol.as<uint32_t>();
+  p.solutions = ctx->d_sol.as<double2>();
+  p.partials = ctx->d_partials.as<float>();
+  p.tables = ctx->d_tables.as<float2>();
+  p.table_f2 = ctx->table_f2;
+  p.tab_off = ctx->d_tab_off.as<uint32_t>();
+  p.tab_ent = ctx->d_tab_ent.as<uint32_t>();
+  p.n_ant = ctx->n_ant;
+  p.n_dir = ctx->n_dir;
+  p.n_sub = ctx->n_sub;
+  p.n_cb = ctx->n_cb;
+  p.acc_stride = ctx->acc_stride;
+  p.gain_stride = ctx->gain_stride;
+  p.stages = ctx->pipe_stages;
+  p.acc_floats = ctx->n_ant * ctx->acc_stride;
+  p.owner_groups = ctx->owner_groups;
+  p.off_acc = ctx->off_acc;
+  p.off_gtab = ctx->off_gtab;
+  p.off_stg = ctx->off_stg;
+  p.off_cnt = ctx->off_cnt;
+  p.off_off = ctx->off_off;
+  p.off_pair = ctx->off_pair;
+  p.off_ent = ctx->off_ent;
+  p.off_wsum = ctx->off_wsum;
+  p.off_stages = ctx->off_stages;
+  p.fin_off = ctx->d_fin_off.as<uint32_t>();
+  p.fin_visits = ctx->d_fin_visits.as<uint32_t>();
+  p.dir_of_sub = ctx->d_dir_of_sub.as<uint32_t>();
+  p.cb_flag = ctx->d_cb_flag.as<uint32_t>();
+  p.cb_avg = ctx->d_cb_avg.as<double>();
+  p.cb_newflag = ctx->d_cb_done.as<uint32_t>();
+  p.block_sum = ctx->d_block_sum.as<double>();
+  p.block_cnt = ctx->d_block_cnt.as<uint32_t>();
+  p.counters = ctx->d_counters.as<uint32_t>();
+  p.next_out = ctx->d_next.as<double2>();
+  p.host_mode = host_mode ? 1 : 0;
+  p.settings = ctx->d_settings.as<DevSettings>();
+  p.state = ctx->d_state.as<LoopState>();
+  p.step_magnitudes = ctx->d_mags.as<double>();
+  p.handle = ctx->handle;
+  p.use_handle = use_handle ? 1 : 0;
+  return p;
+}
+
+// Gain tables of the pipelined path from the current solutions.
+int LaunchBuildTables(ddsolve_ctx* ctx) {
+  if (!ctx->use_pipe) return DDSOLVE_OK;
+  const uint32_t n = ctx->n_tables * ctx->n_ant * ctx->n_dir;
+  if (n == 0) return DDSOLVE_OK;
+  const uint32_t blocks = (n + 255) / 256;
+  if (ctx->n_pol == 2)
+    build_tables_kernel<2><<<blocks, 256, 0, ctx->stream>>>(
+        ctx->d_sol.as<double2>(), ctx->d_tables.as<float2>(), ctx->d_tab_cb.as<uint32_t>(),
+        ctx->d_tab_sol.as<uint32_t>(), ctx->n_tables, ctx->n_ant, ctx->n_dir, ctx->n_sub,
+        ctx->gain_stride, ctx->table_f2);
+  else
+    build_tables_kernel<1><<<blocks, 256, 0, ctx->stream>>>(
+        ctx->d_sol.as<double2>(), ctx->d_tables.as<float2>(), ctx->d_tab_cb.as<uint32_t>(),
+        ctx->d_tab_sol.as<uint32_t>(), ctx->n_tables, ctx->n_ant, ctx->n_dir, ctx->n_sub,
+        ctx->gain_stride, ctx->table_f2);
+  DDS_CHECK_CUDA(ctx, cudaGetLastError());
+  return DDSOLVE_OK;
+}
+
+int LaunchMakeFinite(ddsolve_ctx* ctx, bool use_handle) {
+  const uint32_t per_cb = ctx->n_ant * ctx->n_sub * ctx->n_pol;
+  if (ctx->n_pol == 2)
+    make_finite_kernel<2><<<ctx->n_cb, kThreads, 0, ctx->stream>>>(
+        ctx->d_sol.as<double2>(), ctx->d_nonfinite.as<uint32_t>(), per_cb,
+        ctx->handle, use_handle ? 1 : 0);
+  else
+    make_finite_kernel<1><<<ctx->n_cb, kThreads, 0, ctx->stream>>>(
+        ctx->d_sol.as<double2>(), ctx->d_nonfinite.as<uint32_t>(), per_cb,
+        ctx->handle, use_handle ? 1 : 0);
+  DDS_CHECK_CUDA(ctx, cudaGetLastError());
+  return DDSOLVE_OK;
+}
+
+// Launches one iteration's kernels on the context stream: pipe_kernel alone
+// on the pipelined path (its fused finalisation repairs non-finite solutions
+// lazily, so make_finite_kernel only runs once before the loop), else
+// make_finite_kernel + stream_kernel + finalize_kernel.
 int LaunchIteration(ddsolve_ctx* ctx, bool host_mode, bool use_handle,
                     bool with_make_finite) {
-  const uint32_t per_cb = ctx->n_ant * ctx->n_sub * ctx->n_pol;
+  if (ctx->use_pipe) {
+    // Cooperative launch: pipe_kernel has a grid barrier, so all CTAs must be
+    // resident (the grid is #SM x occupancy).
+    PipeParams pp = MakePipeParams(ctx, host_mode, use_handle);
+    void* args[] = {&pp};
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ctx->n_ctas);
+    cfg.blockDim = dim3(kPipeThreads);
+    cfg.dynamicSmemBytes = ctx->pipe_smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    DDS_CHECK_CUDA(ctx, cudaLaunchKernelExC(&cfg, ctx->pipe_fn, args));
+    return DDSOLVE_OK;
+  }
   if (with_make_finite) {
-    if (ctx->n_pol == 2)
-      make_finite_kernel<2><<<ctx->n_cb, kThreads, 0, ctx->stream>>>(
-          ctx->d_sol.as<double2>(), ctx->d_nonfinite.as<uint32_t>(), per_cb,
-          ctx->handle, use_handle ? 1 : 0);
-    else
-      make_finite_kernel<1><<<ctx->n_cb, kThreads, 0, ctx->stream>>>(
-          ctx->d_sol.as<double2>(), ctx->d_nonfinite.as<uint32_t>(), per_cb,
-          ctx->handle, use_handle ? 1 : 0);
-    DDS_CHECK_CUDA(ctx, cudaGetLastError());
+    const int rc = LaunchMakeFinite(ctx, use_handle);
+    if (rc != DDSOLVE_OK) return rc;
   }
   const StreamParams sp = MakeStreamParams(ctx);
   ctx->stream_fn<<<ctx->n_ctas, kThreads, ctx->stream_smem, ctx->stream>>>(sp);
@@ -1206,6 +2484,19 @@ int LaunchIteration(ddsolve_ctx* ctx, bool host_mode, bool use_handle,
   else
     finalize_kernel<1><<<ctx->fin_blocks, kThreads, 0, ctx->stream>>>(fp);
   DDS_CHECK_CUDA(ctx, cudaGetLastError());
+  return DDSOLVE_OK;
+}
+
+int CheckDeviceError(ddsolve_ctx* ctx) {
+  if (!ctx->use_pipe) return DDSOLVE_OK;
+  uint32_t c[2] = {0, 0};
+  DDS_CHECK_CUDA(ctx, cudaMemcpy(c, ctx->d_counters.ptr, 8, cudaMemcpyDeviceToHost));
+  if (c[1] != 0) {
+    cudaMemsetAsync(ctx->d_counters.ptr, 0, 16, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    return ctx->Fail(DDSOLVE_E_TIMEOUT,
+                     "a bounded device wait of pipe_kernel timed out; results are invalid");
+  }
   return DDSOLVE_OK;
 }
 
@@ -1416,12 +2707,39 @@ int ddsolve_set_channel_block_regular(ddsolve_ctx* ctx, uint32_t cbi,
   ChannelBlockStore& cb = ctx->cbs[cbi];
   cb.n_vis = uint64_t(n_times) * n_baselines * n_channels;
   cb.slabs.clear();
+  // Runs in cyclic-diagonal order. Each baseline is oriented so that its
+  // cyclic distance delta = (a2 - a1) mod n_ant is at most n_ant / 2 (a
+  // swapped baseline is stored Hermitian-transposed by the repack, which does
+  // not change the normal equations); runs are sorted by (delta, a1). A
+  // cyclic diagonal is then a permutation (distinct first and distinct second
+  // antennas), so windows of up to n_ant consecutive runs have distinct
+  // antennas on each side: conflict-free shared-memory accumulation.
+  const uint32_t n_ant = ctx->n_ant;
+  std::vector<uint32_t> o_a1(n_baselines), o_a2(n_baselines), o_delta(n_baselines);
+  std::vector<uint8_t> o_flip(n_baselines);
+  for (uint32_t b = 0; b < n_baselines; ++b) {
+    const uint32_t a = antenna1[b], c = antenna2[b];
+    const uint32_t d = (c + n_ant - a) % n_ant;
+    bool flip = 2 * d > n_ant;
+    if (2 * d == n_ant) flip = a > c;  // half-way diagonal: first antenna < n/2
+    o_flip[b] = flip;
+    o_a1[b] = flip ? c : a;
+    o_a2[b] = flip ? a : c;
+    o_delta[b] = flip ? n_ant - d : d;
+  }
+  std::vector<uint32_t> order(n_baselines);
+  std::iota(order.begin(), order.end(), 0u);
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+    return o_delta[x] != o_delta[y] ? o_delta[x] < o_delta[y] : o_a1[x] < o_a1[y];
+  });
   cb.run_ant.resize(n_baselines);
   cb.run_src.resize(n_baselines);
-  cb.run_len.assign(n_baselines, n_channels);
-  for (uint32_t b = 0; b < n_baselines; ++b) {
-    cb.run_ant[b] = antenna1[b] | (antenna2[b] << 16);
-    cb.run_src[b] = b * n_channels;
+  cb.run_len.resize(n_baselines);
+  for (uint32_t r = 0; r < n_baselines; ++r) {
+    const uint32_t b = order[r];
+    cb.run_ant[r] = o_a1[b] | (o_a2[b] << 16);
+    cb.run_src[r] = b * n_channels;
+    cb.run_len[r] = n_channels | (o_flip[b] ? kRunFlipped : 0u);
   }
   // Solution index per (direction, time), SolveData.cc:102-105,124-125,167.
   std::vector<uint32_t> nsol(ctx->n_dir), start(ctx->n_dir);
@@ -1434,7 +2752,18 @@ int ddsolve_set_channel_block_regular(ddsolve_ctx* ctx, uint32_t cbi,
   auto sol_of = [&](uint32_t d, uint32_t t) {
     return uint32_t(uint64_t(t) * nsol[d] / n_times) + start[d];
   };
-  const uint32_t max_t = ctx->tune_max_times ? ctx->tune_max_times : n_times;
+  // Time steps folded into one slab: all that share solution indices, unless
+  // that leaves too few 224-run tiles for the SMs; then split so that the
+  // whole interval has about four tiles per SM (load balance).
+  uint32_t max_t = ctx->tune_max_times;
+  if (max_t == 0) {
+    const uint64_t tiles_per_group = (n_baselines + 223) / 224;
+    const uint64_t want = 4ull * uint64_t(ctx->n_sm);
+    const uint64_t groups_per_cb =
+        (want + uint64_t(ctx->n_cb) * tiles_per_group - 1) /
+        (uint64_t(ctx->n_cb) * tiles_per_group);
+    max_t = uint32_t(std::max<uint64_t>(1, n_times / std::max<uint64_t>(1, groups_per_cb)));
+  }
   uint64_t off = 0;
   uint32_t t0 = 0;
   while (t0 < n_times) {
@@ -1502,8 +2831,8 @@ int ddsolve_set_channel_block(ddsolve_ctx* ctx, uint32_t cbi, uint64_t n_vis,
     v = w;
   }
   // Group runs into slabs by (length, solution indices). Runs of one slab are
-  // ordered by antenna 1 so that the warp-level segmented reduction finds
-  // long segments; the sum does not depend on the order.
+  // put in baseline-diagonal order (see the regular upload); the sums do not
+  // depend on the order.
   std::map<std::vector<uint32_t>, std::vector<uint32_t>> groups;
   for (uint32_t i = 0; i < runs.size(); ++i) {
     std::vector<uint32_t> key(ctx->n_dir + 1);
@@ -1518,8 +2847,13 @@ int ddsolve_set_channel_block(ddsolve_ctx* ctx, uint32_t cbi, uint64_t n_vis,
   uint64_t off = 0;
   for (auto& kv : groups) {
     std::vector<uint32_t>& members = kv.second;
+    auto diag = [&](uint32_t x) {
+      const uint32_t a1 = runs[x].ant & 0xFFFFu, a2 = runs[x].ant >> 16;
+      return (a2 + ctx->n_ant - a1) % ctx->n_ant;
+    };
     std::stable_sort(members.begin(), members.end(), [&](uint32_t x, uint32_t y) {
-      return (runs[x].ant & 0xFFFFu) < (runs[y].ant & 0xFFFFu);
+      const uint32_t dx = diag(x), dy = diag(y);
+      return dx != dy ? dx < dy : (runs[x].ant & 0xFFFFu) < (runs[y].ant & 0xFFFFu);
     });
     HostSlab s;
     s.T = 1;
@@ -1559,6 +2893,16 @@ int ddsolve_solve(ddsolve_ctx* ctx, double* solutions, ddsolve_result* result,
   DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_state.ptr, 0, sizeof(LoopState), ctx->stream));
   DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_nonfinite.ptr, 1, size_t(ctx->n_cb) * 4,
                                       ctx->stream));
+  if (ctx->use_pipe) {
+    // Initial MakeSolutionsFinite; later ones are fused into pipe_kernel.
+    DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_flag.ptr, 0, size_t(ctx->n_cb) * 4,
+                                        ctx->stream));
+    DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_done.ptr, 0, size_t(ctx->n_cb) * 4,
+                                        ctx->stream));
+    DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.ptr, 0, 16, ctx->stream));
+    if ((rc = LaunchMakeFinite(ctx, false)) != DDSOLVE_OK) return rc;
+    if ((rc = LaunchBuildTables(ctx)) != DDSOLVE_OK) return rc;
+  }
   if (!ctx->graph_ok) {
     rc = BuildGraph(ctx);
     if (rc != DDSOLVE_OK) {
@@ -1590,7 +2934,9 @@ int ddsolve_solve(ddsolve_ctx* ctx, double* solutions, ddsolve_result* result,
     DDS_CHECK_CUDA(ctx, cudaMemcpy(step_magnitudes, ctx->d_mags.ptr,
                                    size_t(ls.iteration) * 8, cudaMemcpyDeviceToHost));
   }
-  ctx->last_launches = uint64_t(ls.iteration) * 3;
+  ctx->last_launches =
+      ctx->use_pipe ? uint64_t(ls.iteration) + 1 : uint64_t(ls.iteration) * 3;
+  if ((rc = CheckDeviceError(ctx)) != DDSOLVE_OK) return rc;
   if (result) {
     // SolverBase::MakeResult (SolverBase.cc:192-213), constraints satisfied.
     result->iterations = ls.has_converged ? ls.iteration : ls.iteration + 1;
@@ -1610,13 +2956,21 @@ int ddsolve_perform_iteration(ddsolve_ctx* ctx, const double* solutions,
   const size_t n_sol = size_t(ctx->n_cb) * ctx->n_ant * ctx->n_sub * ctx->n_pol;
   DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->d_sol.ptr, solutions, n_sol * sizeof(double2),
                                       cudaMemcpyHostToDevice, ctx->stream));
+  if (ctx->use_pipe) {
+    DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_flag.ptr, 0, size_t(ctx->n_cb) * 4,
+                                        ctx->stream));
+    DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_done.ptr, 0, size_t(ctx->n_cb) * 4,
+                                        ctx->stream));
+    DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.ptr, 0, 16, ctx->stream));
+    if ((rc = LaunchBuildTables(ctx)) != DDSOLVE_OK) return rc;
+  }
   if ((rc = LaunchIteration(ctx, true, false, false)) != DDSOLVE_OK) return rc;
   DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(next_solutions, ctx->d_next.ptr,
                                       n_sol * sizeof(double2), cudaMemcpyDeviceToHost,
                                       ctx->stream));
   DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  ctx->last_launches = 2;
-  return DDSOLVE_OK;
+  ctx->last_launches = ctx->use_pipe ? 1 : 2;
+  return CheckDeviceError(ctx);
 }
 
 int ddsolve_time_stream_kernel(ddsolve_ctx* ctx, uint32_t n_launches, float* mean_ms) {
@@ -1627,12 +2981,23 @@ int ddsolve_time_stream_kernel(ddsolve_ctx* ctx, uint32_t n_launches, float* mea
   cudaEvent_t a, b;
   DDS_CHECK_CUDA(ctx, cudaEventCreate(&a));
   DDS_CHECK_CUDA(ctx, cudaEventCreate(&b));
-  const StreamParams sp = MakeStreamParams(ctx);
-  // warm-up launch
-  ctx->stream_fn<<<ctx->n_ctas, kThreads, ctx->stream_smem, ctx->stream>>>(sp);
-  DDS_CHECK_CUDA(ctx, cudaEventRecord(a, ctx->stream));
-  for (uint32_t i = 0; i < n_launches; ++i)
+  // warm-up launch, then n_launches timed launches of the streaming pass
+  // (pipe_kernel in next-solutions mode, or stream_kernel alone).
+  if (ctx->use_pipe) {
+    DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_flag.ptr, 0, size_t(ctx->n_cb) * 4,
+                                        ctx->stream));
+    if ((rc = LaunchBuildTables(ctx)) != DDSOLVE_OK) return rc;
+    if ((rc = LaunchIteration(ctx, true, false, false)) != DDSOLVE_OK) return rc;
+    DDS_CHECK_CUDA(ctx, cudaEventRecord(a, ctx->stream));
+    for (uint32_t i = 0; i < n_launches; ++i)
+      if ((rc = LaunchIteration(ctx, true, false, false)) != DDSOLVE_OK) return rc;
+  } else {
+    const StreamParams sp = MakeStreamParams(ctx);
     ctx->stream_fn<<<ctx->n_ctas, kThreads, ctx->stream_smem, ctx->stream>>>(sp);
+    DDS_CHECK_CUDA(ctx, cudaEventRecord(a, ctx->stream));
+    for (uint32_t i = 0; i < n_launches; ++i)
+      ctx->stream_fn<<<ctx->n_ctas, kThreads, ctx->stream_smem, ctx->stream>>>(sp);
+  }
   DDS_CHECK_CUDA(ctx, cudaEventRecord(b, ctx->stream));
   DDS_CHECK_CUDA(ctx, cudaEventSynchronize(b));
   float ms = 0;
@@ -1640,7 +3005,7 @@ int ddsolve_time_stream_kernel(ddsolve_ctx* ctx, uint32_t n_launches, float* mea
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   *mean_ms = ms / float(n_launches);
-  return DDSOLVE_OK;
+  return CheckDeviceError(ctx);
 }
 
 }  // extern "C"

@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 from dp3_b200 import synth
+from dp3_b200.solvers import SolveData
 from oracle import oracle_ffi as of
 from tests import helpers as H
 
@@ -55,8 +56,11 @@ def test_perform_iteration_matches_fp64_oracle(built, ncorr, npol, regular, dd):
     sol0 = _perturbed_start(obs, prob)
     ref = of.perform_iteration(prob, sol0, precision=64)
     solver = H.make_solver(prob)
-    if regular and ncorr == 2:
-        sd = obs.solve_data()
+    if regular:
+        cfg = obs.cfg
+        sd = SolveData.regular(prob["data"], prob["model"], cfg.n_times,
+                               cfg.n_baselines, cfg.cb_channels, obs.antenna1,
+                               obs.antenna2, ncorr)
     else:
         sd = H.solve_data_from_problem(prob)
     got = solver.PerformIteration(sd, sol0)
