@@ -201,7 +201,7 @@ def run_gpu_arm(args):
     from dp3_b200 import ddsolve, synth
     from dp3_b200 import build as native_build
     native_build.build_all()
-    cfg = synth.benchmark_configs()[CONFIG_INDEX]
+    cfg = synth.benchmark_configs()[args.config]
     # every rank solves its own interval (independent intervals: weak scaling)
     obs = synth.observe(cfg, pinned=True, noise_seed=cfg.seed * 7919 + 17 + rank)
     n_sub = sum(cfg.nspd)
@@ -226,6 +226,15 @@ def run_gpu_arm(args):
     stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=f"cuda:{device}")
 
     upload()
+    if args.pass_only:
+        # One streaming pass, timed alone (the command profiles use).
+        kernel_ms = ctx.time_stream_kernel(args.kernel_launches)
+        alg_bytes = cfg.n_vis * 16 * (1 + cfg.n_directions)
+        print(json.dumps({"config": cfg.name, "pass_ms": kernel_ms,
+                          "achieved_gbs": alg_bytes / (kernel_ms / 1e3) / 1e9}),
+              flush=True)
+        ctx.close()
+        return 0
     # ---- device-resident timing: K solves of the resident interval --------
     iters = []
     for _ in range(args.warmup):
@@ -340,6 +349,10 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=8.0,
                     help="seconds of CPU work per reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--config", type=int, default=CONFIG_INDEX,
+                    help="benchmark configuration index (synth.benchmark_configs)")
+    ap.add_argument("--pass-only", action="store_true",
+                    help="time only the streaming pass (for profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

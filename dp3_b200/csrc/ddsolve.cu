@@ -48,6 +48,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <type_traits>
 #include <mutex>
 #include <numeric>
 #include <string>
@@ -76,9 +77,15 @@ struct SlabDesc {
 // the tile of runs [r0, r0 + n_runs) of a slab; fragments of one CTA that
 // share a slab form a visit (one partial slot).
 struct Frag {
-  uint32_t slab, r0, n_runs, flags, row_lo, row_hi, visit, pad;
+  uint32_t slab, r0, n_runs, flags, row_lo, row_hi, visit, tile;
+  uint32_t group_end[2];  // direct reduction: end run (exclusive) of groups
+                          // 0..7, one byte each; groups partition [0, n_runs)
 };
-constexpr uint32_t kFragDirect = 1u;  // distinct antennas on both sides
+constexpr uint32_t kFragDirect = 1u;  // runs split into <= 8 groups, each with
+                                      // distinct first and second antennas
+constexpr uint32_t kMaxGroups = 8;
+constexpr uint32_t kFragPower = 2u;   // the fragment adds its tile's precomputed
+                                      // model powers sum |M|^2 (one per tile)
 
 struct Visit {
   uint32_t slab, run_lo, run_hi, pad;
@@ -776,6 +783,10 @@ struct PipeParams {
   uint32_t stages;
   uint32_t acc_floats;    // n_ant * acc_stride = one partial slot
   uint32_t owner_groups;  // direction groups per antenna in the sorted reduction
+  uint32_t n_gbuf;        // gain table buffers in shared memory (1 or 2)
+  const float* powers;    // model powers per tile [tile][dir][corr][kPipeRuns],
+                          // or null: accumulated in the row loop
+  uint32_t power_floats;  // floats per tile in `powers`
   // shared-memory layout (byte offsets)
   uint32_t off_acc, off_gtab, off_stg, off_cnt, off_off, off_pair, off_ent,
       off_wsum, off_stages;
@@ -1181,6 +1192,45 @@ __global__ void build_tables_kernel(const double2* __restrict__ solutions,
 }
 
 // Launched cooperatively (all CTAs co-resident), one CTA per SM.
+// Model powers of the pipelined path: for every tile of runs, direction and
+// correlation, sum over the tile's (time, channel) rows of |M|^2. They depend
+// on the model alone, so they are computed once per upload instead of in
+// every iteration's row loop. One block per (tile, direction), one thread per
+// run; FP64 sums, stored as FP32.
+struct PowerTile {
+  uint32_t slab, r0, n, pad;
+};
+
+template <int NCORR>
+__global__ void __launch_bounds__(kPipeRuns) power_kernel(const SlabDesc* __restrict__ slabs,
+                                                          const PowerTile* __restrict__ tiles,
+                                                          uint32_t n_dir, uint32_t power_floats,
+                                                          float* __restrict__ powers) {
+  const uint32_t tile = blockIdx.x / n_dir;
+  const uint32_t k = blockIdx.x - tile * n_dir;
+  const PowerTile t = tiles[tile];
+  const SlabDesc sl = slabs[t.slab];
+  const uint32_t r = threadIdx.x;
+  double q[NCORR];
+#pragma unroll
+  for (int c = 0; c < NCORR; ++c) q[c] = 0.0;
+  if (r < t.n) {
+    const size_t rows = size_t(sl.T) * sl.L;
+    const float2* m = static_cast<const float2*>(sl.model) +
+                      ((size_t(k) * rows) * sl.R + t.r0 + r) * NCORR;
+    for (size_t row = 0; row < rows; ++row, m += size_t(sl.R) * NCORR) {
+#pragma unroll
+      for (int c = 0; c < NCORR; ++c) {
+        const float2 v = __ldcs(m + c);
+        q[c] += double(v.x) * v.x + double(v.y) * v.y;
+      }
+    }
+  }
+  float* out = powers + size_t(tile) * power_floats + size_t(k) * NCORR * kPipeRuns;
+#pragma unroll
+  for (int c = 0; c < NCORR; ++c) out[c * kPipeRuns + r] = float(q[c]);
+}
+
 template <int NCORR, int NPOL, int DMAX>
 __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams p) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -1203,8 +1253,11 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
   char* stages = reinterpret_cast<char*>(smem + p.off_stages);
   constexpr uint32_t E = NCORR * 8;  // bytes per visibility
   const uint32_t acc_n = p.acc_floats;
-  const uint32_t n_dir = p.n_dir;
-  const uint32_t stage_bytes = (1 + n_dir) * kPipeRuns * E;
+  // Each instantiation serves exactly DMAX directions (no padded ones).
+  constexpr uint32_t n_dir = DMAX;
+  // stage: [run antennas of the fragment, first row only][data][model 0..]
+  constexpr uint32_t kRunsBytes = kPipeRuns * 4;
+  const uint32_t stage_bytes = kRunsBytes + (1 + n_dir) * kPipeRuns * E;
   const uint32_t table_bytes = p.table_f2 * 8;
   const uint32_t S = p.stages;
 
@@ -1233,14 +1286,15 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
     // ---------------- producer warp: one thread issues all bulk copies ----
     if (lane != 0) return;
     uint32_t row = 0, nvis = 0, cur_visit = 0xFFFFFFFFu;
+    uint32_t st = 0, ph = 0;  // stage of `row` and the parity of its use
     bool ok = true;
     for (uint32_t fi = f_begin; fi < f_end && ok; ++fi) {
       const Frag f = p.frags[fi];
       const SlabDesc sl = p.slabs[f.slab];
       if (f.visit != cur_visit) {  // new visit: its gain table first
-        const uint32_t b = nvis & 1u;
-        if (nvis >= 2 &&
-            !PipeWait(&gfree[b], ((nvis - 2) >> 1) & 1u, s_err, &p.counters[1])) {
+        const uint32_t b = nvis % p.n_gbuf;
+        const uint32_t use = nvis / p.n_gbuf;  // earlier uses of buffer b
+        if (use >= 1 && !PipeWait(&gfree[b], (use - 1) & 1u, s_err, &p.counters[1])) {
           ok = false;
           break;
         }
@@ -1252,21 +1306,50 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
       }
       const size_t tlr = size_t(sl.T) * sl.L * sl.R;
       const uint32_t seg = f.n_runs * E;
+      const char* dsrc = static_cast<const char*>(sl.data) +
+                         (size_t(f.row_lo) * sl.R + f.r0) * E;
+      const char* msrc = static_cast<const char*>(sl.model) +
+                         (size_t(f.row_lo) * sl.R + f.r0) * E;
+      const size_t row_step = size_t(sl.R) * E;
+      const size_t dir_step = tlr * E;
       for (uint32_t rr = f.row_lo; rr < f.row_hi; ++rr, ++row) {
-        const uint32_t s = row % S;
-        if (row >= S &&
-            !PipeWait(&empty[s], ((row / S) & 1u) ^ 1u, s_err, &p.counters[1])) {
+        if (row >= S && !PipeWait(&empty[st], ph ^ 1u, s_err, &p.counters[1])) {
           ok = false;
           break;
         }
-        MbarArriveExpectTx(&full[s], seg * (1 + n_dir));
-        char* dst = stages + size_t(s) * stage_bytes;
-        const size_t off = size_t(rr) * sl.R + f.r0;
-        BulkCopyG2S(dst, static_cast<const char*>(sl.data) + off * E, seg, &full[s]);
-        for (uint32_t d = 0; d < n_dir; ++d)
-          BulkCopyG2S(dst + size_t(1 + d) * kPipeRuns * E,
-                      static_cast<const char*>(sl.model) + (d * tlr + off) * E, seg,
-                      &full[s]);
+        // The fragment's run antennas travel with its first row (the run
+        // arrays are padded to whole 16-byte groups).
+        const uint32_t runs_bytes = rr == f.row_lo ? ((f.n_runs + 3u) & ~3u) * 4u : 0u;
+        MbarArriveExpectTx(&full[st], seg * (1 + n_dir) + runs_bytes);
+        char* dst = stages + size_t(st) * stage_bytes;
+        if (runs_bytes) BulkCopyG2S(dst, sl.run_ant + f.r0, runs_bytes, &full[st]);
+        dst += kRunsBytes;
+        BulkCopyG2S(dst, dsrc, seg, &full[st]);
+        const char* m = msrc;
+        for (uint32_t d = 0; d < n_dir; ++d, m += dir_step)
+          BulkCopyG2S(dst + size_t(1 + d) * kPipeRuns * E, m, seg, &full[st]);
+        dsrc += row_step;
+        msrc += row_step;
+        if (++st == S) {
+          st = 0;
+          ph ^= 1u;
+        }
+      }
+      if (ok && (f.flags & kFragPower)) {
+        // one more stage: the tile's model powers [dir][corr][run]
+        if (row >= S && !PipeWait(&empty[st], ph ^ 1u, s_err, &p.counters[1])) {
+          ok = false;
+          break;
+        }
+        const uint32_t pb = n_dir * NCORR * kPipeRuns * 4;
+        MbarArriveExpectTx(&full[st], pb);
+        BulkCopyG2S(stages + size_t(st) * stage_bytes,
+                    p.powers + size_t(f.tile) * p.power_floats, pb, &full[st]);
+        ++row;
+        if (++st == S) {
+          st = 0;
+          ph ^= 1u;
+        }
       }
     }
     // Wait for the last copies, so none is in flight when the CTA ends.
@@ -1274,113 +1357,183 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
       const uint32_t r = row - 1 - k;
       PipeWait(&full[r % S], (r / S) & 1u, s_err, &p.counters[1]);
     }
-    for (uint32_t k = 0; k < 2 && k < nvis; ++k) {
+    for (uint32_t k = 0; k < p.n_gbuf && k < nvis; ++k) {
       const uint32_t v = nvis - 1 - k;
-      PipeWait(&gfull[v & 1u], (v >> 1) & 1u, s_err, &p.counters[1]);
+      PipeWait(&gfull[v % p.n_gbuf], (v / p.n_gbuf) & 1u, s_err, &p.counters[1]);
     }
     return;
   }
 
   // ---------------- consumer warps ----------------
   const int ctid = tid;  // 0 .. kPipeRuns - 1
-  uint32_t row = 0, nvis = 0, cur_visit = 0xFFFFFFFFu;
+  const bool powers_pre = p.powers != nullptr;
+  uint32_t nvis = 0, cur_visit = 0xFFFFFFFFu;
+  uint32_t st = 0, ph = 0;  // stage of the next row and the parity of its use
   const float2* gtab = gtab_buf;
   auto end_visit = [&]() {
     // all consumers are done with the visit: release its gain table buffer
     // and flush the accumulators into the visit's partial slot
     ConsumerBarrier();
     __syncwarp();
-    if (lane == 0) MbarArrive(&gfree[(nvis - 1) & 1u]);
+    if (lane == 0) MbarArrive(&gfree[(nvis - 1) % p.n_gbuf]);
     float* out = p.partials + size_t(cur_visit) * acc_n;
     for (uint32_t i = ctid; i < acc_n; i += kPipeRuns) __stcg(out + i, acc[i]);
     ConsumerBarrier();
   };
+  // The next fragment's descriptor is fetched one fragment ahead, so that its
+  // global-memory latency overlaps the current fragment's rows; the run
+  // antennas arrive in shared memory with the fragment's first row.
+  Frag nf{};
+  if (f_begin < f_end) nf = p.frags[f_begin];
   for (uint32_t fi = f_begin; fi < f_end; ++fi) {
-    const Frag f = p.frags[fi];
-    const SlabDesc sl = p.slabs[f.slab];
+    const Frag f = nf;
+    if (fi + 1 < f_end) nf = p.frags[fi + 1];
     if (f.visit != cur_visit) {
       if (cur_visit != 0xFFFFFFFFu) end_visit();
       for (uint32_t i = ctid; i < acc_n; i += kPipeRuns) acc[i] = 0.f;
-      const uint32_t b = nvis & 1u;
-      PipeWait(&gfull[b], (nvis >> 1) & 1u, s_err, &p.counters[1]);
+      const uint32_t b = nvis % p.n_gbuf;
+      PipeWait(&gfull[b], (nvis / p.n_gbuf) & 1u, s_err, &p.counters[1]);
       gtab = gtab_buf + size_t(b) * p.table_f2;
       cur_visit = f.visit;
       ++nvis;
       ConsumerBarrier();
     }
-    const uint32_t run = f.r0 + ctid;
     const bool active = uint32_t(ctid) < f.n_runs;
+    const bool warp_busy = uint32_t(warp) * 32u < f.n_runs;
     uint32_t a1 = 0, a2 = 0;
-    if (active) {
-      const uint32_t ap = sl.run_ant[run];
-      a1 = ap & 0xFFFFu;
-      a2 = ap >> 16;
-    }
     float2 G[DMAX][NCORR];
     float2 P[DMAX][NCORR];
     float Q[DMAX][NCORR];
 #pragma unroll
-    for (int k = 0; k < DMAX; ++k) {
-      float2 ga[NPOL], gb[NPOL];
-#pragma unroll
-      for (int q = 0; q < NPOL; ++q) {
-        ga[q] = make_float2(0.f, 0.f);
-        gb[q] = make_float2(0.f, 0.f);
-        if (k < int(n_dir)) {
-          ga[q] = gtab[a1 * p.gain_stride + k * NPOL + q];
-          gb[q] = gtab[a2 * p.gain_stride + k * NPOL + q];
-        }
-      }
+    for (int k = 0; k < DMAX; ++k)
 #pragma unroll
       for (int c = 0; c < NCORR; ++c) {
-        G[k][c] = cmul_conj(ga[RowPol<NCORR, NPOL>(c)], gb[ColPol<NCORR, NPOL>(c)]);
         P[k][c] = make_float2(0.f, 0.f);
         Q[k][c] = 0.f;
       }
-    }
-    for (uint32_t rr = f.row_lo; rr < f.row_hi; ++rr, ++row) {
-      const uint32_t s = row % S;
-      PipeWait(&full[s], (row / S) & 1u, s_err, &p.counters[1]);
-      const char* base = stages + size_t(s) * stage_bytes;
-      float2 Rv[NCORR];
-      LoadVisShared<NCORR>(base, ctid, Rv);
-      // Residual R = D - sum_d G_d M_d (first read of the model rows) ...
-#pragma unroll
-      for (int k = 0; k < DMAX; ++k) {
-        float2 M[NCORR];
-        if (k < int(n_dir)) {
-          LoadVisShared<NCORR>(base + size_t(1 + k) * kPipeRuns * E, ctid, M);
-        } else {
-#pragma unroll
-          for (int c = 0; c < NCORR; ++c) M[c] = make_float2(0.f, 0.f);
-        }
-#pragma unroll
-        for (int c = 0; c < NCORR; ++c) {
-          Rv[c].x = fmaf(-G[k][c].x, M[c].x, Rv[c].x);
-          Rv[c].x = fmaf(G[k][c].y, M[c].y, Rv[c].x);
-          Rv[c].y = fmaf(-G[k][c].x, M[c].y, Rv[c].y);
-          Rv[c].y = fmaf(-G[k][c].y, M[c].x, Rv[c].y);
-        }
+    for (uint32_t rr = f.row_lo; rr < f.row_hi; ++rr) {
+      const uint32_t s = st;
+      PipeWait(&full[s], ph, s_err, &p.counters[1]);
+      if (++st == S) {
+        st = 0;
+        ph ^= 1u;
       }
-      // ... then P_d += R conj(M_d), Q_d += |M_d|^2 (second read, shared).
+      // Warps without runs in this tile only release the stage.
+      if (warp_busy) {
+        if (rr == f.row_lo) {
+          // first row of the fragment: run antennas and the run's gain products
+          const uint32_t ap =
+              active ? reinterpret_cast<const uint32_t*>(stages + size_t(s) * stage_bytes)[ctid] : 0u;
+          a1 = ap & 0xFFFFu;
+          a2 = ap >> 16;
 #pragma unroll
-      for (int k = 0; k < DMAX; ++k) {
-        float2 M[NCORR];
-        if (k < int(n_dir)) {
-          LoadVisShared<NCORR>(base + size_t(1 + k) * kPipeRuns * E, ctid, M);
-        } else {
+          for (int k = 0; k < DMAX; ++k) {
+            float2 ga[NPOL], gb[NPOL];
 #pragma unroll
-          for (int c = 0; c < NCORR; ++c) M[c] = make_float2(0.f, 0.f);
+            for (int q = 0; q < NPOL; ++q) {
+              ga[q] = make_float2(0.f, 0.f);
+              gb[q] = make_float2(0.f, 0.f);
+              if (k < int(n_dir)) {
+                ga[q] = gtab[a1 * p.gain_stride + k * NPOL + q];
+                gb[q] = gtab[a2 * p.gain_stride + k * NPOL + q];
+              }
+            }
+#pragma unroll
+            for (int c = 0; c < NCORR; ++c)
+              G[k][c] = cmul_conj(ga[RowPol<NCORR, NPOL>(c)], gb[ColPol<NCORR, NPOL>(c)]);
+          }
         }
+        const char* base = stages + size_t(s) * stage_bytes + kRunsBytes;
+        // Residual R = D - sum_d G_d M_d, then P_d += R conj(M_d), and
+        // Q_d += |M_d|^2 unless the model powers were precomputed. The model
+        // row stays in registers between the two passes when it fits next to
+        // the accumulators (shared-memory bandwidth is the row loop's limit),
+        // else it is read from shared memory twice.
+        auto row_body = [&](auto with_q) {
+          constexpr bool kQ = decltype(with_q)::value;
+          constexpr bool kKeepM = kQ ? DMAX * NCORR <= 12 : DMAX * NCORR <= 20;
+          // The residual is summed in two halves (even and odd directions) to
+          // halve its chain of dependent multiply-adds.
+          float2 Rv[NCORR], Ro[NCORR];
+          LoadVisShared<NCORR>(base, ctid, Rv);
 #pragma unroll
-        for (int c = 0; c < NCORR; ++c) {
-          P[k][c].x = fmaf(Rv[c].x, M[c].x, P[k][c].x);
-          P[k][c].x = fmaf(Rv[c].y, M[c].y, P[k][c].x);
-          P[k][c].y = fmaf(Rv[c].y, M[c].x, P[k][c].y);
-          P[k][c].y = fmaf(-Rv[c].x, M[c].y, P[k][c].y);
-          Q[k][c] = fmaf(M[c].x, M[c].x, Q[k][c]);
-          Q[k][c] = fmaf(M[c].y, M[c].y, Q[k][c]);
-        }
+          for (int c = 0; c < NCORR; ++c) Ro[c] = make_float2(0.f, 0.f);
+          float2 Mk[kKeepM ? DMAX : 1][NCORR];
+#pragma unroll
+          for (int k = 0; k < DMAX; ++k) {
+            float2 M[NCORR];
+            if (k < int(n_dir)) {
+              LoadVisShared<NCORR>(base + size_t(1 + k) * kPipeRuns * E, ctid, M);
+            } else {
+#pragma unroll
+              for (int c = 0; c < NCORR; ++c) M[c] = make_float2(0.f, 0.f);
+            }
+            if constexpr (kKeepM) {
+#pragma unroll
+              for (int c = 0; c < NCORR; ++c) Mk[k][c] = M[c];
+            }
+#pragma unroll
+            for (int c = 0; c < NCORR; ++c) {
+              float2& r = (k & 1) ? Ro[c] : Rv[c];
+              r.x = fmaf(-G[k][c].x, M[c].x, r.x);
+              r.x = fmaf(G[k][c].y, M[c].y, r.x);
+              r.y = fmaf(-G[k][c].x, M[c].y, r.y);
+              r.y = fmaf(-G[k][c].y, M[c].x, r.y);
+            }
+          }
+#pragma unroll
+          for (int c = 0; c < NCORR; ++c) {
+            Rv[c].x += Ro[c].x;
+            Rv[c].y += Ro[c].y;
+          }
+#pragma unroll
+          for (int k = 0; k < DMAX; ++k) {
+            float2 M[NCORR];
+            if constexpr (kKeepM) {
+#pragma unroll
+              for (int c = 0; c < NCORR; ++c) M[c] = Mk[k][c];
+            } else if (k < int(n_dir)) {
+              LoadVisShared<NCORR>(base + size_t(1 + k) * kPipeRuns * E, ctid, M);
+            } else {
+#pragma unroll
+              for (int c = 0; c < NCORR; ++c) M[c] = make_float2(0.f, 0.f);
+            }
+#pragma unroll
+            for (int c = 0; c < NCORR; ++c) {
+              P[k][c].x = fmaf(Rv[c].x, M[c].x, P[k][c].x);
+              P[k][c].x = fmaf(Rv[c].y, M[c].y, P[k][c].x);
+              P[k][c].y = fmaf(Rv[c].y, M[c].x, P[k][c].y);
+              P[k][c].y = fmaf(-Rv[c].x, M[c].y, P[k][c].y);
+              if constexpr (kQ) {
+                Q[k][c] = fmaf(M[c].x, M[c].x, Q[k][c]);
+                Q[k][c] = fmaf(M[c].y, M[c].y, Q[k][c]);
+              }
+            }
+          }
+        };
+        if (powers_pre)
+          row_body(std::false_type{});
+        else
+          row_body(std::true_type{});
+      }
+      __syncwarp();
+      if (lane == 0) MbarArrive(&empty[s]);
+    }
+    if (f.flags & kFragPower) {
+      // the tile's precomputed model powers, in the stage after its rows
+      const uint32_t s = st;
+      PipeWait(&full[s], ph, s_err, &p.counters[1]);
+      if (++st == S) {
+        st = 0;
+        ph ^= 1u;
+      }
+      if (active) {
+        const float* pw = reinterpret_cast<const float*>(stages + size_t(s) * stage_bytes);
+#pragma unroll
+        for (int k = 0; k < DMAX; ++k)
+#pragma unroll
+          for (int c = 0; c < NCORR; ++c)
+            if (k < int(n_dir)) Q[k][c] = pw[(k * NCORR + c) * kPipeRuns + ctid];
       }
       __syncwarp();
       if (lane == 0) MbarArrive(&empty[s]);
@@ -1389,12 +1542,19 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
     // ---- tile reduction into the visit's antenna accumulators ----
     ConsumerBarrier();  // the previous reduction is complete everywhere
     if (f.flags & kFragDirect) {
-      // The tile's first antennas are distinct, and so are its second
-      // antennas: two conflict-free phases of plain shared-memory updates.
+      // The runs form up to eight consecutive groups; within a group the
+      // first antennas are distinct and so are the second antennas. Per
+      // group, two conflict-free phases of plain shared-memory updates.
+      const uint32_t n_groups_t = (f.flags >> 8) & 0xFu;
+      uint32_t my_group = 0;
 #pragma unroll
-      for (int side = 0; side < 2; ++side) {
-        if (side == 1) ConsumerBarrier();
-        if (active) {
+      for (int g = 0; g < int(kMaxGroups) - 1; ++g)
+        my_group += uint32_t(ctid) >= ((f.group_end[g >> 2] >> ((g & 3) * 8)) & 0xFFu) &&
+                    uint32_t(g + 1) < n_groups_t;
+      for (uint32_t phase = 0; phase < 2 * n_groups_t; ++phase) {
+        const int side = int(phase & 1u);
+        if (phase > 0) ConsumerBarrier();
+        if (active && my_group == (phase >> 1)) {
           const uint32_t a = side == 0 ? a1 : a2;
           const uint32_t b = side == 0 ? a2 : a1;
 #pragma unroll
@@ -1494,49 +1654,68 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
       const uint32_t a = task / n_groups;
       const uint32_t grp = task - a * n_groups;
       const uint32_t e0 = a_off[a], e1 = e0 + a_cnt[a];
+      if (e1 == e0) continue;
+      // directions grp, grp + n_groups, ... (at most DMAX), summed in
+      // registers over the antenna's entries, then one shared update each
+      float sum[DMAX][NPOL][3];
+#pragma unroll
+      for (int i = 0; i < DMAX; ++i)
+#pragma unroll
+        for (int q = 0; q < NPOL; ++q) sum[i][q][0] = sum[i][q][1] = sum[i][q][2] = 0.f;
       for (uint32_t e = e0; e < e1; ++e) {
         const uint32_t en = ent[e];
         const uint32_t j = en >> 1;
         const bool second = (en & 1u) != 0;  // antenna a is antenna 2 of run j
         const uint32_t pr = t_pair[j];
         const uint32_t b = second ? (pr & 0xFFFFu) : (pr >> 16);
-        for (uint32_t k = grp; k < n_dir; k += n_groups) {
-          float2 gb[NPOL];
 #pragma unroll
-          for (int q = 0; q < NPOL; ++q) gb[q] = gtab[b * p.gain_stride + k * NPOL + q];
-          float2 Pc[NCORR];
-          float Qc[NCORR];
+        for (int i = 0; i < DMAX; ++i) {
+          const uint32_t k = grp + i * n_groups;
+          if (k < n_dir) {
+            float2 gb[NPOL];
 #pragma unroll
-          for (int c = 0; c < NCORR; ++c) {
-            const float* v = stg + ((k * NCORR + c) * 3) * kPipeRuns + j;
-            Pc[c] = make_float2(v[0], v[kPipeRuns]);
-            Qc[c] = v[2 * kPipeRuns];
+            for (int q = 0; q < NPOL; ++q) gb[q] = gtab[b * p.gain_stride + k * NPOL + q];
+            float2 Pc[NCORR];
+            float Qc[NCORR];
+#pragma unroll
+            for (int c = 0; c < NCORR; ++c) {
+              const float* v = stg + ((k * NCORR + c) * 3) * kPipeRuns + j;
+              Pc[c] = make_float2(v[0], v[kPipeRuns]);
+              Qc[c] = v[2 * kPipeRuns];
+            }
+#pragma unroll
+            for (int q = 0; q < NPOL; ++q) {
+#pragma unroll
+              for (int c = 0; c < NCORR; ++c) {
+                const int rp = RowPol<NCORR, NPOL>(c);
+                const int cp = ColPol<NCORR, NPOL>(c);
+                if (!second && rp == q) {  // num += g_b P, den += |g_b|^2 Q
+                  const float2 t1 = cmul(gb[cp], Pc[c]);
+                  sum[i][q][0] += t1.x;
+                  sum[i][q][1] += t1.y;
+                  sum[i][q][2] += cnorm(gb[cp]) * Qc[c];
+                }
+                if (second && cp == q) {  // num += g_a conj(P), den += |g_a|^2 Q
+                  const float2 t2 = cmul(gb[rp], cconj(Pc[c]));
+                  sum[i][q][0] += t2.x;
+                  sum[i][q][1] += t2.y;
+                  sum[i][q][2] += cnorm(gb[rp]) * Qc[c];
+                }
+              }
+            }
           }
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < DMAX; ++i) {
+        const uint32_t k = grp + i * n_groups;
+        if (k < n_dir) {
           float* x = acc + a * p.acc_stride + k * NPOL * 3;
 #pragma unroll
           for (int q = 0; q < NPOL; ++q) {
-            float2 n = make_float2(0.f, 0.f);
-            float dd = 0.f;
-#pragma unroll
-            for (int c = 0; c < NCORR; ++c) {
-              const int rp = RowPol<NCORR, NPOL>(c);
-              const int cp = ColPol<NCORR, NPOL>(c);
-              if (!second && rp == q) {
-                const float2 t1 = cmul(gb[cp], Pc[c]);
-                n.x += t1.x;
-                n.y += t1.y;
-                dd += cnorm(gb[cp]) * Qc[c];
-              }
-              if (second && cp == q) {
-                const float2 t2 = cmul(gb[rp], cconj(Pc[c]));
-                n.x += t2.x;
-                n.y += t2.y;
-                dd += cnorm(gb[rp]) * Qc[c];
-              }
-            }
-            x[q * 3 + 0] += n.x;
-            x[q * 3 + 1] += n.y;
-            x[q * 3 + 2] += dd;
+            x[q * 3 + 0] += sum[i][q][0];
+            x[q * 3 + 1] += sum[i][q][1];
+            x[q * 3 + 2] += sum[i][q][2];
           }
         }
       }
@@ -1642,6 +1821,15 @@ struct ChannelBlockStore {
   std::vector<uint32_t> prev_run_ant;
 };
 
+// Pads the run arrays to a whole number of 16-byte groups with empty runs.
+void PadRuns(ChannelBlockStore& cb) {
+  while (cb.run_ant.size() & 3u) {
+    cb.run_ant.push_back(0u);
+    cb.run_src.push_back(0u);
+    cb.run_len.push_back(0u);
+  }
+}
+
 using StreamFn = void (*)(StreamParams);
 
 }  // namespace
@@ -1673,10 +1861,14 @@ struct ddsolve_ctx {
   uint32_t pipe_stages = 0, acc_stride = 0, gain_stride = 0;
   DevBuf d_cb_done /* new non-finite flags */, d_cb_flag, d_cb_avg, d_counters;
   DevBuf d_frags, d_cta_frag_off, d_tables, d_tab_cb, d_tab_sol, d_tab_off, d_tab_ent;
-  uint32_t n_tables = 0, table_f2 = 0, owner_groups = 1;
+  uint32_t n_tables = 0, table_f2 = 0, owner_groups = 1, n_gbuf = 2;
   uint32_t off_acc = 0, off_gtab = 0, off_stg = 0, off_cnt = 0, off_off = 0,
            off_pair = 0, off_ent = 0, off_wsum = 0, off_stages = 0;
   uint32_t n_ctas = 0, n_visits = 0, fin_blocks = 0;
+  // precomputed model powers (pipe_kernel), refreshed after every upload
+  bool use_powers = false, powers_dirty = true;
+  uint32_t n_power_tiles = 0, power_floats = 0;
+  DevBuf d_power_tiles, d_powers;
   DevBuf d_slabs, d_visits, d_cta_off, d_slab_sol, d_partials, d_fin_off,
       d_fin_visits, d_dir_of_sub, d_block_sum, d_block_cnt;
   // solver state
@@ -1751,12 +1943,20 @@ constexpr KernelEntry PipeEntry() {
 
 const std::vector<KernelEntry>& PipeKernels() {
   static const std::vector<KernelEntry> k = {
-      PipeEntry<2, 2, 2>(), PipeEntry<2, 2, 4>(), PipeEntry<2, 2, 6>(),
-      PipeEntry<2, 2, 8>(), PipeEntry<2, 2, 10>(), PipeEntry<2, 2, 12>(),
-      PipeEntry<2, 1, 2>(), PipeEntry<2, 1, 4>(), PipeEntry<2, 1, 6>(),
-      PipeEntry<2, 1, 8>(), PipeEntry<2, 1, 10>(), PipeEntry<2, 1, 12>(),
-      PipeEntry<4, 2, 2>(), PipeEntry<4, 2, 4>(),
-      PipeEntry<4, 1, 2>(), PipeEntry<4, 1, 4>(),
+      // One instantiation per direction count: a padded direction would
+      // cost a full share of the row loop, and exact counts need no guards.
+      PipeEntry<2, 2, 1>(), PipeEntry<2, 2, 2>(), PipeEntry<2, 2, 3>(),
+      PipeEntry<2, 2, 4>(), PipeEntry<2, 2, 5>(), PipeEntry<2, 2, 6>(),
+      PipeEntry<2, 2, 7>(), PipeEntry<2, 2, 8>(), PipeEntry<2, 2, 9>(),
+      PipeEntry<2, 2, 10>(), PipeEntry<2, 2, 11>(), PipeEntry<2, 2, 12>(),
+      PipeEntry<2, 1, 1>(), PipeEntry<2, 1, 2>(), PipeEntry<2, 1, 3>(),
+      PipeEntry<2, 1, 4>(), PipeEntry<2, 1, 5>(), PipeEntry<2, 1, 6>(),
+      PipeEntry<2, 1, 7>(), PipeEntry<2, 1, 8>(), PipeEntry<2, 1, 9>(),
+      PipeEntry<2, 1, 10>(), PipeEntry<2, 1, 11>(), PipeEntry<2, 1, 12>(),
+      PipeEntry<4, 2, 1>(), PipeEntry<4, 2, 2>(), PipeEntry<4, 2, 3>(),
+      PipeEntry<4, 2, 4>(),
+      PipeEntry<4, 1, 1>(), PipeEntry<4, 1, 2>(), PipeEntry<4, 1, 3>(),
+      PipeEntry<4, 1, 4>(),
   };
   return k;
 }
@@ -1764,16 +1964,21 @@ const std::vector<KernelEntry>& PipeKernels() {
 const KernelEntry* FindPipeKernel(int ncorr, int npol, int n_dir) {
   const KernelEntry* best = nullptr;
   for (const KernelEntry& e : PipeKernels())
-    if (e.ncorr == ncorr && e.npol == npol && e.dmax >= n_dir &&
-        (!best || e.dmax < best->dmax))
-      best = &e;
+    if (e.ncorr == ncorr && e.npol == npol && e.dmax == n_dir) best = &e;
   return best;
 }
 
 uint32_t OddAtLeast(uint32_t x) { return x | 1u; }
 
-// Shared memory of pipe_kernel for `stages` stages, with the scratch of the
-// sorted tile reduction (the layout is fixed in BuildPipePlan).
+// One pipeline stage of pipe_kernel: the fragment's run antennas (first row
+// only), then one row of data and of every direction's model.
+size_t PipeStageBytes(const ddsolve_ctx* ctx) {
+  return size_t(kPipeRuns) * 4 + size_t(1 + ctx->n_dir) * kPipeRuns * ctx->elem_bytes;
+}
+
+// Shared memory of pipe_kernel for `stages` stages, with one gain-table
+// buffer and the scratch of the sorted tile reduction (the layout is fixed in
+// BuildPipePlan, which adds the second gain-table buffer when it fits).
 size_t PipeSmemBytes(const ddsolve_ctx* ctx, uint32_t stages, uint32_t acc_stride,
                      uint32_t gain_stride) {
   auto align = [](size_t x, size_t a) { return (x + a - 1) / a * a; };
@@ -1781,11 +1986,11 @@ size_t PipeSmemBytes(const ddsolve_ctx* ctx, uint32_t stages, uint32_t acc_strid
   const size_t table_f2 = (size_t(ctx->n_ant) * gain_stride + 1) & ~size_t(1);
   size_t off = align(256 + size_t(kPipeRuns) * 12, 16);
   off += align(size_t(ctx->n_ant) * acc_stride * 4, 16);
-  off += 2 * table_f2 * 8;
+  off += table_f2 * 8;
   off += size_t(3) * ctx->n_corr * ctx->n_dir * kPipeRuns * 4 + 2 * n_ant4 * 4 +
          size_t(kPipeRuns) * 4 + size_t(kPipeRuns) * 4 + 128;
   off = align(off, 128);
-  return off + size_t(stages) * (1 + ctx->n_dir) * kPipeRuns * ctx->elem_bytes;
+  return off + size_t(stages) * PipeStageBytes(ctx);
 }
 
 int PreferredDirsPerLane(int ncorr) { return ncorr == 4 ? 2 : (ncorr == 2 ? 5 : 8); }
@@ -1880,6 +2085,7 @@ int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const float* data,
     cb.prev_run_ant = cb.run_ant;
   }
   cb.set = true;
+  ctx->powers_dirty = true;
   return DDSOLVE_OK;
 }
 
@@ -1922,30 +2128,68 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
 
   // ---- tiles ----
   struct Tile {
-    uint32_t slab, r0, n, rows, direct;
+    uint32_t slab, r0, n, rows, flags;
+    uint32_t group_end[2];
   };
   std::vector<Tile> tiles;
   std::vector<uint32_t> stamp1(n_ant, 0xFFFFFFFFu), stamp2(n_ant, 0xFFFFFFFFu);
-  uint32_t tile_id = 0;
+  uint32_t group_id = 0;
   bool any_sorted = false;
   for (uint32_t gi = 0; gi < descs.size(); ++gi) {
     const SlabDesc& sd = descs[gi];
     const ChannelBlockStore& cbs = ctx->cbs[sd.cb];
     const uint32_t run_off = uint32_t(sd.run_ant - cbs.run_ant_dev.as<uint32_t>());
-    for (uint32_t r0 = 0; r0 < sd.R; r0 += kPipeRuns, ++tile_id) {
-      const uint32_t n = std::min<uint32_t>(kPipeRuns, sd.R - r0);
-      bool direct = true;
-      for (uint32_t r = r0; r < r0 + n && direct; ++r) {
+    // Equal tiles (a multiple of 4 runs, so that each tile's run antennas
+    // start on a 16-byte boundary): a short remainder tile would stream its
+    // rows at a fraction of the bytes per pipeline stage.
+    const uint32_t n_tiles_slab = (sd.R + kPipeRuns - 1) / kPipeRuns;
+    const uint32_t tile_runs =
+        n_tiles_slab ? ((sd.R + n_tiles_slab - 1) / n_tiles_slab + 3u) & ~3u : kPipeRuns;
+    for (uint32_t r0 = 0; r0 < sd.R; r0 += tile_runs) {
+      const uint32_t n = std::min<uint32_t>(tile_runs, sd.R - r0);
+      // Greedy split into consecutive groups whose first antennas are
+      // distinct and whose second antennas are distinct (a cyclic diagonal
+      // of the regular layout is one such group).
+      Tile t{gi, r0, n, sd.T * sd.L, 0u, {0u, 0u}};
+      uint32_t n_groups = 1;
+      ++group_id;
+      for (uint32_t r = r0; r < r0 + n; ++r) {
         const uint32_t ap = cbs.run_ant[run_off + r];
         const uint32_t a1 = ap & 0xFFFFu, a2 = ap >> 16;
-        if (stamp1[a1] == tile_id || stamp2[a2] == tile_id) direct = false;
-        stamp1[a1] = tile_id;
-        stamp2[a2] = tile_id;
+        if (stamp1[a1] == group_id || stamp2[a2] == group_id) {
+          if (n_groups == kMaxGroups) {
+            n_groups = kMaxGroups + 1;
+            break;
+          }
+          const uint32_t g = n_groups - 1;
+          t.group_end[g >> 2] |= (r - r0) << ((g & 3) * 8);
+          ++n_groups;
+          ++group_id;
+        }
+        stamp1[a1] = group_id;
+        stamp2[a2] = group_id;
       }
-      any_sorted = any_sorted || !direct;
-      tiles.push_back({gi, r0, n, sd.T * sd.L, direct ? 1u : 0u});
+      if (n_groups <= kMaxGroups) {
+        const uint32_t g = n_groups - 1;
+        t.group_end[g >> 2] |= n << ((g & 3) * 8);
+        t.flags = kFragDirect | (n_groups << 8);
+      } else {
+        t.group_end[0] = t.group_end[1] = 0;
+        any_sorted = true;
+      }
+      tiles.push_back(t);
     }
   }
+  // Model powers are precomputed (one stage per tile and iteration) when the
+  // tiles are deep enough in rows for that stage to cost less than the two
+  // multiply-adds per row, direction and correlation it replaces.
+  uint64_t run_rows = 0, n_runs_all = 0;
+  for (const Tile& t : tiles) {
+    run_rows += uint64_t(t.n) * t.rows;
+    n_runs_all += t.n;
+  }
+  const bool use_powers = !std::getenv("DDSOLVE_NO_POWERS") && n_runs_all > 0 &&
+                          run_rows >= 16 * n_runs_all;
   // ---- fragments: rows balanced over the CTAs ----
   uint64_t total_rows = 0;
   double total_w = 0.0;
@@ -1974,7 +2218,10 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
           ++hi;
         }
         if (hi > lo) {
-          frags.push_back({t.slab, t.r0, t.n, t.direct, lo, hi, 0, 0});
+          const uint32_t ti = uint32_t(&t - tiles.data());
+          const uint32_t fl = t.flags | (use_powers && lo == 0 ? kFragPower : 0u);
+          frags.push_back({t.slab, t.r0, t.n, fl, lo, hi, 0, ti,
+                           {t.group_end[0], t.group_end[1]}});
           cum += double(hi - lo) * w;
           lo = hi;
         }
@@ -2023,7 +2270,16 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
   ctx->off_acc = uint32_t(align(off, 16));
   off = ctx->off_acc + align(size_t(n_ant) * ctx->acc_stride * 4, 16);
   ctx->off_gtab = uint32_t(off);
-  off += size_t(2) * table_f2 * 8;
+  // Two gain-table buffers (the next visit's table loads while the current
+  // one is in use) unless that leaves fewer than four stages.
+  {
+    const size_t stage_b = PipeStageBytes(ctx);
+    const size_t rest = size_t(3) * ctx->n_corr * n_dir * kPipeRuns * 4 + 2 * align(n_ant, 4) * 4 +
+                        size_t(kPipeRuns) * 8 + 256;
+    const size_t with2 = off + 2 * size_t(table_f2) * 8 + (any_sorted ? rest : 256);
+    ctx->n_gbuf = (with2 + 4 * stage_b <= size_t(max_optin)) ? 2u : 1u;
+  }
+  off += size_t(ctx->n_gbuf) * table_f2 * 8;
   const size_t n_ant4 = align(n_ant, 4);
   ctx->off_stg = uint32_t(off);
   if (any_sorted) off += size_t(3) * ctx->n_corr * n_dir * kPipeRuns * 4;
@@ -2038,7 +2294,7 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
   ctx->off_wsum = uint32_t(off);
   off += 32 * 4;
   ctx->off_stages = uint32_t(align(off, 128));
-  const size_t stage_bytes = size_t(1 + n_dir) * kPipeRuns * ctx->elem_bytes;
+  const size_t stage_bytes = PipeStageBytes(ctx);
   const size_t room = size_t(max_optin) > ctx->off_stages ? size_t(max_optin) - ctx->off_stages : 0;
   const uint32_t stages = uint32_t(std::min<size_t>(kPipeMaxStages, room / stage_bytes));
   if (stages < 2)
@@ -2076,6 +2332,16 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
   if ((rc = upload(ctx->d_tab_sol, tab_sol.data(), tab_sol.size() * 4))) return rc;
   if ((rc = upload(ctx->d_tab_off, tab_off.data(), tab_off.size() * 4))) return rc;
   if ((rc = upload(ctx->d_tab_ent, tab_ent.data(), tab_ent.size() * 4))) return rc;
+  ctx->use_powers = use_powers;
+  ctx->powers_dirty = true;
+  ctx->n_power_tiles = uint32_t(tiles.size());
+  ctx->power_floats = n_dir * ctx->n_corr * kPipeRuns;
+  if (use_powers) {
+    std::vector<PowerTile> pt(tiles.size());
+    for (size_t i = 0; i < tiles.size(); ++i) pt[i] = {tiles[i].slab, tiles[i].r0, tiles[i].n, 0u};
+    if ((rc = upload(ctx->d_power_tiles, pt.data(), pt.size() * sizeof(PowerTile)))) return rc;
+    DDS_CHECK_CUDA(ctx, ctx->d_powers.Reserve(tiles.size() * ctx->power_floats * 4));
+  }
   DDS_CHECK_CUDA(ctx, ctx->d_tables.Reserve(size_t(n_tables) * table_f2 * 8));
   DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_tables.ptr, 0, size_t(n_tables) * table_f2 * 8,
                                       ctx->stream));
@@ -2384,6 +2650,9 @@ PipeParams MakePipeParams(ddsolve_ctx* ctx, bool host_mode, bool use_handle) {
   p.stages = ctx->pipe_stages;
   p.acc_floats = ctx->n_ant * ctx->acc_stride;
   p.owner_groups = ctx->owner_groups;
+  p.n_gbuf = ctx->n_gbuf;
+  p.powers = ctx->use_powers ? ctx->d_powers.as<float>() : nullptr;
+  p.power_floats = ctx->power_floats;
   p.off_acc = ctx->off_acc;
   p.off_gtab = ctx->off_gtab;
   p.off_stg = ctx->off_stg;
@@ -2429,6 +2698,26 @@ int LaunchBuildTables(ddsolve_ctx* ctx) {
         ctx->d_tab_sol.as<uint32_t>(), ctx->n_tables, ctx->n_ant, ctx->n_dir, ctx->n_sub,
         ctx->gain_stride, ctx->table_f2);
   DDS_CHECK_CUDA(ctx, cudaGetLastError());
+  return DDSOLVE_OK;
+}
+
+// Model powers of the pipelined path, when the plan uses them and the model
+// changed since they were last computed (or `force`).
+int LaunchPowers(ddsolve_ctx* ctx, bool force) {
+  if (!ctx->use_pipe || !ctx->use_powers || (!ctx->powers_dirty && !force)) return DDSOLVE_OK;
+  const uint32_t blocks = ctx->n_power_tiles * ctx->n_dir;
+  if (blocks) {
+    if (ctx->n_corr == 2)
+      power_kernel<2><<<blocks, kPipeRuns, 0, ctx->stream>>>(
+          ctx->d_slabs.as<SlabDesc>(), ctx->d_power_tiles.as<PowerTile>(), ctx->n_dir,
+          ctx->power_floats, ctx->d_powers.as<float>());
+    else
+      power_kernel<4><<<blocks, kPipeRuns, 0, ctx->stream>>>(
+          ctx->d_slabs.as<SlabDesc>(), ctx->d_power_tiles.as<PowerTile>(), ctx->n_dir,
+          ctx->power_floats, ctx->d_powers.as<float>());
+    DDS_CHECK_CUDA(ctx, cudaGetLastError());
+  }
+  ctx->powers_dirty = false;
   return DDSOLVE_OK;
 }
 
@@ -2732,9 +3021,12 @@ int ddsolve_set_channel_block_regular(ddsolve_ctx* ctx, uint32_t cbi,
   std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
     return o_delta[x] != o_delta[y] ? o_delta[x] < o_delta[y] : o_a1[x] < o_a1[y];
   });
-  cb.run_ant.resize(n_baselines);
-  cb.run_src.resize(n_baselines);
-  cb.run_len.resize(n_baselines);
+  // Run arrays padded to whole 16-byte groups (pipe_kernel bulk-copies
+  // them); padding runs have no antennas and no visibilities.
+  const size_t n_run_pad = (size_t(n_baselines) + 3) & ~size_t(3);
+  cb.run_ant.assign(n_run_pad, 0u);
+  cb.run_src.assign(n_run_pad, 0u);
+  cb.run_len.assign(n_run_pad, 0u);
   for (uint32_t r = 0; r < n_baselines; ++r) {
     const uint32_t b = order[r];
     cb.run_ant[r] = o_a1[b] | (o_a2[b] << 16);
@@ -2752,18 +3044,9 @@ int ddsolve_set_channel_block_regular(ddsolve_ctx* ctx, uint32_t cbi,
   auto sol_of = [&](uint32_t d, uint32_t t) {
     return uint32_t(uint64_t(t) * nsol[d] / n_times) + start[d];
   };
-  // Time steps folded into one slab: all that share solution indices, unless
-  // that leaves too few 224-run tiles for the SMs; then split so that the
-  // whole interval has about four tiles per SM (load balance).
-  uint32_t max_t = ctx->tune_max_times;
-  if (max_t == 0) {
-    const uint64_t tiles_per_group = (n_baselines + 223) / 224;
-    const uint64_t want = 4ull * uint64_t(ctx->n_sm);
-    const uint64_t groups_per_cb =
-        (want + uint64_t(ctx->n_cb) * tiles_per_group - 1) /
-        (uint64_t(ctx->n_cb) * tiles_per_group);
-    max_t = uint32_t(std::max<uint64_t>(1, n_times / std::max<uint64_t>(1, groups_per_cb)));
-  }
+  // Time steps folded into one slab: all that share solution indices (the
+  // pipelined kernel splits slabs along their rows for load balance).
+  const uint32_t max_t = ctx->tune_max_times ? ctx->tune_max_times : n_times;
   uint64_t off = 0;
   uint32_t t0 = 0;
   while (t0 < n_times) {
@@ -2862,6 +3145,7 @@ int ddsolve_set_channel_block(ddsolve_ctx* ctx, uint32_t cbi, uint64_t n_vis,
     s.elem_off = off;
     s.src_base = 0;
     s.tstride = 0;
+    PadRuns(cb);  // every slab's runs start on a 16-byte boundary
     s.run_off = uint32_t(cb.run_ant.size());
     s.sol.assign(kv.first.begin() + 1, kv.first.end());
     for (uint32_t m : members) {
@@ -2873,10 +3157,11 @@ int ddsolve_set_channel_block(ddsolve_ctx* ctx, uint32_t cbi, uint64_t n_vis,
     cb.slabs.push_back(std::move(s));
   }
   cb.n_elems = off;
+  PadRuns(cb);
   if (cb.run_ant.empty()) {
-    cb.run_ant.push_back(0);
-    cb.run_src.push_back(0);
-    cb.run_len.push_back(0);
+    cb.run_ant.assign(4, 0u);
+    cb.run_src.assign(4, 0u);
+    cb.run_len.assign(4, 0u);
   }
   return UploadAndPack(ctx, cb, data, model);
 }
@@ -2902,6 +3187,9 @@ int ddsolve_solve(ddsolve_ctx* ctx, double* solutions, ddsolve_result* result,
     DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.ptr, 0, 16, ctx->stream));
     if ((rc = LaunchMakeFinite(ctx, false)) != DDSOLVE_OK) return rc;
     if ((rc = LaunchBuildTables(ctx)) != DDSOLVE_OK) return rc;
+    // A solve always recomputes the model powers: they are part of solving
+    // the interval, not a result carried over from an earlier solve.
+    if ((rc = LaunchPowers(ctx, true)) != DDSOLVE_OK) return rc;
   }
   if (!ctx->graph_ok) {
     rc = BuildGraph(ctx);
@@ -2963,6 +3251,7 @@ int ddsolve_perform_iteration(ddsolve_ctx* ctx, const double* solutions,
                                         ctx->stream));
     DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.ptr, 0, 16, ctx->stream));
     if ((rc = LaunchBuildTables(ctx)) != DDSOLVE_OK) return rc;
+    if ((rc = LaunchPowers(ctx, false)) != DDSOLVE_OK) return rc;
   }
   if ((rc = LaunchIteration(ctx, true, false, false)) != DDSOLVE_OK) return rc;
   DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(next_solutions, ctx->d_next.ptr,
@@ -2987,6 +3276,7 @@ int ddsolve_time_stream_kernel(ddsolve_ctx* ctx, uint32_t n_launches, float* mea
     DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_flag.ptr, 0, size_t(ctx->n_cb) * 4,
                                         ctx->stream));
     if ((rc = LaunchBuildTables(ctx)) != DDSOLVE_OK) return rc;
+    if ((rc = LaunchPowers(ctx, false)) != DDSOLVE_OK) return rc;
     if ((rc = LaunchIteration(ctx, true, false, false)) != DDSOLVE_OK) return rc;
     DDS_CHECK_CUDA(ctx, cudaEventRecord(a, ctx->stream));
     for (uint32_t i = 0; i < n_launches; ++i)
