@@ -50,34 +50,56 @@ def _peaks():
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during a region."""
+    """Samples the SM clock and the clock-event (throttle) reasons of one GPU
+    every 20 ms during a region, through NVML (read-only queries), or through
+    nvidia-smi where NVML cannot be loaded."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,"
-              "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-              "clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,"
-              "clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40,
+               "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
 
-    def __init__(self, device):
+    def __init__(self, device, period_s=0.02):
         self.device = device
-        self.samples = []
+        self.period = period_s
+        self.samples = []  # (sm_mhz, sm_max_mhz, reasons bitmask)
         self._stop = threading.Event()
         self._thread = None
+        self._nvml = None
+
+    def _sample_nvml(self):
+        n = self._nvml
+        h = self._handle
+        sm = n.nvmlDeviceGetClockInfo(h, n.NVML_CLOCK_SM)
+        reasons = n.nvmlDeviceGetCurrentClocksEventReasons(h)
+        return (float(sm), self._max, int(reasons))
+
+    def _sample_smi(self):
+        out = subprocess.run(
+            ["nvidia-smi", "-i", str(self.device),
+             "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active",
+             "--format=csv,noheader,nounits"],
+            capture_output=True, text=True, timeout=5).stdout.strip()
+        sm, smax, act = [x.strip() for x in out.split(",")]
+        return (float(sm), float(smax), int(act, 16))
 
     def _run(self):
         while not self._stop.is_set():
             try:
-                out = subprocess.run(
-                    ["nvidia-smi", "-i", str(self.device),
-                     f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits"],
-                    capture_output=True, text=True, timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([x.strip() for x in out.split(",")])
+                self.samples.append(self._sample_nvml() if self._nvml
+                                    else self._sample_smi())
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            self._stop.wait(self.period)
 
     def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._handle = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+            self._max = float(pynvml.nvmlDeviceGetMaxClockInfo(
+                self._handle, pynvml.NVML_CLOCK_SM))
+            self._nvml = pynvml
+        except Exception:
+            self._nvml = None
         self._thread = threading.Thread(target=self._run, daemon=True)
         self._thread.start()
         return self
@@ -88,19 +110,14 @@ class ClockSampler:
 
     def summary(self):
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        smax = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
-                 "sw_power_cap"]
-        reasons = set()
-        for s in self.samples:
-            for n, v in zip(names, s[5:9]):
-                if v.strip().lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"],
+                    "samples": 0}
+        reasons = sorted({name for _, _, m in self.samples
+                          for name, bit in self.REASONS.items() if m & bit})
+        return {"sm_mhz": statistics.median(s[0] for s in self.samples),
+                "sm_max_mhz": max(s[1] for s in self.samples),
+                "reasons": reasons, "samples": len(self.samples),
+                "source": "nvml" if self._nvml else "nvidia-smi"}
 
 
 def _dist_setup():
@@ -292,11 +309,11 @@ def run_gpu_arm(args):
     peak, peak_kind = _peaks()
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "stream_kernel_traffic.json")
+    prof = os.path.join(ROOT, "profiles", f"pipe_kernel_c{args.config}_traffic.json")
     if os.path.exists(prof):
         try:
             with open(prof) as f:
-                traffic = json.load(f).get("dram_bytes_per_launch_full_size")
+                traffic = json.load(f).get("dram_bytes_per_launch")
         except Exception:
             traffic = None
 
@@ -317,7 +334,7 @@ def run_gpu_arm(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "stream_kernel", "kernel_ms": kernel_ms,
+                     "kernel": "pipe_kernel", "kernel_ms": kernel_ms,
                      "algorithmic_bytes_per_launch": alg_bytes},
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
@@ -340,7 +357,7 @@ def run_gpu_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--kernel-launches", type=int, default=20)

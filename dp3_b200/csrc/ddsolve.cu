@@ -3191,7 +3191,9 @@ int ddsolve_solve(ddsolve_ctx* ctx, double* solutions, ddsolve_result* result,
     // the interval, not a result carried over from an earlier solve.
     if ((rc = LaunchPowers(ctx, true)) != DDSOLVE_OK) return rc;
   }
-  if (!ctx->graph_ok) {
+  // DDSOLVE_NO_GRAPH: host-driven launches, one per kernel (for profilers
+  // that do not see kernels inside conditional graph nodes).
+  if (!ctx->graph_ok && !std::getenv("DDSOLVE_NO_GRAPH")) {
     rc = BuildGraph(ctx);
     if (rc != DDSOLVE_OK) {
       // Conditional graphs unavailable: fall back to host-driven launches.
@@ -3222,8 +3224,11 @@ int ddsolve_solve(ddsolve_ctx* ctx, double* solutions, ddsolve_result* result,
     DDS_CHECK_CUDA(ctx, cudaMemcpy(step_magnitudes, ctx->d_mags.ptr,
                                    size_t(ls.iteration) * 8, cudaMemcpyDeviceToHost));
   }
-  ctx->last_launches =
-      ctx->use_pipe ? uint64_t(ls.iteration) + 1 : uint64_t(ls.iteration) * 3;
+  // pipe path: make_finite + build_tables (+ power_kernel) + one pipe_kernel
+  // per iteration; else three kernels per iteration
+  ctx->last_launches = ctx->use_pipe
+                           ? uint64_t(ls.iteration) + 2 + (ctx->use_powers ? 1 : 0)
+                           : uint64_t(ls.iteration) * 3;
   if ((rc = CheckDeviceError(ctx)) != DDSOLVE_OK) return rc;
   if (result) {
     // SolverBase::MakeResult (SolverBase.cc:192-213), constraints satisfied.
@@ -3241,6 +3246,7 @@ int ddsolve_perform_iteration(ddsolve_ctx* ctx, const double* solutions,
   cudaSetDevice(ctx->device);
   int rc;
   if (ctx->plan_dirty && (rc = BuildPlan(ctx)) != DDSOLVE_OK) return rc;
+  bool powers_launched = false;
   const size_t n_sol = size_t(ctx->n_cb) * ctx->n_ant * ctx->n_sub * ctx->n_pol;
   DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->d_sol.ptr, solutions, n_sol * sizeof(double2),
                                       cudaMemcpyHostToDevice, ctx->stream));
@@ -3251,6 +3257,7 @@ int ddsolve_perform_iteration(ddsolve_ctx* ctx, const double* solutions,
                                         ctx->stream));
     DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.ptr, 0, 16, ctx->stream));
     if ((rc = LaunchBuildTables(ctx)) != DDSOLVE_OK) return rc;
+    powers_launched = ctx->use_powers && ctx->powers_dirty;
     if ((rc = LaunchPowers(ctx, false)) != DDSOLVE_OK) return rc;
   }
   if ((rc = LaunchIteration(ctx, true, false, false)) != DDSOLVE_OK) return rc;
@@ -3258,7 +3265,9 @@ int ddsolve_perform_iteration(ddsolve_ctx* ctx, const double* solutions,
                                       n_sol * sizeof(double2), cudaMemcpyDeviceToHost,
                                       ctx->stream));
   DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  ctx->last_launches = ctx->use_pipe ? 1 : 2;
+  // pipe path: build_tables (+ power_kernel) + pipe_kernel; else
+  // stream_kernel + finalize_kernel
+  ctx->last_launches = ctx->use_pipe ? 2 + (powers_launched ? 1 : 0) : 2;
   return CheckDeviceError(ctx);
 }
 
