@@ -1,0 +1,834 @@
+// Learned warm start: a three-layer perceptron trained and evaluated on the
+// B200 tensor cores. The C ABI is in include/ddwarm_b200.h.
+//
+// Every matrix product is one launch of gemm_kernel<NT>: C = A . B^T for
+// A (M x K) and B (N x K), BF16 operands, FP32 accumulation. A CTA owns a
+// 128-row tile of C (the 128 lanes of tensor memory) and NT columns; its four
+// warps stage 64-wide K chunks of A and B into shared memory in the canonical
+// K-major layout without swizzle (8 x 16-byte core matrices, 128 B apart
+// along K, 1024 B apart along M/N), double-buffered; one thread issues four
+// tcgen05.mma (kind::f16, M = 128, N = NT, K = 16) per chunk and commits them
+// to the chunk's mbarrier; the epilogue reads the accumulator with
+// tcgen05.ld (32 lanes x 32 columns per warp and instruction) and applies the
+// bias / ReLU / ReLU-derivative in FP32. Operands are read through either
+// orientation (A(m, k) = a[m * lda + k] or a[k * lda + m]), so the training
+// products (dW = dZ^T . H, dH = dZ . W) need no transposed copies.
+//
+// Waits on mbarriers are bounded (2 s of %globaltimer); a wait that runs out
+// sets an error flag, the kernel still waits (bounded) for its in-flight MMAs
+// and frees its tensor memory, and the host reports DDSOLVE_E_TIMEOUT.
+
+#include "ddwarm_b200.h"
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <numeric>
+#include <random>
+#include <string>
+#include <vector>
+
+namespace {
+
+constexpr int kGemmThreads = 128;  // four warps: one quarter of the TMEM lanes each
+constexpr int kMTile = 128;        // rows per CTA = tensor-memory lanes
+constexpr int kKChunk = 64;        // K per shared-memory stage: four MMAs of K = 16
+constexpr unsigned long long kWaitNs = 2000000000ull;
+
+enum Epilogue : int {
+  kEpiF32 = 0,       // C fp32 = acc (+ bias)
+  kEpiBf16Relu = 1,  // C bf16 = relu(acc + bias)
+  kEpiBf16Mask = 2,  // C bf16 = acc where mask > 0, else 0 (ReLU derivative)
+};
+
+struct GemmParams {
+  const uint16_t* a;  // BF16 bits
+  const uint16_t* b;
+  void* c;
+  const float* bias;     // [N] or null
+  const uint16_t* mask;  // [M][ldc] BF16 bits (kEpiBf16Mask)
+  unsigned int* error;
+  int lda, ldb, ldc;
+  int a_trans, b_trans;
+  int M, N, K;
+  int epilogue;
+};
+
+__device__ __forceinline__ uint32_t SmemAddr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long GlobalTimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void MbarInit(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(SmemAddr(bar)), "r"(count)
+               : "memory");
+}
+
+// Bounded wait for the completion of phase `parity` of `bar`.
+__device__ __forceinline__ bool MbarWait(uint64_t* bar, uint32_t parity, unsigned int* error) {
+  const uint32_t addr = SmemAddr(bar);
+  const unsigned long long t0 = GlobalTimer();
+  while (true) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n"
+        " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (GlobalTimer() - t0 > kWaitNs) {
+      atomicExch(error, 1u);
+      return false;
+    }
+  }
+}
+
+// Shared-memory matrix descriptor (tcgen05 format): start address, leading
+// (K-direction core matrix) and stride (8-row group) byte offsets, all in
+// 16-byte units; bits 46-47 = 1 (descriptor version of sm_100); base offset
+// 0; layout type 0 = no swizzle.
+__device__ __forceinline__ uint64_t SmemDesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
+         (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), A
+// and B BF16 (bits 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0),
+// N / 8 in bits 17-22, M / 16 in bits 24-28.
+__host__ __device__ constexpr uint32_t InstrDesc(int m, int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) | (uint32_t(m >> 4) << 24);
+}
+
+// Loads an R x 64 (rows x K) chunk starting at (row0, k0) into the canonical
+// K-major layout: element (r, k) at ((r / 8) * 8 + k / 8) * 128 + (r % 8) * 16
+// + (k % 8) * 2 bytes. Out-of-range elements are zero.
+template <int R>
+__device__ __forceinline__ void LoadChunk(unsigned char* dst, const uint16_t* src, int ld,
+                                          int trans, int rows, int K, int row0, int k0) {
+  constexpr int kGroups = R * (kKChunk / 8);
+  for (int g = threadIdx.x; g < kGroups; g += kGemmThreads) {
+    const int r = g >> 3, kc = g & 7;
+    const int row = row0 + r, k = k0 + kc * 8;
+    uint16_t v[8];
+    if (!trans && row < rows && k + 8 <= K && (ld & 7) == 0) {
+      const uint4 q = *reinterpret_cast<const uint4*>(src + size_t(row) * ld + k);
+      memcpy(v, &q, 16);
+    } else {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const bool in = row < rows && k + j < K;
+        v[j] = in ? (trans ? src[size_t(k + j) * ld + row] : src[size_t(row) * ld + k + j]) : 0;
+      }
+    }
+    uint4 q;
+    memcpy(&q, v, 16);
+    *reinterpret_cast<uint4*>(dst + ((r >> 3) * 8 + kc) * 128 + (r & 7) * 16) = q;
+  }
+}
+
+__device__ __forceinline__ uint16_t ToBf16(float x) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(x);
+  uint16_t u;
+  memcpy(&u, &h, 2);
+  return u;
+}
+
+__device__ __forceinline__ float FromBf16(uint16_t u) {
+  return __uint_as_float(uint32_t(u) << 16);
+}
+
+template <int NT>
+__global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmParams p) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  constexpr uint32_t kABytes = kMTile * kKChunk * 2;  // 16 KB
+  constexpr uint32_t kBBytes = NT * kKChunk * 2;
+  unsigned char* a_buf = smem;
+  unsigned char* b_buf = smem + 2 * kABytes;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + 2 * kABytes + 2 * kBBytes);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * kMTile, n0 = blockIdx.y * NT;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     SmemAddr(tmem_slot)),
+                 "r"(uint32_t(NT))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    MbarInit(&mbar[0], 1);
+    MbarInit(&mbar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  const int n_chunks = (p.K + kKChunk - 1) / kKChunk;
+  uint32_t waits[2] = {0u, 0u};  // completed waits per buffer = parity of the next
+  uint32_t commits[2] = {0u, 0u};
+  constexpr uint32_t kIdesc = InstrDesc(kMTile, NT);
+  for (int c = 0; c < n_chunks; ++c) {
+    const int b = c & 1;
+    if (commits[b] > waits[b]) {  // the MMAs of chunk c - 2 still read buffer b
+      MbarWait(&mbar[b], waits[b] & 1u, p.error);
+      ++waits[b];
+    }
+    LoadChunk<kMTile>(a_buf + b * kABytes, p.a, p.lda, p.a_trans, p.M, p.K, m0, c * kKChunk);
+    LoadChunk<NT>(b_buf + b * kBBytes, p.b, p.ldb, p.b_trans, p.N, p.K, n0, c * kKChunk);
+    // generic-proxy shared-memory writes -> visible to the tensor core (async proxy)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a_addr = SmemAddr(a_buf + b * kABytes);
+      const uint32_t b_addr = SmemAddr(b_buf + b * kBBytes);
+#pragma unroll
+      for (int s = 0; s < kKChunk / 16; ++s) {
+        const uint64_t ad = SmemDesc(a_addr + s * 256, 128, 1024);
+        const uint64_t bd = SmemDesc(b_addr + s * 256, 128, 1024);
+        const uint32_t acc = (c > 0 || s > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n .reg .pred p;\n"
+            " setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+            "l"(ad), "l"(bd), "r"(kIdesc), "r"(acc)
+            : "memory");
+      }
+      asm volatile(
+          "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+              SmemAddr(&mbar[b]))
+          : "memory");
+    }
+    ++commits[b];  // every thread tracks the commit count
+  }
+  // All MMAs done (also before freeing tensor memory after a timeout).
+  for (int b = 0; b < 2; ++b)
+    while (commits[b] > waits[b]) {
+      MbarWait(&mbar[b], waits[b] & 1u, p.error);
+      ++waits[b];
+    }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+  // Epilogue: warp w reads TMEM lanes 32w..32w+31 = rows m0 + 32w + lane.
+  const int row = m0 + warp * 32 + lane;
+  for (int col = 0; col < NT; col += 32) {
+    uint32_t r[32];
+    const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + uint32_t(col);
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+        "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+        "%28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+          "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    if (row >= p.M) continue;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const int n = n0 + col + j;
+      if (n >= p.N) break;
+      float v = __uint_as_float(r[j]);
+      if (p.bias) v += p.bias[n];
+      const size_t o = size_t(row) * p.ldc + n;
+      if (p.epilogue == kEpiF32) {
+        static_cast<float*>(p.c)[o] = v;
+      } else if (p.epilogue == kEpiBf16Relu) {
+        static_cast<uint16_t*>(p.c)[o] = ToBf16(fmaxf(v, 0.f));
+      } else {
+        static_cast<uint16_t*>(p.c)[o] = ToBf16(FromBf16(p.mask[o]) > 0.f ? v : 0.f);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(uint32_t(NT))
+                 : "memory");
+}
+
+template <int NT>
+constexpr size_t GemmSmem() {
+  return 2 * size_t(kMTile) * kKChunk * 2 + 2 * size_t(NT) * kKChunk * 2 + 64;
+}
+
+// x fp32 [n][n_in] (rows idx[i] if idx) -> bf16 [n][ld] zero-padded; target
+// fp32 [n][n_out] -> fp32 [n][ld_t] zero-padded.
+__global__ void gather_rows_kernel(const float* __restrict__ x, uint32_t n_in, const uint32_t* idx,
+                                   uint32_t n, uint16_t* __restrict__ xb, uint32_t ld,
+                                   const float* __restrict__ t, uint32_t n_out,
+                                   float* __restrict__ tb, uint32_t ld_t) {
+  const uint32_t r = blockIdx.x;
+  if (r >= n) return;
+  const uint32_t src = idx ? idx[r] : r;
+  for (uint32_t j = threadIdx.x; j < ld; j += blockDim.x)
+    xb[size_t(r) * ld + j] = ToBf16(j < n_in ? x[size_t(src) * n_in + j] : 0.f);
+  if (t)
+    for (uint32_t j = threadIdx.x; j < ld_t; j += blockDim.x)
+      tb[size_t(r) * ld_t + j] = j < n_out ? t[size_t(src) * n_out + j] : 0.f;
+}
+
+// dY = 2 (y - t) / (n * n_out) on the first n_out columns (0 elsewhere), as
+// BF16; per-block partial sums of (y - t)^2.
+__global__ void loss_grad_kernel(const float* __restrict__ y, const float* __restrict__ t,
+                                 uint32_t n, uint32_t n_out, uint32_t ld,
+                                 uint16_t* __restrict__ dy, double* __restrict__ partial) {
+  __shared__ double s[256];
+  double acc = 0.0;
+  const float scale = 2.f / (float(n) * float(n_out));
+  const size_t total = size_t(n) * ld;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += size_t(gridDim.x) * blockDim.x) {
+    const uint32_t col = uint32_t(i % ld);
+    float g = 0.f;
+    if (col < n_out) {
+      const float d = y[i] - t[i];
+      acc += double(d) * d;
+      g = scale * d;
+    }
+    dy[i] = ToBf16(g);
+  }
+  s[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (int(threadIdx.x) < w) s[threadIdx.x] += s[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = s[0];
+}
+
+__global__ void loss_sum_kernel(const double* __restrict__ partial, uint32_t n_part,
+                                double denom, float* __restrict__ loss_out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double s = 0.0;
+  for (uint32_t i = 0; i < n_part; ++i) s += partial[i];
+  *loss_out = float(s / denom);
+}
+
+// Column sums of a BF16 matrix [n][ld] (first `cols` columns) into fp32.
+__global__ void col_sum_kernel(const uint16_t* __restrict__ d, uint32_t n, uint32_t ld,
+                               uint32_t cols, float* __restrict__ out) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  float s = 0.f;
+  for (uint32_t r = 0; r < n; ++r) s += FromBf16(d[size_t(r) * ld + c]);
+  out[c] = s;
+}
+
+// Adam on the FP32 masters; refreshes the BF16 copies (padded layouts).
+struct AdamParams {
+  float* w;
+  const float* g;
+  float* m;
+  float* v;
+  uint16_t* wb;  // BF16 copy, or null (biases)
+  uint32_t rows, cols, ld;  // master/grad are [rows][ld] padded; bf16 copy same layout
+  float lr, b1, b2, eps, c1, c2;  // c1 = 1 - b1^t, c2 = 1 - b2^t
+};
+
+__global__ void adam_kernel(const AdamParams a) {
+  const size_t total = size_t(a.rows) * a.ld;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += size_t(gridDim.x) * blockDim.x) {
+    if (uint32_t(i % a.ld) >= a.cols) continue;  // padding stays zero
+    const float g = a.g[i];
+    const float m = a.b1 * a.m[i] + (1.f - a.b1) * g;
+    const float v = a.b2 * a.v[i] + (1.f - a.b2) * g * g;
+    a.m[i] = m;
+    a.v[i] = v;
+    const float w = a.w[i] - a.lr * (m / a.c1) / (sqrtf(v / a.c2) + a.eps);
+    a.w[i] = w;
+    if (a.wb) a.wb[i] = ToBf16(w);
+  }
+}
+
+__global__ void to_bf16_kernel(const float* __restrict__ w, size_t n, uint16_t* __restrict__ wb) {
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += size_t(gridDim.x) * blockDim.x)
+    wb[i] = ToBf16(w[i]);
+}
+
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() {
+    if (ptr) cudaFree(ptr);
+  }
+  cudaError_t Reserve(size_t n) {
+    if (n <= bytes && ptr) return cudaSuccess;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    const cudaError_t e = cudaMalloc(&ptr, std::max<size_t>(n, 256));
+    if (e == cudaSuccess) bytes = std::max<size_t>(n, 256);
+    return e;
+  }
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(ptr);
+  }
+};
+
+uint32_t RoundUp(uint32_t x, uint32_t m) { return (x + m - 1) / m * m; }
+
+}  // namespace
+
+// One layer's parameters in padded device layout: W [rows][ld] (rows = out,
+// ld = padded in), b [rows].
+struct Layer {
+  uint32_t out, in, rows, ld;  // logical out/in, padded rows (out) and ld (in)
+  DevBuf w, b, gw, gb, mw, vw, mb, vb, wb;
+};
+
+struct ddwarm_ctx {
+  int device = 0;
+  std::string err;
+  uint32_t n_in = 0, n_hidden = 0, n_out = 0;
+  uint32_t di = 0, dh = 0, dout = 0;  // padded widths
+  Layer L[3];
+  cudaStream_t stream = nullptr;
+  uint64_t adam_t = 0;
+  // activations for up to `cap` rows
+  uint32_t cap = 0;
+  DevBuf xb, h1, h2, y, t, dy, dz2, dz1, partial, loss, error;
+  // training data set
+  DevBuf ds_x, ds_t, ds_idx;
+
+  int Fail(int code, const std::string& m) {
+    err = m;
+    return code;
+  }
+  ~ddwarm_ctx() {
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+#define WARM_CHECK(ctx, expr)                                             \
+  do {                                                                    \
+    const cudaError_t e_ = (expr);                                        \
+    if (e_ != cudaSuccess)                                                \
+      return (ctx)->Fail(2, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+namespace {
+
+int Reserve(ddwarm_ctx* ctx, uint32_t rows) {
+  if (rows <= ctx->cap) return 0;
+  const uint32_t r = RoundUp(rows, kMTile);
+  WARM_CHECK(ctx, ctx->xb.Reserve(size_t(r) * ctx->di * 2));
+  WARM_CHECK(ctx, ctx->h1.Reserve(size_t(r) * ctx->dh * 2));
+  WARM_CHECK(ctx, ctx->h2.Reserve(size_t(r) * ctx->dh * 2));
+  WARM_CHECK(ctx, ctx->y.Reserve(size_t(r) * ctx->dout * 4));
+  WARM_CHECK(ctx, ctx->t.Reserve(size_t(r) * ctx->dout * 4));
+  WARM_CHECK(ctx, ctx->dy.Reserve(size_t(r) * ctx->dout * 2));
+  WARM_CHECK(ctx, ctx->dz2.Reserve(size_t(r) * ctx->dh * 2));
+  WARM_CHECK(ctx, ctx->dz1.Reserve(size_t(r) * ctx->dh * 2));
+  WARM_CHECK(ctx, ctx->partial.Reserve(256 * 8));
+  WARM_CHECK(ctx, ctx->loss.Reserve(8));
+  ctx->cap = r;
+  return 0;
+}
+
+int Gemm(ddwarm_ctx* ctx, const uint16_t* a, int lda, int a_trans, const uint16_t* b, int ldb,
+         int b_trans, int M, int N, int K, void* c, int ldc, const float* bias,
+         const uint16_t* mask, int epilogue) {
+  GemmParams p;
+  p.a = a;
+  p.b = b;
+  p.c = c;
+  p.bias = bias;
+  p.mask = mask;
+  p.error = ctx->error.as<unsigned int>();
+  p.lda = lda;
+  p.ldb = ldb;
+  p.ldc = ldc;
+  p.a_trans = a_trans;
+  p.b_trans = b_trans;
+  p.M = M;
+  p.N = N;
+  p.K = K;
+  p.epilogue = epilogue;
+  const uint32_t gm = (uint32_t(M) + kMTile - 1) / kMTile;
+  if (N % 256 == 0) {
+    dim3 grid(gm, uint32_t(N) / 256);
+    gemm_kernel<256><<<grid, kGemmThreads, GemmSmem<256>(), ctx->stream>>>(p);
+  } else {
+    dim3 grid(gm, (uint32_t(N) + 63) / 64);
+    gemm_kernel<64><<<grid, kGemmThreads, GemmSmem<64>(), ctx->stream>>>(p);
+  }
+  WARM_CHECK(ctx, cudaGetLastError());
+  return 0;
+}
+
+// Forward pass on the first n rows of ctx->xb: h1, h2 (BF16), y (FP32).
+int Forward(ddwarm_ctx* ctx, uint32_t n) {
+  int rc;
+  Layer& l1 = ctx->L[0];
+  Layer& l2 = ctx->L[1];
+  Layer& l3 = ctx->L[2];
+  if ((rc = Gemm(ctx, ctx->xb.as<uint16_t>(), ctx->di, 0, l1.wb.as<uint16_t>(), l1.ld, 0, n,
+                 ctx->dh, ctx->di, ctx->h1.ptr, ctx->dh, l1.b.as<float>(), nullptr,
+                 kEpiBf16Relu)))
+    return rc;
+  if ((rc = Gemm(ctx, ctx->h1.as<uint16_t>(), ctx->dh, 0, l2.wb.as<uint16_t>(), l2.ld, 0, n,
+                 ctx->dh, ctx->dh, ctx->h2.ptr, ctx->dh, l2.b.as<float>(), nullptr,
+                 kEpiBf16Relu)))
+    return rc;
+  return Gemm(ctx, ctx->h2.as<uint16_t>(), ctx->dh, 0, l3.wb.as<uint16_t>(), l3.ld, 0, n,
+              ctx->dout, ctx->dh, ctx->y.ptr, ctx->dout, l3.b.as<float>(), nullptr, kEpiF32);
+}
+
+// Loss and gradients for the first n rows of xb / t (after Forward).
+int Backward(ddwarm_ctx* ctx, uint32_t n) {
+  int rc;
+  Layer& l1 = ctx->L[0];
+  Layer& l2 = ctx->L[1];
+  Layer& l3 = ctx->L[2];
+  const uint32_t blocks = 128;
+  loss_grad_kernel<<<blocks, 256, 0, ctx->stream>>>(ctx->y.as<float>(), ctx->t.as<float>(), n,
+                                                    ctx->n_out, ctx->dout, ctx->dy.as<uint16_t>(),
+                                                    ctx->partial.as<double>());
+  loss_sum_kernel<<<1, 32, 0, ctx->stream>>>(ctx->partial.as<double>(), blocks,
+                                             double(n) * ctx->n_out, ctx->loss.as<float>());
+  WARM_CHECK(ctx, cudaGetLastError());
+  // dW3 = dY^T . H2   [dout x dh]
+  if ((rc = Gemm(ctx, ctx->dy.as<uint16_t>(), ctx->dout, 1, ctx->h2.as<uint16_t>(), ctx->dh, 1,
+                 ctx->dout, ctx->dh, n, l3.gw.ptr, l3.ld, nullptr, nullptr, kEpiF32)))
+    return rc;
+  // dZ2 = (dY . W3) * [H2 > 0]   [n x dh]
+  if ((rc = Gemm(ctx, ctx->dy.as<uint16_t>(), ctx->dout, 0, l3.wb.as<uint16_t>(), l3.ld, 1, n,
+                 ctx->dh, ctx->dout, ctx->dz2.ptr, ctx->dh, nullptr, ctx->h2.as<uint16_t>(),
+                 kEpiBf16Mask)))
+    return rc;
+  // dW2 = dZ2^T . H1
+  if ((rc = Gemm(ctx, ctx->dz2.as<uint16_t>(), ctx->dh, 1, ctx->h1.as<uint16_t>(), ctx->dh, 1,
+                 ctx->dh, ctx->dh, n, l2.gw.ptr, l2.ld, nullptr, nullptr, kEpiF32)))
+    return rc;
+  // dZ1 = (dZ2 . W2) * [H1 > 0]
+  if ((rc = Gemm(ctx, ctx->dz2.as<uint16_t>(), ctx->dh, 0, l2.wb.as<uint16_t>(), l2.ld, 1, n,
+                 ctx->dh, ctx->dh, ctx->dz1.ptr, ctx->dh, nullptr, ctx->h1.as<uint16_t>(),
+                 kEpiBf16Mask)))
+    return rc;
+  // dW1 = dZ1^T . X
+  if ((rc = Gemm(ctx, ctx->dz1.as<uint16_t>(), ctx->dh, 1, ctx->xb.as<uint16_t>(), ctx->di, 1,
+                 ctx->dh, ctx->di, n, l1.gw.ptr, l1.ld, nullptr, nullptr, kEpiF32)))
+    return rc;
+  col_sum_kernel<<<(ctx->dout + 127) / 128, 128, 0, ctx->stream>>>(
+      ctx->dy.as<uint16_t>(), n, ctx->dout, ctx->dout, l3.gb.as<float>());
+  col_sum_kernel<<<(ctx->dh + 127) / 128, 128, 0, ctx->stream>>>(
+      ctx->dz2.as<uint16_t>(), n, ctx->dh, ctx->dh, l2.gb.as<float>());
+  col_sum_kernel<<<(ctx->dh + 127) / 128, 128, 0, ctx->stream>>>(
+      ctx->dz1.as<uint16_t>(), n, ctx->dh, ctx->dh, l1.gb.as<float>());
+  WARM_CHECK(ctx, cudaGetLastError());
+  return 0;
+}
+
+int AdamStep(ddwarm_ctx* ctx, float lr) {
+  ++ctx->adam_t;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.f - std::pow(b1, float(ctx->adam_t));
+  const float c2 = 1.f - std::pow(b2, float(ctx->adam_t));
+  for (Layer& l : ctx->L) {
+    AdamParams a{l.w.as<float>(), l.gw.as<float>(), l.mw.as<float>(), l.vw.as<float>(),
+                 l.wb.as<uint16_t>(), l.rows, l.in, l.ld, lr, b1, b2, 1e-8f, c1, c2};
+    adam_kernel<<<256, 256, 0, ctx->stream>>>(a);
+    AdamParams ab{l.b.as<float>(), l.gb.as<float>(), l.mb.as<float>(), l.vb.as<float>(),
+                  nullptr, 1, l.out, l.rows, lr, b1, b2, 1e-8f, c1, c2};
+    adam_kernel<<<4, 256, 0, ctx->stream>>>(ab);
+  }
+  WARM_CHECK(ctx, cudaGetLastError());
+  return 0;
+}
+
+int CheckError(ddwarm_ctx* ctx) {
+  unsigned int e = 0;
+  WARM_CHECK(ctx, cudaMemcpyAsync(&e, ctx->error.ptr, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  WARM_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+  if (e) return ctx->Fail(5, "a bounded tensor-core wait timed out; results are invalid");
+  return 0;
+}
+
+// Host packed (logical) <-> device padded parameter copies.
+int CopyParams(ddwarm_ctx* ctx, float* host, bool to_host, bool grads) {
+  size_t off = 0;
+  std::vector<float> tmp;
+  for (Layer& l : ctx->L) {
+    DevBuf& w = grads ? l.gw : l.w;
+    DevBuf& b = grads ? l.gb : l.b;
+    tmp.assign(size_t(l.rows) * l.ld, 0.f);
+    if (to_host) {
+      WARM_CHECK(ctx, cudaMemcpyAsync(tmp.data(), w.ptr, tmp.size() * 4, cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+      WARM_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+      for (uint32_t r = 0; r < l.out; ++r)
+        memcpy(host + off + size_t(r) * l.in, tmp.data() + size_t(r) * l.ld, size_t(l.in) * 4);
+    } else {
+      for (uint32_t r = 0; r < l.out; ++r)
+        memcpy(tmp.data() + size_t(r) * l.ld, host + off + size_t(r) * l.in, size_t(l.in) * 4);
+      WARM_CHECK(ctx, cudaMemcpyAsync(w.ptr, tmp.data(), tmp.size() * 4, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+      WARM_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    off += size_t(l.out) * l.in;
+    std::vector<float> tb(l.rows, 0.f);
+    if (to_host) {
+      WARM_CHECK(ctx, cudaMemcpyAsync(tb.data(), b.ptr, tb.size() * 4, cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+      WARM_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+      memcpy(host + off, tb.data(), size_t(l.out) * 4);
+    } else {
+      memcpy(tb.data(), host + off, size_t(l.out) * 4);
+      WARM_CHECK(ctx, cudaMemcpyAsync(b.ptr, tb.data(), tb.size() * 4, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+      WARM_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    off += l.out;
+    if (!to_host && !grads) {
+      to_bf16_kernel<<<64, 256, 0, ctx->stream>>>(l.w.as<float>(), size_t(l.rows) * l.ld,
+                                                  l.wb.as<uint16_t>());
+      WARM_CHECK(ctx, cudaGetLastError());
+    }
+  }
+  return 0;
+}
+
+int Upload(ddwarm_ctx* ctx, DevBuf& dst, const void* src, size_t bytes) {
+  WARM_CHECK(ctx, dst.Reserve(bytes));
+  WARM_CHECK(ctx, cudaMemcpyAsync(dst.ptr, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ddwarm_create(uint32_t n_in, uint32_t n_hidden, uint32_t n_out, uint64_t seed, int device,
+                  ddwarm_ctx** out) {
+  if (!out) return 1;
+  *out = nullptr;
+  if (n_in == 0 || n_in > 256 || n_out == 0 || n_out > 256 || n_hidden < 64 ||
+      n_hidden > 256 || n_hidden % 64)
+    return 1;
+  int n_dev = 0;
+  if (cudaGetDeviceCount(&n_dev) != cudaSuccess || device < 0 || device >= n_dev) return 2;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return 2;
+  if (prop.major != 10) return 4;  // tcgen05 needs an sm_100-class device
+  auto* ctx = new ddwarm_ctx();
+  ctx->device = device;
+  cudaSetDevice(device);
+  ctx->n_in = n_in;
+  ctx->n_hidden = n_hidden;
+  ctx->n_out = n_out;
+  ctx->di = RoundUp(n_in, 64);
+  ctx->dh = n_hidden;
+  ctx->dout = RoundUp(n_out, 64);
+  const uint32_t outs[3] = {n_hidden, n_hidden, n_out};
+  const uint32_t ins[3] = {n_in, n_hidden, n_hidden};
+  const uint32_t rows[3] = {ctx->dh, ctx->dh, ctx->dout};
+  const uint32_t lds[3] = {ctx->di, ctx->dh, ctx->dh};
+  int rc = 0;
+  auto fail = [&](int code) {
+    delete ctx;
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(2);
+  if (cudaFuncSetAttribute(gemm_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           int(GemmSmem<256>())) != cudaSuccess ||
+      cudaFuncSetAttribute(gemm_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           int(GemmSmem<64>())) != cudaSuccess)
+    return fail(2);
+  std::mt19937_64 rng(seed);
+  for (int i = 0; i < 3; ++i) {
+    Layer& l = ctx->L[i];
+    l.out = outs[i];
+    l.in = ins[i];
+    l.rows = rows[i];
+    l.ld = lds[i];
+    const size_t nw = size_t(l.rows) * l.ld;
+    for (DevBuf* b : {&l.w, &l.gw, &l.mw, &l.vw})
+      if (b->Reserve(nw * 4) != cudaSuccess) return fail(2);
+    if (l.wb.Reserve(nw * 2) != cudaSuccess) return fail(2);
+    for (DevBuf* b : {&l.b, &l.gb, &l.mb, &l.vb})
+      if (b->Reserve(size_t(l.rows) * 4) != cudaSuccess) return fail(2);
+    for (DevBuf* b : {&l.w, &l.gw, &l.mw, &l.vw, &l.b, &l.gb, &l.mb, &l.vb})
+      cudaMemsetAsync(b->ptr, 0, b->bytes, ctx->stream);
+    cudaMemsetAsync(l.wb.ptr, 0, l.wb.bytes, ctx->stream);
+  }
+  // He-uniform weights (bound sqrt(6 / fan_in)), last layer scaled by 0.1 so
+  // that the untrained network predicts small corrections.
+  std::vector<float> params(ddwarm_param_count(ctx), 0.f);
+  size_t off = 0;
+  for (int i = 0; i < 3; ++i) {
+    const Layer& l = ctx->L[i];
+    const double bound = std::sqrt(6.0 / l.in) * (i == 2 ? 0.1 : 1.0);
+    for (size_t k = 0; k < size_t(l.out) * l.in; ++k) {
+      const double u = double(rng() >> 11) * (1.0 / 9007199254740992.0);  // [0, 1)
+      params[off + k] = float((2.0 * u - 1.0) * bound);
+    }
+    off += size_t(l.out) * l.in + l.out;
+  }
+  if (ctx->error.Reserve(16) != cudaSuccess) return fail(2);
+  cudaMemsetAsync(ctx->error.ptr, 0, 16, ctx->stream);
+  if ((rc = CopyParams(ctx, params.data(), false, false))) return fail(rc);
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return fail(2);
+  *out = ctx;
+  return 0;
+}
+
+void ddwarm_destroy(ddwarm_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  delete ctx;
+}
+
+const char* ddwarm_last_error(const ddwarm_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+uint64_t ddwarm_param_count(const ddwarm_ctx* ctx) {
+  if (!ctx) return 0;
+  uint64_t n = 0;
+  for (const Layer& l : ctx->L) n += uint64_t(l.out) * l.in + l.out;
+  return n;
+}
+
+int ddwarm_get_params(ddwarm_ctx* ctx, float* params) {
+  if (!ctx || !params) return 1;
+  cudaSetDevice(ctx->device);
+  return CopyParams(ctx, params, true, false);
+}
+
+int ddwarm_set_params(ddwarm_ctx* ctx, const float* params) {
+  if (!ctx || !params) return 1;
+  cudaSetDevice(ctx->device);
+  ctx->adam_t = 0;
+  for (Layer& l : ctx->L)
+    for (DevBuf* b : {&l.mw, &l.vw, &l.mb, &l.vb}) cudaMemsetAsync(b->ptr, 0, b->bytes, ctx->stream);
+  return CopyParams(ctx, const_cast<float*>(params), false, false);
+}
+
+int ddwarm_predict(ddwarm_ctx* ctx, uint32_t n, const float* x, float* y) {
+  if (!ctx || (n && (!x || !y))) return 1;
+  if (n == 0) return 0;
+  cudaSetDevice(ctx->device);
+  int rc;
+  if ((rc = Reserve(ctx, n))) return rc;
+  if ((rc = Upload(ctx, ctx->ds_x, x, size_t(n) * ctx->n_in * 4))) return rc;
+  gather_rows_kernel<<<n, 128, 0, ctx->stream>>>(ctx->ds_x.as<float>(), ctx->n_in, nullptr, n,
+                                                 ctx->xb.as<uint16_t>(), ctx->di, nullptr, 0,
+                                                 nullptr, 0);
+  WARM_CHECK(ctx, cudaGetLastError());
+  if ((rc = Forward(ctx, n))) return rc;
+  std::vector<float> tmp(size_t(n) * ctx->dout);
+  WARM_CHECK(ctx, cudaMemcpyAsync(tmp.data(), ctx->y.ptr, tmp.size() * 4, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+  if ((rc = CheckError(ctx))) return rc;
+  for (uint32_t r = 0; r < n; ++r)
+    memcpy(y + size_t(r) * ctx->n_out, tmp.data() + size_t(r) * ctx->dout, size_t(ctx->n_out) * 4);
+  return 0;
+}
+
+int ddwarm_gradients(ddwarm_ctx* ctx, uint32_t n, const float* x, const float* target,
+                     float* grads, float* loss) {
+  if (!ctx || n == 0 || !x || !target || !grads) return 1;
+  cudaSetDevice(ctx->device);
+  int rc;
+  if ((rc = Reserve(ctx, n))) return rc;
+  if ((rc = Upload(ctx, ctx->ds_x, x, size_t(n) * ctx->n_in * 4))) return rc;
+  if ((rc = Upload(ctx, ctx->ds_t, target, size_t(n) * ctx->n_out * 4))) return rc;
+  gather_rows_kernel<<<n, 128, 0, ctx->stream>>>(ctx->ds_x.as<float>(), ctx->n_in, nullptr, n,
+                                                 ctx->xb.as<uint16_t>(), ctx->di,
+                                                 ctx->ds_t.as<float>(), ctx->n_out,
+                                                 ctx->t.as<float>(), ctx->dout);
+  WARM_CHECK(ctx, cudaGetLastError());
+  if ((rc = Forward(ctx, n))) return rc;
+  if ((rc = Backward(ctx, n))) return rc;
+  if ((rc = CheckError(ctx))) return rc;
+  if ((rc = CopyParams(ctx, grads, true, true))) return rc;
+  if (loss) {
+    WARM_CHECK(ctx, cudaMemcpyAsync(loss, ctx->loss.ptr, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    WARM_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return 0;
+}
+
+int ddwarm_train(ddwarm_ctx* ctx, uint32_t n, const float* x, const float* target,
+                 uint32_t epochs, uint32_t batch, float lr, uint64_t seed, float* epoch_loss) {
+  if (!ctx || n == 0 || !x || !target || batch == 0) return 1;
+  cudaSetDevice(ctx->device);
+  int rc;
+  batch = std::min(batch, n);
+  if ((rc = Reserve(ctx, batch))) return rc;
+  if ((rc = Upload(ctx, ctx->ds_x, x, size_t(n) * ctx->n_in * 4))) return rc;
+  if ((rc = Upload(ctx, ctx->ds_t, target, size_t(n) * ctx->n_out * 4))) return rc;
+  WARM_CHECK(ctx, ctx->ds_idx.Reserve(size_t(n) * 4));
+  DevBuf losses;
+  const uint32_t steps_per_epoch = (n + batch - 1) / batch;
+  WARM_CHECK(ctx, losses.Reserve(size_t(std::max<uint32_t>(epochs, 1)) * steps_per_epoch * 4));
+  std::mt19937_64 rng(seed);
+  std::vector<uint32_t> order(n);
+  std::iota(order.begin(), order.end(), 0u);
+  std::vector<uint32_t> all(size_t(epochs) * n);
+  for (uint32_t e = 0; e < epochs; ++e) {
+    // Fisher-Yates with explicit draws (no implementation-defined shuffle)
+    for (uint32_t i = n - 1; i > 0; --i) {
+      const uint32_t j = uint32_t(rng() % (uint64_t(i) + 1));
+      std::swap(order[i], order[j]);
+    }
+    std::copy(order.begin(), order.end(), all.begin() + size_t(e) * n);
+  }
+  DevBuf idx_all;
+  if ((rc = Upload(ctx, idx_all, all.data(), all.size() * 4))) return rc;
+  for (uint32_t e = 0; e < epochs; ++e) {
+    for (uint32_t s = 0; s < steps_per_epoch; ++s) {
+      const uint32_t r0 = s * batch;
+      const uint32_t nb = std::min(batch, n - r0);
+      gather_rows_kernel<<<nb, 128, 0, ctx->stream>>>(
+          ctx->ds_x.as<float>(), ctx->n_in, idx_all.as<uint32_t>() + size_t(e) * n + r0, nb,
+          ctx->xb.as<uint16_t>(), ctx->di, ctx->ds_t.as<float>(), ctx->n_out,
+          ctx->t.as<float>(), ctx->dout);
+      WARM_CHECK(ctx, cudaGetLastError());
+      if ((rc = Forward(ctx, nb))) return rc;
+      if ((rc = Backward(ctx, nb))) return rc;
+      WARM_CHECK(ctx, cudaMemcpyAsync(losses.as<float>() + size_t(e) * steps_per_epoch + s,
+                                      ctx->loss.ptr, 4, cudaMemcpyDeviceToDevice, ctx->stream));
+      if ((rc = AdamStep(ctx, lr))) return rc;
+    }
+  }
+  if ((rc = CheckError(ctx))) return rc;
+  if (epoch_loss && epochs) {
+    std::vector<float> l(size_t(epochs) * steps_per_epoch);
+    WARM_CHECK(ctx, cudaMemcpyAsync(l.data(), losses.ptr, l.size() * 4, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+    WARM_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+    for (uint32_t e = 0; e < epochs; ++e) {
+      double s = 0.0;
+      for (uint32_t k = 0; k < steps_per_epoch; ++k) s += l[size_t(e) * steps_per_epoch + k];
+      epoch_loss[e] = float(s / steps_per_epoch);
+    }
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -186,6 +186,39 @@ def frequencies(cfg: ObservationConfig):
     return f
 
 
+def gain_sequence(cfg: ObservationConfig, n_intervals, seed=None, phase_sigma=0.05,
+                  amp_sigma=0.01, dispersive_sigma=0.05):
+    """True gains of `n_intervals` consecutive solution intervals,
+    [n_intervals, n_channels, n_stations, n_directions, 2] complex128.
+
+    Interval 0 has the gains of `gains(cfg)`. From one interval to the next,
+    per station, direction and polarization the phase takes a Gaussian
+    random-walk step (phase_sigma rad) and the log-amplitude one of
+    amp_sigma (lognormal drift); per station and direction a dispersive phase
+    kappa * nu_mid / nu is added whose coefficient kappa random-walks with
+    steps of dispersive_sigma rad (at the band centre nu_mid). Seeded
+    numpy PCG64 streams."""
+    g0 = gains(cfg)
+    rng = np.random.Generator(np.random.PCG64(cfg.seed * 7 + 3 if seed is None else seed))
+    freqs = frequencies(cfg)
+    nu_mid = 0.5 * (cfg.freq_lo_hz + cfg.freq_hi_hz)
+    ns, nd = cfg.n_stations, cfg.n_directions
+    phase = np.zeros((ns, nd, 2))
+    logamp = np.zeros((ns, nd, 2))
+    kappa = np.zeros((ns, nd))
+    out = np.zeros((n_intervals,) + g0.shape, np.complex128)
+    disp_shape = (nu_mid / freqs)[:, None, None, None]
+    for i in range(n_intervals):
+        if i > 0:
+            phase += rng.normal(0.0, phase_sigma, phase.shape)
+            logamp += rng.normal(0.0, amp_sigma, logamp.shape)
+            kappa += rng.normal(0.0, dispersive_sigma, kappa.shape)
+        drift = np.exp(logamp + 1j * phase)[None, :, :, :]
+        disp = np.exp(1j * kappa[None, :, :, None] * disp_shape)
+        out[i] = g0 * drift * disp
+    return out
+
+
 def _alloc(shape, pinned):
     if pinned:
         import torch

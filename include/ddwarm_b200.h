@@ -1,0 +1,76 @@
+/*
+ * ddwarm_b200 — learned warm start for the direction-iterative gain solver.
+ *
+ * A three-layer perceptron (n_in -> n_hidden -> n_hidden -> n_out, ReLU)
+ * whose forward and training passes run on the B200's 5th-generation tensor
+ * cores (tcgen05.mma, BF16 operands, FP32 accumulation in tensor memory). In
+ * the solver it maps, per (antenna, direction), the last solutions and the
+ * current interval's one-pass residual statistics to the initial gains of the
+ * new interval; the solver then iterates to the same tolerance as without it,
+ * so only the iteration count changes.
+ *
+ * The reference (DP3 DDECal) has no learned component: none of these entry
+ * points replaces a reference interface. Its nearest counterpart is the
+ * solution propagation of DDECal (steps/DDECal.cc, `propagatesolutions`),
+ * which starts an interval from the previous interval's solutions; this
+ * network is an alternative source of those initial solutions, passed to
+ * ddsolve_solve (include/ddsolve_b200.h) exactly as propagated ones are.
+ *
+ * Parameters are FP32 masters (Adam state in FP32) with BF16 copies used by
+ * the tensor cores. Packed parameter order (FP32, logical shapes, row-major):
+ *   W1 [n_hidden][n_in], b1 [n_hidden], W2 [n_hidden][n_hidden],
+ *   b2 [n_hidden], W3 [n_out][n_hidden], b3 [n_out].
+ * Loss: mean over rows and outputs of (y - target)^2.
+ *
+ * Status codes as in ddsolve_b200.h (0 ok, 1 invalid, 2 CUDA, 4 unsupported,
+ * 5 a bounded device wait ran out).
+ */
+#ifndef DDWARM_B200_H
+#define DDWARM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#ifndef DDSOLVE_API
+#define DDSOLVE_API __attribute__((visibility("default")))
+#endif
+
+typedef struct ddwarm_ctx ddwarm_ctx;
+
+/* n_in, n_out in [1, 256]; n_hidden a multiple of 64 in [64, 256].
+ * Weights: He-uniform from std::mt19937_64(seed), biases zero. */
+DDSOLVE_API int ddwarm_create(uint32_t n_in, uint32_t n_hidden, uint32_t n_out,
+                              uint64_t seed, int device, ddwarm_ctx** out);
+DDSOLVE_API void ddwarm_destroy(ddwarm_ctx* ctx);
+DDSOLVE_API const char* ddwarm_last_error(const ddwarm_ctx* ctx);
+
+/* Number of packed FP32 parameters. */
+DDSOLVE_API uint64_t ddwarm_param_count(const ddwarm_ctx* ctx);
+DDSOLVE_API int ddwarm_get_params(ddwarm_ctx* ctx, float* params);
+DDSOLVE_API int ddwarm_set_params(ddwarm_ctx* ctx, const float* params);
+
+/* Forward pass: x [n][n_in] -> y [n][n_out], host FP32 buffers. */
+DDSOLVE_API int ddwarm_predict(ddwarm_ctx* ctx, uint32_t n, const float* x, float* y);
+
+/* Loss and its gradient for one batch (no update): grads packed as the
+ * parameters. For checking the training kernels. */
+DDSOLVE_API int ddwarm_gradients(ddwarm_ctx* ctx, uint32_t n, const float* x,
+                                 const float* target, float* grads, float* loss);
+
+/* Trains on the data set x [n][n_in], target [n][n_out] (host FP32, uploaded
+ * once): `epochs` passes of shuffled mini-batches of `batch` rows (the order
+ * from std::mt19937_64(seed)), Adam (beta 0.9 / 0.999, eps 1e-8) at learning
+ * rate `lr`. epoch_loss[e] (optional, `epochs` entries) receives the mean
+ * batch loss of epoch e. */
+DDSOLVE_API int ddwarm_train(ddwarm_ctx* ctx, uint32_t n, const float* x,
+                             const float* target, uint32_t epochs, uint32_t batch,
+                             float lr, uint64_t seed, float* epoch_loss);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
