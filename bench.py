@@ -172,6 +172,118 @@ def cpu_baseline_port(cfg, obs, iterations_per_interval, budget_s=20.0):
                       f"{iterations_per_interval} iterations"}
 
 
+def _max_rel_diff(a, b):
+    """max |a - b| / |b| over finite elements after referencing both to
+    antenna 0's phase (per channel block, sub-solution, polarization)."""
+    def ref(s):
+        r = s[:, :1]
+        ph = np.where(np.abs(r) > 0, r / np.abs(r), 1.0)
+        return s * np.conj(ph)
+    ar, br = ref(a), ref(b)
+    with np.errstate(all="ignore"):
+        return float(np.nanmax(np.abs(ar - br) / np.maximum(np.abs(br), 1e-30)))
+
+
+def run_warm_start(args, device):
+    """Learned warm start vs previous-solution start on the random-walk
+    sequence: 62 stations, 10 directions, 120 channels / 12 blocks, 2
+    timesteps per interval, `args.warm_intervals` intervals; the networks are
+    trained on the plain solver's solutions of the first half and evaluated on
+    the second half. Per evaluated interval (data resident on the GPU, wall
+    clock around the whole start + solve, each path from its own previous
+    solutions): plain = solve from the previous solutions (host arrays, as a
+    DDECal caller passes them); warm = two-stage network start (including its
+    undamped feature passes) + solve, with the solutions kept on the GPU."""
+    import torch
+    from dp3_b200 import ddsolve, synth, warmstart
+    cfg = synth.benchmark_configs()[4]
+    n_int = args.warm_intervals
+    n_train = n_int // 2
+    seq = synth.gain_sequence(cfg, n_int)
+    n_sub = sum(cfg.nspd)
+    ctx = ddsolve.Context(cfg.n_stations, cfg.nspd, cfg.n_channel_blocks, 2, 2, device=device)
+    st = ddsolve.default_settings()
+    st.max_iterations = 100
+    st.accuracy = cfg.tolerance
+    st.step_size = cfg.step_size
+    ctx.set_settings(st)
+    tight = ddsolve.default_settings()
+    tight.max_iterations, tight.accuracy, tight.step_size = 400, 1e-8, cfg.step_size
+    tight.detect_stalling = 0
+    tight_plain = tight_warm = 0.0
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=f"cuda:{device}")
+    ws = warmstart.LearnedWarmStart(cfg.n_channel_blocks, cfg.n_stations, n_sub, 2,
+                                    passes=(3, 3), provisional_after=max(8, n_train * 3 // 8),
+                                    device=device)
+    unit = np.ones((cfg.n_channel_blocks, cfg.n_stations, n_sub, 2), np.complex128)
+    dev = torch.device(f"cuda:{device}")
+    plain_hist = [unit] * 4
+    warm_hist = [torch.from_numpy(unit).to(dev)] * 4  # the warm path stays on the GPU
+    t_plain, t_warm, it_plain, it_warm, worst = [], [], [], [], 0.0
+    t_train = 0.0
+    for i in range(n_int):
+        obs = synth.observe(cfg, true_gains=seq[i], start_time_s=i * cfg.n_times * cfg.time_step_s,
+                            noise_seed=cfg.seed * 31 + i)
+        for cb, nc in enumerate(cfg.cb_channels):
+            ctx.set_channel_block_regular(cb, cfg.n_times, cfg.n_baselines, nc, obs.data[cb],
+                                          obs.model[cb], obs.antenna1, obs.antenna2)
+        stream.synchronize()  # upload and repack done before the clock starts
+        t0 = time.perf_counter()
+        s = plain_hist[0].copy()
+        r = ctx.solve(s)
+        t1 = time.perf_counter()
+        if i < n_train:
+            if i >= 4:
+                t2 = time.perf_counter()
+                ws.add_interval(ctx, plain_hist, s)
+                t_train += time.perf_counter() - t2
+            if i == n_train - 1:
+                t2 = time.perf_counter()
+                ws.fit()
+                t_train += time.perf_counter() - t2
+            warm_hist = [torch.from_numpy(s).to(dev)] + warm_hist[:3]
+        else:
+            t_plain.append(t1 - t0)
+            it_plain.append(r.iterations)
+            t2 = time.perf_counter()
+            g_dev = ws.start(ctx, warm_hist)
+            rw = ctx.solve(g_dev)
+            t_warm.append(time.perf_counter() - t2)
+            it_warm.append(rw.iterations)
+            g = g_dev.cpu().numpy()
+            worst = max(worst, _max_rel_diff(g, s))
+            if len(t_warm) <= args.warm_tight:
+                # distance of both answers to a tight-tolerance solve
+                ref = s.copy()
+                ctx.set_settings(tight)
+                ctx.solve(ref)
+                ctx.set_settings(st)
+                tight_plain = max(tight_plain, _max_rel_diff(s, ref))
+                tight_warm = max(tight_warm, _max_rel_diff(g, ref))
+            warm_hist = [g_dev] + warm_hist[:3]
+        plain_hist = [s] + plain_hist[:3]
+    passes = ws.passes
+    ws.close()
+    ctx.close()
+    plain_s, warm_s = float(np.mean(t_plain)), float(np.mean(t_warm))
+    return {
+        "workload": ("62 stations, 10 directions, 120 channels / 12 blocks, 2 timesteps per "
+                     f"interval, {n_int} random-walk intervals (trained on the first "
+                     f"{n_train}, evaluated on the last {n_int - n_train})"),
+        "plain_s_per_interval": plain_s, "warm_s_per_interval": warm_s,
+        "speedup": plain_s / warm_s,
+        "plain_iterations": float(np.mean(it_plain)),
+        "warm_iterations": float(np.mean(it_warm)),
+        "warm_feature_passes": passes,
+        "max_rel_diff_vs_plain": worst,
+        "max_rel_diff_vs_tight_solve": {"plain": tight_plain, "warm": tight_warm,
+                                        "intervals": min(args.warm_tight, len(t_warm)),
+                                        "tight_accuracy": 1e-8},
+        "train_s": t_train,
+        "network": "2 stages x (n_in -> 256 -> 256 -> 48), BF16 on tcgen05, FP32 accumulation",
+    }
+
+
 def run_reference_arm(args):
     world, rank, local = _dist_setup()
     if rank != 0:
@@ -339,6 +451,8 @@ def run_gpu_arm(args):
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
     }
+    if rank == 0 and world == 1 and args.warm_intervals > 0:
+        result["warm_start"] = run_warm_start(args, device)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle_ffi as of
         of.build()
@@ -368,6 +482,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--config", type=int, default=CONFIG_INDEX,
                     help="benchmark configuration index (synth.benchmark_configs)")
+    ap.add_argument("--warm-intervals", type=int, default=200,
+                    help="intervals of the learned-warm-start sequence (0: skip)")
+    ap.add_argument("--warm-tight", type=int, default=20,
+                    help="evaluated intervals also solved to tolerance 1e-8 for accuracy")
     ap.add_argument("--pass-only", action="store_true",
                     help="time only the streaming pass (for profiling)")
     args = ap.parse_args()

@@ -1873,12 +1873,22 @@ struct ddsolve_ctx {
       d_fin_visits, d_dir_of_sub, d_block_sum, d_block_cnt;
   // solver state
   DevBuf d_sol, d_next, d_state, d_nonfinite, d_mags, d_settings;
+  DevBuf d_chain;  // outputs of ddsolve_perform_iterations
   // graph
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   cudaGraphConditionalHandle handle = 0;
   bool graph_ok = false;
   uint64_t last_launches = 0;
+  // Pinned host staging of the per-call read-backs (error counters, loop
+  // state, step magnitudes), copied before the call's single synchronization.
+  struct HostStage {
+    uint32_t counters[4];
+    LoopState ls;
+    double mags[1];  // [mags_cap]
+  };
+  HostStage* h_stage = nullptr;
+  size_t mags_cap = 0;
 
   int Fail(int code, const std::string& msg) {
     err = msg;
@@ -1888,6 +1898,19 @@ struct ddsolve_ctx {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
     if (stream) cudaStreamDestroy(stream);
+    if (h_stage) cudaFreeHost(h_stage);
+  }
+  cudaError_t ReserveStage(size_t n_mags) {
+    if (h_stage && n_mags <= mags_cap) return cudaSuccess;
+    if (h_stage) cudaFreeHost(h_stage);
+    h_stage = nullptr;
+    const size_t cap = std::max<size_t>(n_mags, 64);
+    void* p = nullptr;
+    const cudaError_t e = cudaMallocHost(&p, sizeof(HostStage) + cap * sizeof(double));
+    if (e != cudaSuccess) return e;
+    h_stage = static_cast<HostStage*>(p);
+    mags_cap = cap;
+    return cudaSuccess;
   }
   void DestroyGraph() {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -2701,8 +2724,8 @@ int LaunchBuildTables(ddsolve_ctx* ctx) {
   return DDSOLVE_OK;
 }
 
-// Model powers of the pipelined path, when the plan uses them and the model
-// changed since they were last computed (or `force`).
+// Model powers of the pipelined path, when the plan uses them and they are
+// stale (new data, or a solve used them since), or `force`.
 int LaunchPowers(ddsolve_ctx* ctx, bool force) {
   if (!ctx->use_pipe || !ctx->use_powers || (!ctx->powers_dirty && !force)) return DDSOLVE_OK;
   const uint32_t blocks = ctx->n_power_tiles * ctx->n_dir;
@@ -2776,10 +2799,26 @@ int LaunchIteration(ddsolve_ctx* ctx, bool host_mode, bool use_handle,
   return DDSOLVE_OK;
 }
 
-int CheckDeviceError(ddsolve_ctx* ctx) {
+// Enqueues the copy of the device error counters into the pinned stage (read
+// by CheckDeviceError after the call's synchronization).
+int StageCounters(ddsolve_ctx* ctx) {
+  if (!ctx->use_pipe) return DDSOLVE_OK;
+  DDS_CHECK_CUDA(ctx, ctx->ReserveStage(0));
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage->counters, ctx->d_counters.ptr, 16,
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+  return DDSOLVE_OK;
+}
+
+// After the stream was synchronized: `staged` = the counters were copied by
+// StageCounters in this call; otherwise they are read here.
+int CheckDeviceError(ddsolve_ctx* ctx, bool staged = false) {
   if (!ctx->use_pipe) return DDSOLVE_OK;
   uint32_t c[2] = {0, 0};
-  DDS_CHECK_CUDA(ctx, cudaMemcpy(c, ctx->d_counters.ptr, 8, cudaMemcpyDeviceToHost));
+  if (staged) {
+    c[1] = ctx->h_stage->counters[1];
+  } else {
+    DDS_CHECK_CUDA(ctx, cudaMemcpy(c, ctx->d_counters.ptr, 8, cudaMemcpyDeviceToHost));
+  }
   if (c[1] != 0) {
     cudaMemsetAsync(ctx->d_counters.ptr, 0, 16, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
@@ -3171,10 +3210,11 @@ int ddsolve_solve(ddsolve_ctx* ctx, double* solutions, ddsolve_result* result,
   if (!ctx || !solutions) return DDSOLVE_E_INVALID;
   cudaSetDevice(ctx->device);
   int rc;
+  bool solve_powers = false;
   if (ctx->plan_dirty && (rc = BuildPlan(ctx)) != DDSOLVE_OK) return rc;
   const size_t n_sol = size_t(ctx->n_cb) * ctx->n_ant * ctx->n_sub * ctx->n_pol;
   DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->d_sol.ptr, solutions, n_sol * sizeof(double2),
-                                      cudaMemcpyHostToDevice, ctx->stream));
+                                      cudaMemcpyDefault, ctx->stream));
   DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_state.ptr, 0, sizeof(LoopState), ctx->stream));
   DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_nonfinite.ptr, 1, size_t(ctx->n_cb) * 4,
                                       ctx->stream));
@@ -3187,9 +3227,11 @@ int ddsolve_solve(ddsolve_ctx* ctx, double* solutions, ddsolve_result* result,
     DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.ptr, 0, 16, ctx->stream));
     if ((rc = LaunchMakeFinite(ctx, false)) != DDSOLVE_OK) return rc;
     if ((rc = LaunchBuildTables(ctx)) != DDSOLVE_OK) return rc;
-    // A solve always recomputes the model powers: they are part of solving
-    // the interval, not a result carried over from an earlier solve.
-    if ((rc = LaunchPowers(ctx, true)) != DDSOLVE_OK) return rc;
+    // The model powers are part of solving the interval: a solve recomputes
+    // them unless a ddsolve_perform_iteration[s] call computed them on the
+    // same data since the last solve, and leaves them stale for the next.
+    solve_powers = ctx->use_powers && ctx->powers_dirty;
+    if ((rc = LaunchPowers(ctx, false)) != DDSOLVE_OK) return rc;
   }
   // DDSOLVE_NO_GRAPH: host-driven launches, one per kernel (for profilers
   // that do not see kernels inside conditional graph nodes).
@@ -3202,10 +3244,19 @@ int ddsolve_solve(ddsolve_ctx* ctx, double* solutions, ddsolve_result* result,
     }
   }
   LoopState ls{};
+  const size_t n_mags = std::max(std::max(ctx->settings.max_iterations,
+                                          ctx->settings.min_iterations), 1u);
+  DDS_CHECK_CUDA(ctx, ctx->ReserveStage(n_mags));
+  bool staged = false;
   if (ctx->graph_ok) {
     DDS_CHECK_CUDA(ctx, cudaGraphLaunch(ctx->graph_exec, ctx->stream));
-    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(&ls, ctx->d_state.ptr, sizeof(ls),
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(&ctx->h_stage->ls, ctx->d_state.ptr, sizeof(ls),
                                         cudaMemcpyDeviceToHost, ctx->stream));
+    if (step_magnitudes)
+      DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->h_stage->mags, ctx->d_mags.ptr, n_mags * 8,
+                                          cudaMemcpyDeviceToHost, ctx->stream));
+    if ((rc = StageCounters(ctx)) != DDSOLVE_OK) return rc;
+    staged = true;
   } else {
     const uint32_t cap = std::max(std::max(ctx->settings.max_iterations,
                                            ctx->settings.min_iterations), 1u);
@@ -3218,18 +3269,26 @@ int ddsolve_solve(ddsolve_ctx* ctx, double* solutions, ddsolve_result* result,
     }
   }
   DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(solutions, ctx->d_sol.ptr, n_sol * sizeof(double2),
-                                      cudaMemcpyDeviceToHost, ctx->stream));
+                                      cudaMemcpyDefault, ctx->stream));
   DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (staged) ls = ctx->h_stage->ls;
   if (step_magnitudes && ls.iteration > 0) {
-    DDS_CHECK_CUDA(ctx, cudaMemcpy(step_magnitudes, ctx->d_mags.ptr,
-                                   size_t(ls.iteration) * 8, cudaMemcpyDeviceToHost));
+    if (staged) {
+      memcpy(step_magnitudes, ctx->h_stage->mags,
+             std::min<size_t>(ls.iteration, n_mags) * 8);
+    } else {
+      DDS_CHECK_CUDA(ctx, cudaMemcpy(step_magnitudes, ctx->d_mags.ptr,
+                                     size_t(ls.iteration) * 8, cudaMemcpyDeviceToHost));
+    }
   }
   // pipe path: make_finite + build_tables (+ power_kernel) + one pipe_kernel
   // per iteration; else three kernels per iteration
   ctx->last_launches = ctx->use_pipe
-                           ? uint64_t(ls.iteration) + 2 + (ctx->use_powers ? 1 : 0)
+                           ? uint64_t(ls.iteration) + 2 + (solve_powers ? 1 : 0)
                            : uint64_t(ls.iteration) * 3;
-  if ((rc = CheckDeviceError(ctx)) != DDSOLVE_OK) return rc;
+  // the model powers are fresh for one solve only (see LaunchPowers)
+  ctx->powers_dirty = true;
+  if ((rc = CheckDeviceError(ctx, staged)) != DDSOLVE_OK) return rc;
   if (result) {
     // SolverBase::MakeResult (SolverBase.cc:192-213), constraints satisfied.
     result->iterations = ls.has_converged ? ls.iteration : ls.iteration + 1;
@@ -3249,7 +3308,7 @@ int ddsolve_perform_iteration(ddsolve_ctx* ctx, const double* solutions,
   bool powers_launched = false;
   const size_t n_sol = size_t(ctx->n_cb) * ctx->n_ant * ctx->n_sub * ctx->n_pol;
   DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->d_sol.ptr, solutions, n_sol * sizeof(double2),
-                                      cudaMemcpyHostToDevice, ctx->stream));
+                                      cudaMemcpyDefault, ctx->stream));
   if (ctx->use_pipe) {
     DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_flag.ptr, 0, size_t(ctx->n_cb) * 4,
                                         ctx->stream));
@@ -3262,13 +3321,62 @@ int ddsolve_perform_iteration(ddsolve_ctx* ctx, const double* solutions,
   }
   if ((rc = LaunchIteration(ctx, true, false, false)) != DDSOLVE_OK) return rc;
   DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(next_solutions, ctx->d_next.ptr,
-                                      n_sol * sizeof(double2), cudaMemcpyDeviceToHost,
+                                      n_sol * sizeof(double2), cudaMemcpyDefault,
                                       ctx->stream));
   DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   // pipe path: build_tables (+ power_kernel) + pipe_kernel; else
   // stream_kernel + finalize_kernel
   ctx->last_launches = ctx->use_pipe ? 2 + (powers_launched ? 1 : 0) : 2;
   return CheckDeviceError(ctx);
+}
+
+int ddsolve_perform_iterations(ddsolve_ctx* ctx, const double* start, uint32_t n_passes,
+                               double* outputs) {
+  if (!ctx || !start || !outputs || n_passes == 0) return DDSOLVE_E_INVALID;
+  cudaSetDevice(ctx->device);
+  int rc;
+  if (ctx->plan_dirty && (rc = BuildPlan(ctx)) != DDSOLVE_OK) return rc;
+  const size_t n_sol = size_t(ctx->n_cb) * ctx->n_ant * ctx->n_sub * ctx->n_pol;
+  const size_t bytes = n_sol * sizeof(double2);
+  DDS_CHECK_CUDA(ctx, ctx->d_chain.Reserve(bytes * n_passes));
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->d_sol.ptr, start, bytes, cudaMemcpyDefault,
+                                      ctx->stream));
+  uint64_t launches = 0;
+  // Pass k reads its solutions from the previous pass's slot of the chain
+  // buffer and writes its own slot: the solver's solution buffers are
+  // pointed there for the duration of the call (no copies between passes).
+  struct Restore {
+    ddsolve_ctx* c;
+    void *sol, *next;
+    ~Restore() {
+      c->d_sol.ptr = sol;
+      c->d_next.ptr = next;
+    }
+  } restore{ctx, ctx->d_sol.ptr, ctx->d_next.ptr};
+  for (uint32_t k = 0; k < n_passes; ++k) {
+    if (k > 0) ctx->d_sol.ptr = ctx->d_chain.as<char>() + bytes * (k - 1);
+    ctx->d_next.ptr = ctx->d_chain.as<char>() + bytes * k;
+    if (ctx->use_pipe) {
+      DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_flag.ptr, 0, size_t(ctx->n_cb) * 4,
+                                          ctx->stream));
+      DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_done.ptr, 0, size_t(ctx->n_cb) * 4,
+                                          ctx->stream));
+      DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.ptr, 0, 16, ctx->stream));
+      if ((rc = LaunchBuildTables(ctx)) != DDSOLVE_OK) return rc;
+      if (ctx->use_powers && ctx->powers_dirty) ++launches;
+      if ((rc = LaunchPowers(ctx, false)) != DDSOLVE_OK) return rc;
+      launches += 2;
+    } else {
+      launches += 2;
+    }
+    if ((rc = LaunchIteration(ctx, true, false, false)) != DDSOLVE_OK) return rc;
+  }
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(outputs, ctx->d_chain.ptr, bytes * n_passes,
+                                      cudaMemcpyDefault, ctx->stream));
+  if ((rc = StageCounters(ctx)) != DDSOLVE_OK) return rc;
+  DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->last_launches = launches;
+  return CheckDeviceError(ctx, true);
 }
 
 int ddsolve_time_stream_kernel(ddsolve_ctx* ctx, uint32_t n_launches, float* mean_ms) {

@@ -112,28 +112,39 @@ __host__ __device__ constexpr uint32_t InstrDesc(int m, int n) {
 
 // Loads an R x 64 (rows x K) chunk starting at (row0, k0) into the canonical
 // K-major layout: element (r, k) at ((r / 8) * 8 + k / 8) * 128 + (r % 8) * 16
-// + (k % 8) * 2 bytes. Out-of-range elements are zero.
+// + (k % 8) * 2 bytes. Out-of-range elements are zero. All of a thread's
+// 16-byte groups are loaded into registers before any is stored, so that
+// their global-memory latencies overlap.
 template <int R>
 __device__ __forceinline__ void LoadChunk(unsigned char* dst, const uint16_t* src, int ld,
                                           int trans, int rows, int K, int row0, int k0) {
   constexpr int kGroups = R * (kKChunk / 8);
-  for (int g = threadIdx.x; g < kGroups; g += kGemmThreads) {
+  constexpr int kPerThread = kGroups / kGemmThreads;
+  static_assert(kGroups % kGemmThreads == 0, "chunk groups must split evenly");
+  uint4 q[kPerThread];
+  const bool fast = !trans && (ld & 7) == 0;
+#pragma unroll
+  for (int i = 0; i < kPerThread; ++i) {
+    const int g = threadIdx.x + i * kGemmThreads;
     const int r = g >> 3, kc = g & 7;
     const int row = row0 + r, k = k0 + kc * 8;
-    uint16_t v[8];
-    if (!trans && row < rows && k + 8 <= K && (ld & 7) == 0) {
-      const uint4 q = *reinterpret_cast<const uint4*>(src + size_t(row) * ld + k);
-      memcpy(v, &q, 16);
+    if (fast && row < rows && k + 8 <= K) {
+      q[i] = __ldg(reinterpret_cast<const uint4*>(src + size_t(row) * ld + k));
     } else {
+      uint16_t v[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const bool in = row < rows && k + j < K;
         v[j] = in ? (trans ? src[size_t(k + j) * ld + row] : src[size_t(row) * ld + k + j]) : 0;
       }
+      memcpy(&q[i], v, 16);
     }
-    uint4 q;
-    memcpy(&q, v, 16);
-    *reinterpret_cast<uint4*>(dst + ((r >> 3) * 8 + kc) * 128 + (r & 7) * 16) = q;
+  }
+#pragma unroll
+  for (int i = 0; i < kPerThread; ++i) {
+    const int g = threadIdx.x + i * kGemmThreads;
+    const int r = g >> 3, kc = g & 7;
+    *reinterpret_cast<uint4*>(dst + ((r >> 3) * 8 + kc) * 128 + (r & 7) * 16) = q[i];
   }
 }
 
@@ -367,6 +378,76 @@ __global__ void to_bf16_kernel(const float* __restrict__ w, size_t n, uint16_t* 
     wb[i] = ToBf16(w[i]);
 }
 
+constexpr uint32_t kMaxSets = 16;
+struct SetPtrs {
+  const double2* p[kMaxSets];  // device addresses of the solution sets
+};
+
+// Network samples from solution sets (see ddwarm_features); one thread per
+// (row, value, set >= 1). Writes FP32 features (x32, ld = n_feat) and / or
+// BF16 features (xb, ld = ldb).
+__global__ void features_kernel(const SetPtrs sets, uint32_t n_sets, uint32_t n_cb,
+                                uint32_t n_ant, uint32_t n_sub, uint32_t n_pol, double scale,
+                                float* __restrict__ x32, uint16_t* __restrict__ xb,
+                                uint32_t ldb) {
+  const uint32_t w_n = n_cb * n_pol;
+  const uint32_t rows = n_ant * n_sub;
+  const size_t total = size_t(rows) * w_n * (n_sets - 1);
+  const uint32_t n_feat = 2 * w_n * (n_sets - 1);
+  for (size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+       t += size_t(gridDim.x) * blockDim.x) {
+    const uint32_t w = uint32_t(t % w_n);
+    const uint32_t row = uint32_t((t / w_n) % rows);
+    const uint32_t k = 1 + uint32_t(t / (size_t(w_n) * rows));
+    const uint32_t cb = w / n_pol, pol = w - cb * n_pol;
+    const uint32_t ant = row / n_sub, sub = row - ant * n_sub;
+    const size_t i = ((size_t(cb) * n_ant + ant) * n_sub + sub) * n_pol + pol;
+    const double2 b = sets.p[0][i];
+    const double2 v = sets.p[k][i];
+    // r = v / b; log r = (log |r|, arg r)
+    const double den = b.x * b.x + b.y * b.y;
+    const double rr = (v.x * b.x + v.y * b.y) / den;
+    const double ri = (v.y * b.x - v.x * b.y) / den;
+    double lre = 0.5 * log(rr * rr + ri * ri);
+    double lim = atan2(ri, rr);
+    if (!isfinite(lre) || !isfinite(lim)) lre = lim = 0.0;
+    const uint32_t c = (k - 1) * 2 * w_n + w;
+    if (x32) {
+      x32[size_t(row) * n_feat + c] = float(scale * lre);
+      x32[size_t(row) * n_feat + c + w_n] = float(scale * lim);
+    }
+    if (xb) {
+      xb[size_t(row) * ldb + c] = ToBf16(float(scale * lre));
+      xb[size_t(row) * ldb + c + w_n] = ToBf16(float(scale * lim));
+    }
+  }
+}
+
+// start = base * exp((y_re + i y_im) / scale); base where not finite.
+__global__ void apply_kernel(const double2* __restrict__ base, const float* __restrict__ y,
+                             uint32_t ldy, uint32_t n_cb, uint32_t n_ant, uint32_t n_sub,
+                             uint32_t n_pol, double scale, double2* __restrict__ start) {
+  const uint32_t w_n = n_cb * n_pol;
+  const size_t n_sol = size_t(n_cb) * n_ant * n_sub * n_pol;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n_sol;
+       i += size_t(gridDim.x) * blockDim.x) {
+    const uint32_t pol = uint32_t(i % n_pol);
+    const uint32_t sub = uint32_t((i / n_pol) % n_sub);
+    const uint32_t ant = uint32_t((i / (size_t(n_pol) * n_sub)) % n_ant);
+    const uint32_t cb = uint32_t(i / (size_t(n_pol) * n_sub * n_ant));
+    const uint32_t row = ant * n_sub + sub, w = cb * n_pol + pol;
+    const double lre = double(y[size_t(row) * ldy + w]) / scale;
+    const double lim = double(y[size_t(row) * ldy + w + w_n]) / scale;
+    const double m = exp(lre);
+    double s, c;
+    sincos(lim, &s, &c);
+    const double2 b = base[i];
+    double2 o = make_double2(m * (b.x * c - b.y * s), m * (b.x * s + b.y * c));
+    if (!isfinite(o.x) || !isfinite(o.y)) o = b;
+    start[i] = o;
+  }
+}
+
 struct DevBuf {
   void* ptr = nullptr;
   size_t bytes = 0;
@@ -413,6 +494,7 @@ struct ddwarm_ctx {
   // activations for up to `cap` rows
   uint32_t cap = 0;
   DevBuf xb, h1, h2, y, t, dy, dz2, dz1, partial, loss, error;
+  DevBuf sets, start, x32;  // warm-start features / predictions
   // training data set
   DevBuf ds_x, ds_t, ds_idx;
 
@@ -471,7 +553,9 @@ int Gemm(ddwarm_ctx* ctx, const uint16_t* a, int lda, int a_trans, const uint16_
   p.K = K;
   p.epilogue = epilogue;
   const uint32_t gm = (uint32_t(M) + kMTile - 1) / kMTile;
-  if (N % 256 == 0) {
+  // Wide tiles when there are enough row tiles to fill the GPU; otherwise
+  // 64-column tiles spread a small batch over more SMs.
+  if (N % 256 == 0 && gm >= 32) {
     dim3 grid(gm, uint32_t(N) / 256);
     gemm_kernel<256><<<grid, kGemmThreads, GemmSmem<256>(), ctx->stream>>>(p);
   } else {
@@ -628,7 +712,7 @@ int ddwarm_create(uint32_t n_in, uint32_t n_hidden, uint32_t n_out, uint64_t see
                   ddwarm_ctx** out) {
   if (!out) return 1;
   *out = nullptr;
-  if (n_in == 0 || n_in > 256 || n_out == 0 || n_out > 256 || n_hidden < 64 ||
+  if (n_in == 0 || n_in > 1024 || n_out == 0 || n_out > 256 || n_hidden < 64 ||
       n_hidden > 256 || n_hidden % 64)
     return 1;
   int n_dev = 0;
@@ -829,6 +913,100 @@ int ddwarm_train(ddwarm_ctx* ctx, uint32_t n, const float* x, const float* targe
     }
   }
   return 0;
+}
+
+// Device addresses of the solution sets: device memory of this context's
+// device is used in place, host memory is staged into ctx->sets.
+static int ResolveSets(ddwarm_ctx* ctx, const ddwarm_layout* lay, uint32_t n_sets,
+                       const double* const* sets, SetPtrs* out, size_t* n_sol_out) {
+  const size_t n_sol = size_t(lay->n_channel_blocks) * lay->n_antennas * lay->n_sub * lay->n_pol;
+  WARM_CHECK(ctx, ctx->sets.Reserve(n_sol * 16 * n_sets));
+  for (uint32_t k = 0; k < n_sets; ++k) {
+    cudaPointerAttributes attr{};
+    const bool dev = cudaPointerGetAttributes(&attr, sets[k]) == cudaSuccess &&
+                     (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged) &&
+                     attr.device == ctx->device;
+    cudaGetLastError();  // unregistered host memory is not an error here
+    if (dev) {
+      out->p[k] = reinterpret_cast<const double2*>(sets[k]);
+    } else {
+      char* dst = ctx->sets.as<char>() + n_sol * 16 * k;
+      WARM_CHECK(ctx, cudaMemcpyAsync(dst, sets[k], n_sol * 16, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+      out->p[k] = reinterpret_cast<const double2*>(dst);
+    }
+  }
+  *n_sol_out = n_sol;
+  return 0;
+}
+
+static bool BadLayout(const ddwarm_layout* lay, uint32_t n_sets, const double* const* sets) {
+  if (!lay || !sets || n_sets < 2 || n_sets > kMaxSets) return true;
+  if (!lay->n_channel_blocks || !lay->n_antennas || !lay->n_sub || !lay->n_pol) return true;
+  if (!(lay->scale > 0.0)) return true;
+  for (uint32_t k = 0; k < n_sets; ++k)
+    if (!sets[k]) return true;
+  return false;
+}
+
+int ddwarm_features(ddwarm_ctx* ctx, const ddwarm_layout* lay, uint32_t n_sets,
+                    const double* const* sets, float* x) {
+  if (!ctx || !x || BadLayout(lay, n_sets, sets)) return 1;
+  cudaSetDevice(ctx->device);
+  int rc;
+  size_t n_sol = 0;
+  SetPtrs sp{};
+  if ((rc = ResolveSets(ctx, lay, n_sets, sets, &sp, &n_sol))) return rc;
+  const size_t rows = size_t(lay->n_antennas) * lay->n_sub;
+  const size_t n_feat = size_t(2) * lay->n_channel_blocks * lay->n_pol * (n_sets - 1);
+  WARM_CHECK(ctx, ctx->x32.Reserve(rows * n_feat * 4));
+  features_kernel<<<256, 256, 0, ctx->stream>>>(sp, n_sets, lay->n_channel_blocks,
+                                                lay->n_antennas, lay->n_sub, lay->n_pol,
+                                                lay->scale, ctx->x32.as<float>(), nullptr, 0);
+  WARM_CHECK(ctx, cudaGetLastError());
+  WARM_CHECK(ctx, cudaMemcpyAsync(x, ctx->x32.ptr, rows * n_feat * 4, cudaMemcpyDefault,
+                                  ctx->stream));
+  WARM_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+  return 0;
+}
+
+int ddwarm_predict_start(ddwarm_ctx* ctx, const ddwarm_layout* lay, uint32_t n_sets,
+                         const double* const* sets, double* start) {
+  if (!ctx || !start || BadLayout(lay, n_sets, sets)) return 1;
+  const uint32_t w_n = lay->n_channel_blocks * lay->n_pol;
+  if (ctx->n_in != 2 * w_n * (n_sets - 1) || ctx->n_out != 2 * w_n)
+    return ctx->Fail(1, "network shape does not match the layout and the number of sets");
+  cudaSetDevice(ctx->device);
+  int rc;
+  size_t n_sol = 0;
+  const uint32_t rows = lay->n_antennas * lay->n_sub;
+  if ((rc = Reserve(ctx, rows))) return rc;
+  SetPtrs sp{};
+  if ((rc = ResolveSets(ctx, lay, n_sets, sets, &sp, &n_sol))) return rc;
+  WARM_CHECK(ctx, cudaMemsetAsync(ctx->xb.ptr, 0, size_t(rows) * ctx->di * 2, ctx->stream));
+  features_kernel<<<256, 256, 0, ctx->stream>>>(sp, n_sets, lay->n_channel_blocks,
+                                                lay->n_antennas, lay->n_sub, lay->n_pol,
+                                                lay->scale, nullptr, ctx->xb.as<uint16_t>(),
+                                                ctx->di);
+  WARM_CHECK(ctx, cudaGetLastError());
+  if ((rc = Forward(ctx, rows))) return rc;
+  cudaPointerAttributes attr{};
+  const bool dev_out = cudaPointerGetAttributes(&attr, start) == cudaSuccess &&
+                       (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged) &&
+                       attr.device == ctx->device;
+  cudaGetLastError();
+  double2* out = reinterpret_cast<double2*>(start);
+  if (!dev_out) {
+    WARM_CHECK(ctx, ctx->start.Reserve(n_sol * 16));
+    out = ctx->start.as<double2>();
+  }
+  apply_kernel<<<256, 256, 0, ctx->stream>>>(sp.p[0], ctx->y.as<float>(), ctx->dout,
+                                             lay->n_channel_blocks, lay->n_antennas, lay->n_sub,
+                                             lay->n_pol, lay->scale, out);
+  WARM_CHECK(ctx, cudaGetLastError());
+  if (!dev_out)
+    WARM_CHECK(ctx, cudaMemcpyAsync(start, out, n_sol * 16, cudaMemcpyDeviceToHost, ctx->stream));
+  return CheckError(ctx);
 }
 
 }  // extern "C"

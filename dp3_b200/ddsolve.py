@@ -23,6 +23,7 @@ EXPORTED_SYMBOLS = (
     "ddsolve_solve", "ddsolve_perform_iteration", "ddsolve_stream",
     "ddsolve_set_tuning", "ddsolve_time_stream_kernel",
     "ddsolve_last_launch_count", "ddsolve_perform_iteration_noalloc",
+    "ddsolve_perform_iterations",
 )
 
 
@@ -80,6 +81,7 @@ def lib():
                                                         vp, vp, vp, vp]
         L.ddsolve_solve.argtypes = [vp, vp, ctypes.POINTER(Result), vp]
         L.ddsolve_perform_iteration.argtypes = [vp, vp, vp]
+        L.ddsolve_perform_iterations.argtypes = [vp, vp, u32, vp]
         L.ddsolve_stream.argtypes = [vp]
         L.ddsolve_stream.restype = vp
         L.ddsolve_set_tuning.argtypes = [vp, u32, u32]
@@ -98,7 +100,16 @@ def default_settings():
 
 
 def _addr(a):
-    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+    """Address of a numpy array or of a torch tensor (host or CUDA)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr())
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _is_torch(a):
+    return hasattr(a, "data_ptr") and hasattr(a, "is_cuda")
 
 
 class Context:
@@ -182,8 +193,14 @@ class Context:
             "ddsolve_set_channel_block_regular")
 
     def solve(self, solutions, step_magnitudes=None):
-        """solutions: complex128 [n_cb, n_ant, n_sub, n_pol], updated in place."""
-        assert solutions.dtype == np.complex128 and solutions.flags.c_contiguous
+        """solutions: complex128 [n_cb, n_ant, n_sub, n_pol], updated in place
+        (a numpy array, or a contiguous torch tensor on the host or on the
+        context's GPU)."""
+        if _is_torch(solutions):
+            import torch
+            assert solutions.dtype == torch.complex128 and solutions.is_contiguous()
+        else:
+            assert solutions.dtype == np.complex128 and solutions.flags.c_contiguous
         res = Result()
         self._check(lib().ddsolve_solve(self._h, _addr(solutions),
                                         ctypes.byref(res),
@@ -197,6 +214,23 @@ class Context:
                                                     _addr(nxt)),
                     "ddsolve_perform_iteration")
         return nxt
+
+    def perform_iterations(self, start, n_passes):
+        """n_passes chained PerformIteration passes from `start`; returns
+        [n_passes] + start.shape (pass k starts from pass k - 1's output).
+        A CUDA torch tensor in gives a CUDA tensor out (no host copies)."""
+        if _is_torch(start):
+            import torch
+            start = start.contiguous()
+            out = torch.empty((n_passes,) + tuple(start.shape), dtype=torch.complex128,
+                              device=start.device)
+        else:
+            start = np.ascontiguousarray(start, dtype=np.complex128)
+            out = np.empty((n_passes,) + start.shape, np.complex128)
+        self._check(lib().ddsolve_perform_iterations(self._h, _addr(start), n_passes,
+                                                     _addr(out)),
+                    "ddsolve_perform_iterations")
+        return out
 
     def time_stream_kernel(self, n_launches=10):
         ms = ctypes.c_float()

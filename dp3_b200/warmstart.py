@@ -1,26 +1,27 @@
 """Learned warm start for the direction-iterative solver.
 
 `MLP` binds libddwarm_b200.so (the C ABI in include/ddwarm_b200.h): a
-three-layer perceptron whose forward and training passes run on the B200
-tensor cores (BF16 weights, FP32 accumulation). `LearnedWarmStart` turns
-solver state into network samples and back:
+three-layer perceptron (two hidden layers of 256) whose forward and training
+passes run on the B200 tensor cores (BF16 weights, FP32 accumulation).
+`LearnedWarmStart` predicts the initial solutions of a new solution interval
+in two stages, each a network over one sample per (antenna, sub-solution)
+across all channel blocks and polarizations:
 
-* one sample per (antenna, sub-solution), across all channel blocks and
-  polarizations;
-* inputs: the last four converged solutions h1..h4 of that antenna and
-  direction (h1 = the previous interval) and the current interval's one-pass
-  residual statistic z = the undamped solver update from h1 (the
-  `PerformIteration` output next = num / den, ddsolve_perform_iteration), all
-  as complex logarithms relative to h1: log(h_k / h1), k = 2..4, and
-  log(z / h1), real and imaginary parts, scaled by `scale`;
-* target: log(g / h1) of the converged solution g of the interval, scaled
-  alike; prediction g_hat = h1 * exp(y / scale).
+* inputs are complex logarithms of solution sets relative to a base set
+  (features computed on the GPU, ddwarm_features): stage 1 uses the last four
+  converged solutions h1..h4 (base h1) and K1 chained undamped passes of the
+  solver over the current interval from h1 (the `PerformIteration` output
+  next = num / den, ddsolve_perform_iterations: the per-antenna-direction
+  residual statistics of the new data); stage 2 uses stage 1's prediction g1
+  (base) and K2 passes from g1;
+* targets are log(g / base) of the plain solver's converged solution g;
+* prediction: base * exp(output) (ddwarm_predict_start).
 
-The solver then runs from g_hat to the same tolerance as from the previous
-solutions (DDECal's solution propagation), so only the iteration count
-changes: the network is a source of initial values, never of the answer.
-Entries that are not finite (flagged antennas) are zero in the inputs and
-fall back to h1 in the prediction.
+The solver then runs from the prediction to the same tolerance as from the
+previous solutions (DDECal's solution propagation), so only the iteration
+count changes: the networks are a source of initial values, never of the
+answer. Entries that are not finite (flagged antennas) are zero in the inputs
+and keep the base value in the prediction.
 
 There is no CPU fallback: loading fails loudly when the library is missing.
 """
@@ -36,7 +37,7 @@ LIB_PATH = os.path.join(HERE, "libddwarm_b200.so")
 EXPORTED_SYMBOLS = (
     "ddwarm_create", "ddwarm_destroy", "ddwarm_last_error", "ddwarm_param_count",
     "ddwarm_get_params", "ddwarm_set_params", "ddwarm_predict",
-    "ddwarm_gradients", "ddwarm_train",
+    "ddwarm_gradients", "ddwarm_train", "ddwarm_features", "ddwarm_predict_start",
 )
 
 _lib = None
@@ -65,6 +66,8 @@ def lib():
         L.ddwarm_predict.argtypes = [vp, u32, vp, vp]
         L.ddwarm_gradients.argtypes = [vp, u32, vp, vp, vp, vp]
         L.ddwarm_train.argtypes = [vp, u32, vp, vp, u32, u32, f32, u64, vp]
+        L.ddwarm_features.argtypes = [vp, vp, u32, vp, vp]
+        L.ddwarm_predict_start.argtypes = [vp, vp, u32, vp, vp]
         _lib = L
     return _lib
 
@@ -146,69 +149,144 @@ class MLP:
         return losses[:epochs]
 
 
-def _clog(r):
-    """Complex log with non-finite / zero entries mapped to 0."""
-    with np.errstate(all="ignore"):
-        out = np.log(r)
-    bad = ~np.isfinite(out)
-    out[bad] = 0.0
-    return out
+class Layout(ctypes.Structure):
+    _fields_ = [("n_channel_blocks", ctypes.c_uint32), ("n_antennas", ctypes.c_uint32),
+                ("n_sub", ctypes.c_uint32), ("n_pol", ctypes.c_uint32),
+                ("scale", ctypes.c_double)]
 
 
-class LearnedWarmStart:
-    """Features, targets and predictions for solutions shaped
-    [n_cb][n_ant][n_sub][n_pol] (the solver's layout)."""
+def _sets_arg(sets):
+    """Pointer array to solution sets: numpy arrays (host) or contiguous
+    complex128 torch tensors (host or GPU)."""
+    arrs, addrs = [], []
+    for x in sets:
+        if hasattr(x, "data_ptr"):
+            x = x.contiguous()
+            addrs.append(x.data_ptr())
+        else:
+            x = np.ascontiguousarray(x, np.complex128)
+            addrs.append(x.ctypes.data)
+        arrs.append(x)
+    return arrs, (ctypes.c_void_p * len(arrs))(*addrs)
 
-    HISTORY = 4
 
-    def __init__(self, n_cb, n_ant, n_sub, n_pol, hidden=256, scale=20.0, seed=1, device=0):
-        self.n_cb, self.n_ant, self.n_sub, self.n_pol = n_cb, n_ant, n_sub, n_pol
-        self.scale = scale
-        self.width = n_cb * n_pol  # complex values per sample and solution set
-        self.n_in = 2 * self.width * self.HISTORY  # 3 history ratios + z
-        self.n_out = 2 * self.width
-        if self.n_in > 256 or self.n_out > 256:
-            raise ValueError("too many channel blocks x polarizations for the network")
-        self.mlp = MLP(self.n_in, self.n_out, hidden=hidden, seed=seed, device=device)
+class Stage:
+    """One network from solution sets [base, others...] to initial solutions
+    (ddwarm_features / ddwarm_predict_start)."""
 
-    def _samples(self, a):
-        """[cb][ant][sub][pol] -> [ant * sub][cb * pol] (sample-major)."""
-        return np.transpose(a, (1, 2, 0, 3)).reshape(self.n_ant * self.n_sub, self.width)
+    def __init__(self, layout, n_sets, hidden=256, seed=1, device=0):
+        self.layout = layout
+        self.n_sets = n_sets
+        self.width = layout.n_channel_blocks * layout.n_pol
+        self.mlp = MLP(2 * self.width * (n_sets - 1), 2 * self.width, hidden=hidden, seed=seed,
+                       device=device)
+        self.x, self.t = [], []
 
-    def _unsamples(self, s):
-        return np.transpose(s.reshape(self.n_ant, self.n_sub, self.n_cb, self.n_pol),
-                            (2, 0, 1, 3))
+    def features(self, sets):
+        arrs, ptrs = _sets_arg(sets)
+        rows = self.layout.n_antennas * self.layout.n_sub
+        x = np.zeros((rows, 2 * self.width * (len(sets) - 1)), np.float32)
+        self.mlp._check(lib().ddwarm_features(self.mlp._h, ctypes.byref(self.layout), len(arrs),
+                                              ptrs, _ptr(x)))
+        return x
 
-    def features(self, history, z):
-        """history: [h1, h2, h3, h4] (most recent first); z: the one-pass
-        update from h1. Returns [n_ant * n_sub][n_in] float32."""
-        h1 = self._samples(history[0])
-        parts = []
-        with np.errstate(all="ignore"):
-            for h in history[1:self.HISTORY]:
-                parts.append(_clog(self._samples(h) / h1))
-            parts.append(_clog(self._samples(z) / h1))
-        x = np.concatenate([np.concatenate([p.real, p.imag], axis=1) for p in parts], axis=1)
-        return (x * self.scale).astype(np.float32)
+    def add(self, sets, converged):
+        """One training interval: features of `sets`, target log(converged / base)."""
+        self.x.append(self.features(sets))
+        self.t.append(self.features([sets[0], converged]))
 
-    def targets(self, h1, g):
-        with np.errstate(all="ignore"):
-            r = _clog(self._samples(g) / self._samples(h1))
-        return (np.concatenate([r.real, r.imag], axis=1) * self.scale).astype(np.float32)
+    def fit(self, epochs=150, batch=1024, lr=1e-3, seed=1):
+        return self.mlp.train(np.concatenate(self.x), np.concatenate(self.t), epochs=epochs,
+                              batch=batch, lr=lr, seed=seed)
 
-    def predict(self, history, z):
-        """Initial solutions of the new interval."""
-        y = self.mlp.predict(self.features(history, z)).astype(np.float64) / self.scale
-        w = self.width
-        logr = y[:, :w] + 1j * y[:, w:]
-        h1 = self._samples(history[0])
-        g = h1 * np.exp(logr)
-        bad = ~np.isfinite(g)
-        g[bad] = h1[bad]
-        return np.ascontiguousarray(self._unsamples(g))
-
-    def train(self, x, t, **kw):
-        return self.mlp.train(x, t, **kw)
+    def predict(self, sets):
+        """Initial solutions, on the device of sets[0] (numpy in, numpy out)."""
+        arrs, ptrs = _sets_arg(sets)
+        if hasattr(arrs[0], "data_ptr"):
+            import torch
+            start = torch.empty_like(arrs[0])
+            out = ctypes.c_void_p(start.data_ptr())
+        else:
+            start = np.empty_like(arrs[0])
+            out = _ptr(start)
+        self.mlp._check(lib().ddwarm_predict_start(self.mlp._h, ctypes.byref(self.layout),
+                                                   len(arrs), ptrs, out))
+        return start
 
     def close(self):
         self.mlp.close()
+
+
+class LearnedWarmStart:
+    """Two-stage learned warm start for solutions shaped
+    [n_cb][n_ant][n_sub][n_pol] (the solver's layout).
+
+    Stage 1 maps [h1, h2, h3, h4, z_1..z_K1] to g1, where h1..h4 are the last
+    four converged solutions (h1 the previous interval's) and z_k are K1
+    chained undamped passes over the current interval from h1
+    (ddsolve_perform_iterations). Stage 2 maps [g1, y_1..y_K2], K2 passes from
+    g1, to g2, the start of the solve. Training (`add_interval`, `fit`) uses
+    intervals that the plain solver has solved; stage 2 learns from stage-1
+    predictions of a provisional stage-1 network that has not seen the
+    interval (fitted after `provisional_after` intervals), so that its inputs
+    carry out-of-sample stage-1 errors.
+    """
+
+    HISTORY = 4
+
+    def __init__(self, n_cb, n_ant, n_sub, n_pol, passes=(3, 3), hidden=256, scale=20.0,
+                 seed=1, device=0, provisional_after=36):
+        self.layout = Layout(n_cb, n_ant, n_sub, n_pol, scale)
+        self.k1, self.k2 = passes
+        self.provisional_after = provisional_after
+        if 2 * n_cb * n_pol * (self.HISTORY - 1 + self.k1) > 1024 or 2 * n_cb * n_pol > 256:
+            raise ValueError("too many channel blocks x polarizations for the network")
+        self.stage1 = Stage(self.layout, self.HISTORY + self.k1, hidden, seed, device)
+        self.stage2 = Stage(self.layout, 1 + self.k2, hidden, seed + 1, device)
+        self._provisional = None
+        self._args = (hidden, seed + 2, device)
+
+    @property
+    def passes(self):
+        return self.k1 + self.k2
+
+    def add_interval(self, solver, history, converged):
+        """Adds one solved training interval whose data is loaded in
+        `solver` (a ddsolve.Context); history = [h1, h2, h3, h4]."""
+        z = solver.perform_iterations(history[0], self.k1)
+        sets1 = list(history[:self.HISTORY]) + list(z)
+        if self._provisional is not None:
+            g1 = self._provisional.predict(sets1)
+            y = solver.perform_iterations(g1, self.k2)
+            self.stage2.add([g1] + list(y), converged)
+        self.stage1.add(sets1, converged)
+        if self._provisional is None and len(self.stage1.x) >= self.provisional_after:
+            hidden, seed, device = self._args
+            self._provisional = Stage(self.layout, self.stage1.n_sets, hidden, seed, device)
+            self._provisional.x, self._provisional.t = list(self.stage1.x), list(self.stage1.t)
+            self._provisional.fit()
+
+    def fit(self, **kw):
+        """Trains both stages on the collected intervals; returns the final
+        epoch losses."""
+        if not self.stage2.x:
+            raise RuntimeError("not enough training intervals for the second stage")
+        l1 = self.stage1.fit(**kw)
+        l2 = self.stage2.fit(**kw)
+        if self._provisional is not None:
+            self._provisional.close()
+            self._provisional = None
+        return float(l1[-1]), float(l2[-1])
+
+    def start(self, solver, history):
+        """Initial solutions of the interval loaded in `solver`. With the
+        history as CUDA tensors every step stays on the GPU."""
+        z = solver.perform_iterations(history[0], self.k1)
+        g1 = self.stage1.predict(list(history[:self.HISTORY]) + list(z))
+        y = solver.perform_iterations(g1, self.k2)
+        return self.stage2.predict([g1] + list(y))
+
+    def close(self):
+        for st in (self.stage1, self.stage2, self._provisional):
+            if st is not None:
+                st.close()

@@ -142,8 +142,10 @@ DDSOLVE_API int ddsolve_set_channel_block_regular(ddsolve_ctx* ctx, uint32_t cha
  * replaces IterativeDiagonalSolver<V>::Solve
  * (ddecal/gain_solvers/IterativeDiagonalSolver.cc:38-97) and
  * IterativeScalarSolver<V>::Solve (IterativeScalarSolver.cc:30-89) for a
- * solver without constraints. `solutions` (host) holds the initial values on
- * entry and the result on return, like the reference's in/out argument.
+ * solver without constraints. `solutions` holds the initial values on entry
+ * and the result on return, like the reference's in/out argument; it may be a
+ * host array or, with unified addressing, device memory of the context's
+ * device (as may the solution arrays of ddsolve_perform_iteration[s]).
  * step_magnitudes (optional, host, [max_iterations]) receives the step
  * magnitude of every iteration (the statistics stream of the reference's
  * stat_stream overload). */
@@ -161,6 +163,17 @@ DDSOLVE_API int ddsolve_solve(ddsolve_ctx* ctx, double* solutions, ddsolve_resul
  * pointers, layout as `solutions`. */
 DDSOLVE_API int ddsolve_perform_iteration(ddsolve_ctx* ctx, const double* solutions,
                               double* next_solutions);
+
+/* n_passes consecutive PerformIteration passes (IterativeDiagonalSolver.cc:
+ * 100-127), each pass starting from the previous pass's next_solutions, with
+ * no host round trip in between: outputs[k] ([n_passes][same layout as
+ * `solutions`]) = PerformIteration(outputs[k - 1]), outputs[-1] = start. Each
+ * pass costs one streaming pass over the data. Replaces a host loop of
+ * ddsolve_perform_iteration calls; the learned warm start
+ * (include/ddwarm_b200.h) uses these undamped passes as residual statistics
+ * of the current interval. */
+DDSOLVE_API int ddsolve_perform_iterations(ddsolve_ctx* ctx, const double* start,
+                                           uint32_t n_passes, double* outputs);
 
 /* The CUDA stream of the context (a cudaStream_t), so that callers can order
  * their own work or CUDA events against the solver. */

@@ -40,7 +40,7 @@ extern "C" {
 
 typedef struct ddwarm_ctx ddwarm_ctx;
 
-/* n_in, n_out in [1, 256]; n_hidden a multiple of 64 in [64, 256].
+/* n_in in [1, 1024], n_out in [1, 256]; n_hidden a multiple of 64 in [64, 256].
  * Weights: He-uniform from std::mt19937_64(seed), biases zero. */
 DDSOLVE_API int ddwarm_create(uint32_t n_in, uint32_t n_hidden, uint32_t n_out,
                               uint64_t seed, int device, ddwarm_ctx** out);
@@ -68,6 +68,37 @@ DDSOLVE_API int ddwarm_gradients(ddwarm_ctx* ctx, uint32_t n, const float* x,
 DDSOLVE_API int ddwarm_train(ddwarm_ctx* ctx, uint32_t n, const float* x,
                              const float* target, uint32_t epochs, uint32_t batch,
                              float lr, uint64_t seed, float* epoch_loss);
+
+/* Solver-side layout of the warm start: solutions are [n_channel_blocks]
+ * [n_antennas][n_sub][n_pol] complex128, as in ddsolve_solve. */
+typedef struct {
+  uint32_t n_channel_blocks;
+  uint32_t n_antennas;
+  uint32_t n_sub;  /* sum of the solutions per direction */
+  uint32_t n_pol;
+  double scale;    /* feature / output scale */
+} ddwarm_layout;
+
+/* Network samples from solution sets (each in the layout above): sets[0] is
+ * the base, sets[1..n_sets-1] the others. One row per (antenna,
+ * sub-solution), row = antenna * n_sub + sub; with W = n_channel_blocks *
+ * n_pol values per row and set (index channel_block * n_pol + pol), set k >= 1
+ * fills columns [(k - 1) 2W, (k - 1) 2W + W) with scale * Re log(set_k /
+ * base) and the next W with scale * Im log(set_k / base); non-finite values
+ * give 0. x: [n_antennas * n_sub][2 W (n_sets - 1)] float32 (host). Computed
+ * on the GPU (used for training data and targets). 2 <= n_sets <= 16. */
+DDSOLVE_API int ddwarm_features(ddwarm_ctx* ctx, const ddwarm_layout* layout, uint32_t n_sets,
+                                const double* const* sets, float* x);
+
+/* Initial solutions for the solver: start = base * exp((y_re + i y_im) /
+ * scale), y = the network's output for ddwarm_features(sets) (the network
+ * must have n_in = 2 W (n_sets - 1) and n_out = 2 W); entries whose result is
+ * not finite take the base value. Features, forward pass and the update run
+ * on the GPU. `sets` and `start` may be host arrays or, with unified
+ * addressing, device memory of the context's device (for example the outputs
+ * of ddsolve_perform_iterations kept on the device), which is read in place. */
+DDSOLVE_API int ddwarm_predict_start(ddwarm_ctx* ctx, const ddwarm_layout* layout,
+                                     uint32_t n_sets, const double* const* sets, double* start);
 
 #ifdef __cplusplus
 }
