@@ -143,17 +143,25 @@ def _barrier(world):
         dist.barrier()
 
 
-def cpu_baseline_port(cfg, obs, iterations_per_interval, budget_s=20.0):
+def workload_name(cfg, config_index, npol):
+    if config_index == CONFIG_INDEX and npol == 2:
+        return WORKLOAD
+    gains = "diagonal" if npol == 2 else "scalar"
+    return (f"{cfg.name}, XX/YY complex64, {gains} gains, unit start, tol 1e-5, "
+            f"max {cfg.max_iterations} iterations")
+
+
+def cpu_baseline_port(cfg, obs, iterations_per_interval, budget_s=20.0, npol=2):
     """Times the oracle (restated reference solver, FP32 arithmetic, all host
     threads) on a bounded sample: a few iterations of the same interval,
     scaled to the GPU interval's iteration count."""
     from oracle import oracle_ffi as of
     ap, sm = obs.generic_arrays()
-    prob = dict(n_antennas=cfg.n_stations, n_correlations=2, n_pol=2,
+    prob = dict(n_antennas=cfg.n_stations, n_correlations=2, n_pol=npol,
                 n_solutions_per_direction=cfg.nspd, data=obs.data,
                 model=obs.model, antenna_pairs=ap, solution_map=sm)
     n_threads = os.cpu_count() or 1
-    sol = np.ones((cfg.n_channel_blocks, cfg.n_stations, sum(cfg.nspd), 2),
+    sol = np.ones((cfg.n_channel_blocks, cfg.n_stations, sum(cfg.nspd), npol),
                   np.complex128)
     t0 = time.perf_counter()
     of.perform_iteration(prob, sol, precision=32, n_threads=n_threads)
@@ -289,7 +297,7 @@ def run_reference_arm(args):
     if rank != 0:
         return 0
     from dp3_b200 import synth
-    cfg = synth.benchmark_configs()[CONFIG_INDEX]
+    cfg = synth.benchmark_configs()[args.config]
     obs = synth.observe(cfg)
     from oracle import oracle_ffi as of
     of.build()
@@ -297,7 +305,7 @@ def run_reference_arm(args):
     times = []
     base = None
     for i in range(args.warmup + args.steps):
-        b = cpu_baseline_port(cfg, obs, iters, budget_s=args.ref_budget)
+        b = cpu_baseline_port(cfg, obs, iters, budget_s=args.ref_budget, npol=args.npol)
         if i >= args.warmup:
             times.append(b["value"])
             base = b
@@ -308,7 +316,8 @@ def run_reference_arm(args):
         "warmup": args.warmup, "ms_per_step": value * 1e3,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "threads": base["cores"]},
+        "config": {"workload": workload_name(cfg, args.config, args.npol),
+                   "threads": base["cores"]},
         "cpu_baseline": base,
         "e2e": {"value": value, "unit": "s/interval", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -334,7 +343,7 @@ def run_gpu_arm(args):
     # every rank solves its own interval (independent intervals: weak scaling)
     obs = synth.observe(cfg, pinned=True, noise_seed=cfg.seed * 7919 + 17 + rank)
     n_sub = sum(cfg.nspd)
-    ctx = ddsolve.Context(cfg.n_stations, cfg.nspd, cfg.n_channel_blocks, 2, 2,
+    ctx = ddsolve.Context(cfg.n_stations, cfg.nspd, cfg.n_channel_blocks, 2, args.npol,
                           device=device)
     st = ddsolve.default_settings()
     st.max_iterations = cfg.max_iterations
@@ -350,7 +359,7 @@ def run_gpu_arm(args):
                                           obs.data[cb], obs.model[cb],
                                           obs.antenna1, obs.antenna2)
 
-    sols = np.ones((cfg.n_channel_blocks, cfg.n_stations, n_sub, 2), np.complex128)
+    sols = np.ones((cfg.n_channel_blocks, cfg.n_stations, n_sub, args.npol), np.complex128)
     mags = np.zeros(cfg.max_iterations + 1, np.float64)
     stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=f"cuda:{device}")
 
@@ -435,9 +444,11 @@ def run_gpu_arm(args):
         "ms_per_step": t_dev / args.steps * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_vis": cfg.n_vis,
+        "config": {"workload": workload_name(cfg, args.config, args.npol), "n_vis": cfg.n_vis,
                    "iterations_per_interval": int(r.iterations),
-                   "l2": "inputs larger than L2 (639 MB streamed per iteration)",
+                   "l2": (f"inputs larger than L2 ({alg_bytes / 1e6:.0f} MB streamed per "
+                          "iteration)" if alg_bytes > 126e6 else
+                          f"inputs ({alg_bytes / 1e6:.2f} MB) fit in L2: not a bench line"),
                    "parallelism": f"{world} independent interval(s), one per GPU"},
         "vis_iterations_per_s": cfg.n_vis * device_iters * args.steps * world / t_dev,
         "e2e": {"value": e2e_value, "unit": "s/interval",
@@ -446,7 +457,8 @@ def run_gpu_arm(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "pipe_kernel", "kernel_ms": kernel_ms,
+                     "kernel": "pipe_kernel" if cfg.n_directions <= 12 else "stream_kernel",
+                     "kernel_ms": kernel_ms,
                      "algorithmic_bytes_per_launch": alg_bytes},
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
@@ -458,7 +470,7 @@ def run_gpu_arm(args):
         of.build()
         obs_np = synth.observe(cfg)
         result["cpu_baseline"] = cpu_baseline_port(cfg, obs_np, int(r.iterations),
-                                                   budget_s=args.ref_budget)
+                                                   budget_s=args.ref_budget, npol=args.npol)
     if rank == 0:
         print(json.dumps(result), flush=True)
     ctx.close()
@@ -482,6 +494,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--config", type=int, default=CONFIG_INDEX,
                     help="benchmark configuration index (synth.benchmark_configs)")
+    ap.add_argument("--npol", type=int, default=2, choices=[1, 2],
+                    help="2: IterativeDiagonalSolver, 1: IterativeScalarSolver")
     ap.add_argument("--warm-intervals", type=int, default=200,
                     help="intervals of the learned-warm-start sequence (0: skip)")
     ap.add_argument("--warm-tight", type=int, default=20,

@@ -318,3 +318,45 @@ def test_scale_invariance_full_size_c1(built):
         b.model = b.model * alpha
     got2 = solver.PerformIteration(sd, sol0)
     np.testing.assert_allclose(got2, got, rtol=1e-5)
+
+
+@pytest.mark.parametrize("npol", [2, 1])
+def test_full_size_large_array_pass(built, npol):
+    """The 512-station configuration at full size (130816 baselines, 5
+    directions, 64 channels in 16 blocks, 2 timesteps, 16.7 M visibilities):
+    one pass of the diagonal (npol 2) and of the scalar (npol 1) solver
+    against the FP64 oracle."""
+    cfg = synth.benchmark_configs()[3]
+    obs = synth.observe(cfg)
+    prob = H.problem_from_observation(obs, 2, npol)
+    sol0 = _perturbed_start(obs, prob, scale=0.1)
+    solver = H.make_solver(prob)
+    got = solver.PerformIteration(obs.solve_data(), sol0)
+    ref = of.perform_iteration(prob, sol0, precision=64)
+    err = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-12)
+    assert np.nanmax(err) < RTOL_PASS, np.nanmax(err)
+    np.testing.assert_array_equal(np.isnan(got), np.isnan(ref))
+
+
+def test_full_size_dd_interval_configuration(built):
+    """One interval of the 40-direction configuration at full size (62
+    stations, 40 directions with 8, 4, 2 or 1 solutions per 8-timestep
+    interval, 120 channels in uneven blocks of 3-12 channels): one pass
+    against the FP64 oracle, then a 10-iteration solve against the oracle
+    with the reference's FP32 arithmetic."""
+    cfg = synth.benchmark_configs()[2]
+    obs = synth.observe(cfg)
+    prob = H.problem_from_observation(obs)
+    sol0 = _perturbed_start(obs, prob, scale=0.1)
+    solver = H.make_solver(prob, max_iterations=10, accuracy=cfg.tolerance)
+    got = solver.PerformIteration(obs.solve_data(), sol0)
+    ref = of.perform_iteration(prob, sol0, precision=64)
+    err = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-12)
+    assert np.nanmax(err) < RTOL_PASS, np.nanmax(err)
+    st = of.settings(max_iterations=10, accuracy=cfg.tolerance, step_size=cfg.step_size)
+    ref32 = sol0.copy()
+    r, _ = of.solve(prob, ref32, st, precision=32)
+    got_s = sol0.copy()
+    res = solver.Solve(obs.solve_data(), got_s, 0.0)
+    assert res.iterations == r.iterations
+    assert H.max_rel_diff(got_s, ref32) < RTOL_SOLVE
