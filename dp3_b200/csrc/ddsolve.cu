@@ -1845,6 +1845,9 @@ struct ddsolve_ctx {
   std::string err = "no error";
   ddsolve_settings settings{};
   uint32_t tune_ng = 0, tune_max_times = 0;
+  // plan knobs (ddsolve_tuning): -1 / 0 = automatic
+  int32_t tune_pipe = -1, tune_powers = -1;
+  uint32_t tune_stages = 0, tune_gbuf = 0;
 
   std::vector<ChannelBlockStore> cbs;
   DevBuf staging, pack_desc, run_src_dev, run_len_dev;
@@ -2211,8 +2214,9 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
     run_rows += uint64_t(t.n) * t.rows;
     n_runs_all += t.n;
   }
-  const bool use_powers = !std::getenv("DDSOLVE_NO_POWERS") && n_runs_all > 0 &&
-                          run_rows >= 16 * n_runs_all;
+  const bool use_powers =
+      !std::getenv("DDSOLVE_NO_POWERS") && n_runs_all > 0 &&
+      (ctx->tune_powers == 1 || (ctx->tune_powers < 0 && run_rows >= 16 * n_runs_all));
   // ---- fragments: rows balanced over the CTAs ----
   uint64_t total_rows = 0;
   double total_w = 0.0;
@@ -2301,6 +2305,9 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
                         size_t(kPipeRuns) * 8 + 256;
     const size_t with2 = off + 2 * size_t(table_f2) * 8 + (any_sorted ? rest : 256);
     ctx->n_gbuf = (with2 + 4 * stage_b <= size_t(max_optin)) ? 2u : 1u;
+    // a requested count, where two buffers still leave two stages
+    if (ctx->tune_gbuf == 1) ctx->n_gbuf = 1;
+    if (ctx->tune_gbuf == 2 && with2 + 2 * stage_b <= size_t(max_optin)) ctx->n_gbuf = 2;
   }
   off += size_t(ctx->n_gbuf) * table_f2 * 8;
   const size_t n_ant4 = align(n_ant, 4);
@@ -2319,7 +2326,8 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
   ctx->off_stages = uint32_t(align(off, 128));
   const size_t stage_bytes = PipeStageBytes(ctx);
   const size_t room = size_t(max_optin) > ctx->off_stages ? size_t(max_optin) - ctx->off_stages : 0;
-  const uint32_t stages = uint32_t(std::min<size_t>(kPipeMaxStages, room / stage_bytes));
+  uint32_t stages = uint32_t(std::min<size_t>(kPipeMaxStages, room / stage_bytes));
+  if (ctx->tune_stages >= 2) stages = std::min(stages, ctx->tune_stages);
   if (stages < 2)
     return ctx->Fail(DDSOLVE_E_UNSUPPORTED, "pipelined kernel does not fit in shared memory");
   ctx->pipe_stages = stages;
@@ -2399,7 +2407,7 @@ int BuildPlan(ddsolve_ctx* ctx) {
   // Pipelined kernel when the direction count, the correlation layout and the
   // shared memory allow it (and no lane groups were requested).
   ctx->use_pipe = false;
-  if (ctx->tune_ng == 0 && (ctx->n_corr == 2 || ctx->n_corr == 4) &&
+  if (ctx->tune_ng == 0 && ctx->tune_pipe != 0 && (ctx->n_corr == 2 || ctx->n_corr == 4) &&
       !std::getenv("DDSOLVE_NO_PIPE")) {
     const KernelEntry* pe =
         FindPipeKernel(int(ctx->n_corr), int(ctx->n_pol), int(ctx->n_dir));
@@ -3413,6 +3421,179 @@ int ddsolve_time_stream_kernel(ddsolve_ctx* ctx, uint32_t n_launches, float* mea
   cudaEventDestroy(b);
   *mean_ms = ms / float(n_launches);
   return CheckDeviceError(ctx);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Autotuner: times the plan variants of the streaming pass on the uploaded
+// data and keeps the fastest, cached per process by problem shape (stations,
+// directions, correlations, polarizations, and per channel block its
+// visibilities, channels and slabs, and the solutions per direction).
+// ---------------------------------------------------------------------------
+namespace {
+
+struct TuneKey {
+  std::vector<uint64_t> v;
+  bool operator<(const TuneKey& o) const { return v < o.v; }
+};
+
+std::mutex g_tune_mu;
+std::map<TuneKey, std::pair<ddsolve_tuning, float>> g_tune_cache;
+
+TuneKey MakeTuneKey(const ddsolve_ctx* ctx) {
+  TuneKey k;
+  k.v = {ctx->n_ant, ctx->n_dir, ctx->n_corr, ctx->n_pol, ctx->n_cb};
+  for (const ChannelBlockStore& cb : ctx->cbs) {
+    k.v.push_back(cb.n_elems);
+    k.v.push_back(cb.slabs.empty() ? 0 : cb.slabs[0].L);
+    k.v.push_back(cb.slabs.size());
+  }
+  for (uint32_t d = 0; d < ctx->n_dir; ++d) k.v.push_back(ctx->n_sol_per_dir[d]);
+  return k;
+}
+
+void ApplyTuning(ddsolve_ctx* ctx, const ddsolve_tuning& t) {
+  ctx->tune_pipe = t.use_pipe;
+  ctx->tune_ng = t.direction_groups;
+  ctx->tune_stages = t.stages;
+  ctx->tune_powers = t.model_powers;
+  ctx->tune_gbuf = t.gain_buffers;
+  ctx->plan_dirty = true;
+}
+
+ddsolve_tuning CurrentTuning(const ddsolve_ctx* ctx) {
+  ddsolve_tuning t;
+  t.use_pipe = ctx->tune_pipe;
+  t.direction_groups = ctx->tune_ng;
+  t.stages = ctx->tune_stages;
+  t.model_powers = ctx->tune_powers;
+  t.gain_buffers = ctx->tune_gbuf;
+  return t;
+}
+
+// Mean time of one iteration's kernels in next-solutions mode (pipe_kernel,
+// or stream_kernel + finalize_kernel), plus the once-per-solve model powers
+// spread over the iteration cap; the plan must be built.
+int TimeIteration(ddsolve_ctx* ctx, uint32_t n, float* ms_out) {
+  int rc;
+  cudaEvent_t a, b, c;
+  DDS_CHECK_CUDA(ctx, cudaEventCreate(&a));
+  DDS_CHECK_CUDA(ctx, cudaEventCreate(&b));
+  DDS_CHECK_CUDA(ctx, cudaEventCreate(&c));
+  if (ctx->use_pipe) {
+    DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_flag.ptr, 0, size_t(ctx->n_cb) * 4,
+                                        ctx->stream));
+    DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.ptr, 0, 16, ctx->stream));
+    if ((rc = LaunchBuildTables(ctx)) != DDSOLVE_OK) return rc;
+  }
+  DDS_CHECK_CUDA(ctx, cudaEventRecord(c, ctx->stream));
+  if ((rc = LaunchPowers(ctx, true)) != DDSOLVE_OK) return rc;
+  if ((rc = LaunchIteration(ctx, true, false, false)) != DDSOLVE_OK) return rc;  // warm-up
+  DDS_CHECK_CUDA(ctx, cudaEventRecord(a, ctx->stream));
+  for (uint32_t i = 0; i < n; ++i)
+    if ((rc = LaunchIteration(ctx, true, false, false)) != DDSOLVE_OK) return rc;
+  DDS_CHECK_CUDA(ctx, cudaEventRecord(b, ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaEventSynchronize(b));
+  float ms = 0.f, first = 0.f;
+  DDS_CHECK_CUDA(ctx, cudaEventElapsedTime(&ms, a, b));
+  DDS_CHECK_CUDA(ctx, cudaEventElapsedTime(&first, c, a));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaEventDestroy(c);
+  if ((rc = CheckDeviceError(ctx)) != DDSOLVE_OK) return rc;
+  const float per_it = ms / float(n);
+  // `first` = model powers (when used) + one warm-up iteration
+  const float powers = std::max(0.f, first - per_it);
+  const float cap = float(std::max(ctx->settings.max_iterations, 1u));
+  *ms_out = per_it + (ctx->use_pipe && ctx->use_powers ? powers / cap : 0.f);
+  return DDSOLVE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ddsolve_get_tuning(const ddsolve_ctx* ctx, ddsolve_tuning* tuning) {
+  if (!ctx || !tuning) return DDSOLVE_E_INVALID;
+  *tuning = CurrentTuning(ctx);
+  return DDSOLVE_OK;
+}
+
+int ddsolve_set_plan_tuning(ddsolve_ctx* ctx, const ddsolve_tuning* t) {
+  if (!ctx || !t) return DDSOLVE_E_INVALID;
+  if (t->use_pipe < -1 || t->use_pipe > 1 || t->model_powers < -1 || t->model_powers > 1 ||
+      t->gain_buffers > 2 || t->stages == 1 ||
+      (t->direction_groups != 0 &&
+       (t->direction_groups > 32 || (t->direction_groups & (t->direction_groups - 1)))))
+    return ctx->Fail(DDSOLVE_E_INVALID, "invalid tuning");
+  ApplyTuning(ctx, *t);
+  return DDSOLVE_OK;
+}
+
+int ddsolve_autotune(ddsolve_ctx* ctx, uint32_t launches, ddsolve_tuning* chosen,
+                     float* iteration_ms) {
+  if (!ctx || launches == 0) return DDSOLVE_E_INVALID;
+  cudaSetDevice(ctx->device);
+  int rc;
+  for (uint32_t c = 0; c < ctx->n_cb; ++c)
+    if (!ctx->cbs[c].set) return ctx->Fail(DDSOLVE_E_STATE, "autotune needs uploaded data");
+  const TuneKey key = MakeTuneKey(ctx);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      ApplyTuning(ctx, it->second.first);
+      if ((rc = BuildPlan(ctx)) != DDSOLVE_OK) return rc;
+      if (chosen) *chosen = it->second.first;
+      if (iteration_ms) *iteration_ms = it->second.second;
+      return DDSOLVE_OK;
+    }
+  }
+  // candidates: pipe_kernel plan variants, then stream_kernel lane groups
+  std::vector<ddsolve_tuning> cands;
+  const bool pipe_ok = (ctx->n_corr == 2 || ctx->n_corr == 4) &&
+                       FindPipeKernel(int(ctx->n_corr), int(ctx->n_pol), int(ctx->n_dir));
+  if (pipe_ok)
+    for (int32_t powers : {0, 1})
+      for (uint32_t gbuf : {1u, 2u})
+        for (uint32_t stages : {0u, 3u}) cands.push_back({1, 0, stages, powers, gbuf});
+  for (uint32_t ng = 1; ng <= 32; ng <<= 1)
+    if (FindKernel(int(ctx->n_corr), int(ctx->n_pol), int((ctx->n_dir + ng - 1) / ng)))
+      cands.push_back({0, ng, 0, -1, 0});
+  // defined solutions for the timed passes
+  const size_t n_sol = size_t(ctx->n_cb) * ctx->n_ant * ctx->n_sub * ctx->n_pol;
+  std::vector<double> ones(2 * n_sol, 0.0);
+  for (size_t i = 0; i < n_sol; ++i) ones[2 * i] = 1.0;
+  const ddsolve_tuning before = CurrentTuning(ctx);
+  ddsolve_tuning best = before;
+  float best_ms = -1.f;
+  for (const ddsolve_tuning& c : cands) {
+    ApplyTuning(ctx, c);
+    if (BuildPlan(ctx) != DDSOLVE_OK) continue;  // variant not applicable
+    if (c.use_pipe == 1 && !ctx->use_pipe) continue;
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->d_sol.ptr, ones.data(), n_sol * 16,
+                                        cudaMemcpyHostToDevice, ctx->stream));
+    float ms = 0.f;
+    if ((rc = TimeIteration(ctx, launches, &ms)) != DDSOLVE_OK) return rc;
+    if (best_ms < 0.f || ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  if (best_ms < 0.f) {
+    ApplyTuning(ctx, before);
+    return ctx->Fail(DDSOLVE_E_UNSUPPORTED, "no plan variant could be built");
+  }
+  ApplyTuning(ctx, best);
+  if ((rc = BuildPlan(ctx)) != DDSOLVE_OK) return rc;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache[key] = {best, best_ms};
+  }
+  if (chosen) *chosen = best;
+  if (iteration_ms) *iteration_ms = best_ms;
+  return DDSOLVE_OK;
 }
 
 }  // extern "C"

@@ -23,7 +23,8 @@ EXPORTED_SYMBOLS = (
     "ddsolve_solve", "ddsolve_perform_iteration", "ddsolve_stream",
     "ddsolve_set_tuning", "ddsolve_time_stream_kernel",
     "ddsolve_last_launch_count", "ddsolve_perform_iteration_noalloc",
-    "ddsolve_perform_iterations",
+    "ddsolve_perform_iterations", "ddsolve_get_tuning", "ddsolve_set_plan_tuning",
+    "ddsolve_autotune",
 )
 
 
@@ -45,6 +46,17 @@ class Settings(ctypes.Structure):
                 ("detect_stalling", ctypes.c_int32),
                 ("step_diff_sigma", ctypes.c_double),
                 ("phase_only", ctypes.c_int32)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("use_pipe", ctypes.c_int32),
+                ("direction_groups", ctypes.c_uint32),
+                ("stages", ctypes.c_uint32),
+                ("model_powers", ctypes.c_int32),
+                ("gain_buffers", ctypes.c_uint32)]
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
 
 
 class Result(ctypes.Structure):
@@ -82,6 +94,10 @@ def lib():
         L.ddsolve_solve.argtypes = [vp, vp, ctypes.POINTER(Result), vp]
         L.ddsolve_perform_iteration.argtypes = [vp, vp, vp]
         L.ddsolve_perform_iterations.argtypes = [vp, vp, u32, vp]
+        L.ddsolve_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+        L.ddsolve_set_plan_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+        L.ddsolve_autotune.argtypes = [vp, u32, ctypes.POINTER(Tuning),
+                                       ctypes.POINTER(ctypes.c_float)]
         L.ddsolve_stream.argtypes = [vp]
         L.ddsolve_stream.restype = vp
         L.ddsolve_set_tuning.argtypes = [vp, u32, u32]
@@ -231,6 +247,27 @@ class Context:
                                                      _addr(out)),
                     "ddsolve_perform_iterations")
         return out
+
+    def autotune(self, launches=5):
+        """Times the plan variants on the uploaded data and keeps the fastest
+        (cached per process by problem shape). Returns (tuning dict, ms per
+        iteration)."""
+        t = Tuning()
+        ms = ctypes.c_float()
+        self._check(lib().ddsolve_autotune(self._h, launches, ctypes.byref(t),
+                                           ctypes.byref(ms)), "ddsolve_autotune")
+        return t.as_dict(), ms.value
+
+    def tuning(self):
+        t = Tuning()
+        self._check(lib().ddsolve_get_tuning(self._h, ctypes.byref(t)), "ddsolve_get_tuning")
+        return t.as_dict()
+
+    def set_plan_tuning(self, **kw):
+        t = Tuning(**{**{"use_pipe": -1, "direction_groups": 0, "stages": 0,
+                         "model_powers": -1, "gain_buffers": 0}, **kw})
+        self._check(lib().ddsolve_set_plan_tuning(self._h, ctypes.byref(t)),
+                    "ddsolve_set_plan_tuning")
 
     def time_stream_kernel(self, n_launches=10):
         ms = ctypes.c_float()

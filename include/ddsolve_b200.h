@@ -185,6 +185,33 @@ DDSOLVE_API void* ddsolve_stream(ddsolve_ctx* ctx);
 DDSOLVE_API int ddsolve_set_tuning(ddsolve_ctx* ctx, uint32_t direction_groups,
                        uint32_t max_slab_times);
 
+/* Plan variants of the streaming pass (no reference counterpart: DP3's only
+ * knob is its thread count, SolverBase::NSubThreads). Negative / zero fields
+ * mean "automatic". */
+typedef struct {
+  int32_t use_pipe;          /* -1 auto, 0 stream_kernel + finalize_kernel, 1 pipe_kernel */
+  uint32_t direction_groups; /* stream_kernel: lanes per run, 0 auto, power of 2 <= 32 */
+  uint32_t stages;           /* pipe_kernel: bulk-copy ring stages, 0 = as many as fit, >= 2 */
+  int32_t model_powers;      /* pipe_kernel: -1 auto, 0 summed in the row loop, 1 precomputed */
+  uint32_t gain_buffers;     /* pipe_kernel: gain-table buffers, 0 auto, 1 or 2 */
+} ddsolve_tuning;
+
+DDSOLVE_API int ddsolve_get_tuning(const ddsolve_ctx* ctx, ddsolve_tuning* tuning);
+DDSOLVE_API int ddsolve_set_plan_tuning(ddsolve_ctx* ctx, const ddsolve_tuning* tuning);
+
+/* Autotuner: on the uploaded data, times every applicable plan variant
+ * (pipe_kernel with model powers on / off, one or two gain-table buffers,
+ * all or three ring stages; stream_kernel with 1..32 lanes per run) over
+ * `launches` iterations in next-solutions mode, keeps the fastest (time per
+ * iteration, the once-per-solve model powers spread over max_iterations) and
+ * caches the choice per process, keyed on stations, directions,
+ * correlations, polarizations, the per-block visibilities, channels and slabs
+ * and the solutions per direction: a later context of the same shape takes
+ * the cached choice without timing. The solutions held by the context are
+ * overwritten. */
+DDSOLVE_API int ddsolve_autotune(ddsolve_ctx* ctx, uint32_t launches, ddsolve_tuning* chosen,
+                                 float* iteration_ms);
+
 /* Device time of the streaming kernel: launches it n_launches times on the
  * context stream with the current solutions and returns the mean duration in
  * milliseconds, measured with CUDA events. Solutions are not modified. */

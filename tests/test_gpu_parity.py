@@ -360,3 +360,47 @@ def test_full_size_dd_interval_configuration(built):
     res = solver.Solve(obs.solve_data(), got_s, 0.0)
     assert res.iterations == r.iterations
     assert H.max_rel_diff(got_s, ref32) < RTOL_SOLVE
+
+
+def test_autotune_keeps_results_and_caches(built):
+    """The autotuner picks a plan variant whose pass equals the default one
+    within the pass tolerance, and a second context of the same shape takes
+    the cached choice."""
+    from dp3_b200 import ddsolve
+    import time
+    obs = H.small_observation(n_stations=20, n_directions=5, n_channels=16, n_cb=4,
+                              n_times=4, seed=13)
+    cfg = obs.cfg
+    prob = H.problem_from_observation(obs)
+    sol0 = _perturbed_start(obs, prob, scale=0.1)
+
+    def make():
+        ctx = ddsolve.Context(cfg.n_stations, cfg.nspd, cfg.n_channel_blocks, 2, 2)
+        for cb, nc in enumerate(cfg.cb_channels):
+            ctx.set_channel_block_regular(cb, cfg.n_times, cfg.n_baselines, nc, obs.data[cb],
+                                          obs.model[cb], obs.antenna1, obs.antenna2)
+        return ctx
+
+    ctx = make()
+    expect = ctx.perform_iteration(sol0)
+    choice, ms = ctx.autotune(3)
+    assert ms > 0
+    assert ctx.tuning() == choice
+    got = ctx.perform_iteration(sol0)
+    err = np.abs(got - expect) / np.maximum(np.abs(expect), 1e-12)
+    assert np.nanmax(err) < RTOL_PASS
+    ctx.close()
+    ctx2 = make()
+    t0 = time.perf_counter()
+    choice2, ms2 = ctx2.autotune(3)
+    assert choice2 == choice and ms2 == ms
+    ctx2.close()
+    # every explicit variant gives the same pass
+    for t in ({"use_pipe": 0, "direction_groups": 2}, {"use_pipe": 1, "model_powers": 1,
+              "gain_buffers": 1, "stages": 3}, {"use_pipe": 1, "model_powers": 0}):
+        c = make()
+        c.set_plan_tuning(**t)
+        got = c.perform_iteration(sol0)
+        err = np.abs(got - expect) / np.maximum(np.abs(expect), 1e-12)
+        assert np.nanmax(err) < RTOL_PASS, t
+        c.close()
