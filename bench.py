@@ -128,13 +128,24 @@ def _dist_setup():
 
 
 def _max_over_ranks(x, world, device):
+    """Max of a per-rank timing over all ranks (device None: a CPU tensor,
+    for the gloo backend)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+    t = torch.tensor([x], dtype=torch.float64,
+                     device="cpu" if device is None else f"cuda:{device}")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def weak_scaling_value(t_local, steps, world, device):
+    """Seconds per interval of the whole job: every rank solves `steps`
+    intervals of its own, the job takes the slowest rank's time, so the
+    job's throughput is steps * world intervals in max-over-ranks seconds."""
+    t_max = _max_over_ranks(t_local, world, device)
+    return t_max, t_max / (steps * world)
 
 
 def _barrier(world):
@@ -400,8 +411,7 @@ def run_gpu_arm(args):
     torch.cuda.synchronize()
     _barrier(world)
     t_dev = ev0.elapsed_time(ev1) / 1e3
-    t_dev = _max_over_ranks(t_dev, world, device)
-    value = t_dev / (args.steps * world)
+    t_dev, value = weak_scaling_value(t_dev, args.steps, world, device)
     n_iter_run = r.iterations if not r.has_converged else r.iterations
     device_iters = min(r.iterations, cfg.max_iterations)
 
@@ -426,8 +436,7 @@ def run_gpu_arm(args):
     e1.record(stream)
     e1.synchronize()
     w_e2e = time.perf_counter() - w0
-    t_e2e = _max_over_ranks(e0.elapsed_time(e1) / 1e3, world, device)
-    e2e_value = t_e2e / (args.steps * world)
+    t_e2e, e2e_value = weak_scaling_value(e0.elapsed_time(e1) / 1e3, args.steps, world, device)
 
     # ---- roofline of the streaming kernel ----------------------------------
     kernel_ms = ctx.time_stream_kernel(args.kernel_launches)
