@@ -303,6 +303,30 @@ def run_warm_start(args, device):
     }
 
 
+def run_mlp_only(args):
+    """Training throughput of the warm-start network alone (the shape of the
+    first stage on the 62-station, 12-block workload: 336 inputs, two hidden
+    layers of 256, 48 outputs) on seeded random data; the command the
+    tensor-core profile uses."""
+    import torch
+    from dp3_b200 import warmstart
+    rng = np.random.default_rng(5)
+    n, n_in, n_out = args.mlp_rows, 336, 48
+    x = rng.normal(size=(n, n_in)).astype(np.float32)
+    t = rng.normal(size=(n, n_out)).astype(np.float32) * 0.1
+    mlp = warmstart.MLP(n_in, n_out, hidden=256, seed=1)
+    mlp.train(x[:4096], t[:4096], epochs=1, batch=1024)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    mlp.train(x, t, epochs=args.mlp_epochs, batch=1024)
+    dt = time.perf_counter() - t0
+    flops_row = 2 * (n_in * 256 + 256 * 256 + 256 * n_out) * 3  # forward + 2x backward
+    print(json.dumps({"mlp_train_s": dt, "rows": n, "epochs": args.mlp_epochs,
+                      "tflops": flops_row * n * args.mlp_epochs / dt / 1e12}), flush=True)
+    mlp.close()
+    return 0
+
+
 def run_reference_arm(args):
     world, rank, local = _dist_setup()
     if rank != 0:
@@ -516,6 +540,10 @@ def main():
     ap.add_argument("--warm-tight", type=int, default=20,
                     help="evaluated intervals also solved to tolerance 1e-8 for accuracy")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--mlp-only", action="store_true",
+                    help="time only the warm-start network's training (for profiling)")
+    ap.add_argument("--mlp-rows", type=int, default=60000)
+    ap.add_argument("--mlp-epochs", type=int, default=5)
     ap.add_argument("--pass-only", action="store_true",
                     help="time only the streaming pass (for profiling)")
     args = ap.parse_args()
@@ -523,6 +551,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.mlp_only:
+        return run_mlp_only(args)
     return run_gpu_arm(args)
 
 
