@@ -142,6 +142,16 @@ struct FinParams {
   double* step_magnitudes;
   cudaGraphConditionalHandle handle;
   int32_t use_handle;
+  // independent solution intervals (groups of channel blocks): finalisation
+  // block b covers items [block_item0[b], block_item_end[b]) of interval
+  // block_group[b]; interval g owns blocks [group_blocks[g], group_blocks[g+1])
+  // and its loop state state[g] and step magnitudes step_magnitudes[g * mags_stride]
+  const uint32_t* block_group;
+  const uint32_t* block_item0;
+  const uint32_t* block_item_end;
+  const uint32_t* group_blocks;
+  uint32_t n_groups;
+  uint32_t mags_stride;
 };
 
 // ---------------------------------------------------------------------------
@@ -274,11 +284,13 @@ template <int NPOL>
 __global__ void __launch_bounds__(kThreads)
     make_finite_kernel(double2* __restrict__ sols, uint32_t* nonfinite,
                        uint32_t per_cb, cudaGraphConditionalHandle handle,
-                       int use_handle) {
+                       int use_handle, const uint32_t* cb_group, const LoopState* state) {
   if (use_handle && blockIdx.x == 0 && threadIdx.x == 0)
     cudaGraphSetConditional(handle, 0);
   const uint32_t cb = blockIdx.x;
   if (nonfinite[cb] == 0) return;
+  // a finished interval keeps its solutions as they were when it stopped
+  if (cb_group && state[cb_group[cb]].done) return;
   double2* s = sols + size_t(cb) * per_cb;
   __shared__ double red_sum[kThreads];
   __shared__ uint32_t red_cnt[kThreads];
@@ -564,14 +576,54 @@ __device__ __forceinline__ double2 dinv(double2 s) {
   }
 }
 
+// One interval's AssignSolutions norm, stopping criterion and stall
+// detection after an iteration whose norm sum / count are given; returns
+// whether the interval stops.
+__device__ bool ControlStep(LoopState& ls, const DevSettings& st, double sum, uint64_t cnt,
+                            double* step_magnitudes) {
+  // AssignSolutions (SolverBase.cc:297-306), no constraints: accuracy.
+  const double mag = cnt == 0 ? 0.0 : sum / st.step_size / double(cnt);
+  const uint32_t it = ls.iteration + 1;
+  ls.iteration = it;
+  if (it <= st.hard_cap) step_magnitudes[it - 1] = mag;
+  const bool converged = mag <= st.accuracy;
+  // ReachedStoppingCriterion / DetectStall (SolverBase.h:274-285,
+  // SolverBase.cc:63-86)
+  bool stalled = false;
+  if (st.detect_stalling) {
+    if (it == 1) {
+      ls.n_var_count = 1;
+      ls.step_mean = mag;
+      ls.step_var = 0.0;
+    } else {
+      ls.n_var_count += 1;
+      const double delta_1 = mag - ls.step_mean;
+      ls.step_mean += delta_1 / double(ls.n_var_count);
+      const double delta_2 = mag - ls.step_mean;
+      ls.step_var += delta_1 * delta_2;
+    }
+    if (it >= 30)
+      stalled = ls.step_mean <
+                st.step_diff_sigma * sqrt(ls.step_var / double(ls.n_var_count));
+  }
+  const bool ready = it >= st.max_iterations || converged || stalled;
+  const bool stop = (it >= st.min_iterations && ready) || it >= st.hard_cap;
+  ls.has_converged = converged;
+  ls.has_stalled = stalled;
+  ls.done = stop;
+  return stop;
+}
+
 template <int NPOL>
 __global__ void __launch_bounds__(kThreads) finalize_kernel(const FinParams p) {
-  const uint32_t n_items = p.n_cb * p.n_ant * p.n_sub;
-  const uint32_t item = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t group = p.block_group[blockIdx.x];
+  const uint32_t item = p.block_item0[blockIdx.x] + threadIdx.x;
   double norm_sum = 0.0;
   uint32_t norm_cnt = 0;
   const DevSettings st = *p.settings;
-  if (item < n_items) {
+  // an interval that has stopped keeps its solutions
+  const bool frozen = !p.host_mode && p.state[group].done;
+  if (item < p.block_item_end[blockIdx.x] && !frozen) {
     const uint32_t cb = item / (p.n_ant * p.n_sub);
     const uint32_t rem = item - cb * p.n_ant * p.n_sub;
     const uint32_t ant = rem / p.n_sub;
@@ -692,52 +744,32 @@ __global__ void __launch_bounds__(kThreads) finalize_kernel(const FinParams p) {
     p.block_sum[blockIdx.x] = s_sum[0];
     p.block_cnt[blockIdx.x] = s_cnt[0];
     __threadfence();
-    const uint32_t prev = atomicAdd(&p.state->blocks_done, 1u);
+    const uint32_t prev = atomicAdd(&p.state[0].blocks_done, 1u);
     s_last = (prev == gridDim.x - 1);
   }
   __syncthreads();
-  if (!s_last || threadIdx.x != 0) return;
+  if (!s_last) return;
   __threadfence();
-  double sum = 0.0;
-  uint64_t cnt = 0;
-  for (uint32_t b = 0; b < gridDim.x; ++b) {
-    sum += reinterpret_cast<volatile double*>(p.block_sum)[b];
-    cnt += reinterpret_cast<volatile uint32_t*>(p.block_cnt)[b];
-  }
-  LoopState& ls = *p.state;
-  ls.blocks_done = 0;
-  // AssignSolutions (SolverBase.cc:297-306), no constraints: accuracy.
-  const double mag = cnt == 0 ? 0.0 : sum / st.step_size / double(cnt);
-  const uint32_t it = ls.iteration + 1;
-  ls.iteration = it;
-  if (it <= st.hard_cap) p.step_magnitudes[it - 1] = mag;
-  const bool converged = mag <= st.accuracy;
-  // ReachedStoppingCriterion / DetectStall (SolverBase.h:274-285,
-  // SolverBase.cc:63-86)
-  bool stalled = false;
-  if (st.detect_stalling) {
-    if (it == 1) {
-      ls.n_var_count = 1;
-      ls.step_mean = mag;
-      ls.step_var = 0.0;
-    } else {
-      ls.n_var_count += 1;
-      const double delta_1 = mag - ls.step_mean;
-      ls.step_mean += delta_1 / double(ls.n_var_count);
-      const double delta_2 = mag - ls.step_mean;
-      ls.step_var += delta_1 * delta_2;
+  // The last block runs the control step of every interval still going, one
+  // thread per interval, in a fixed block order.
+  bool active = false;
+  for (uint32_t g = threadIdx.x; g < p.n_groups; g += blockDim.x) {
+    LoopState& ls = p.state[g];
+    if (ls.done) continue;
+    double sum = 0.0;
+    uint64_t cnt = 0;
+    for (uint32_t b = p.group_blocks[g]; b < p.group_blocks[g + 1]; ++b) {
+      sum += reinterpret_cast<volatile double*>(p.block_sum)[b];
+      cnt += reinterpret_cast<volatile uint32_t*>(p.block_cnt)[b];
     }
-    if (it >= 30)
-      stalled = ls.step_mean <
-                st.step_diff_sigma * sqrt(ls.step_var / double(ls.n_var_count));
+    const bool stop = ControlStep(ls, st, sum, cnt, p.step_magnitudes + size_t(g) * p.mags_stride);
+    active = active || !stop;
   }
-  const bool ready = it >= st.max_iterations || converged || stalled;
-  const bool stop = (it >= st.min_iterations && ready) || it >= st.hard_cap;
-  ls.has_converged = converged;
-  ls.has_stalled = stalled;
-  ls.done = stop;
-  if (p.use_handle) cudaGraphSetConditional(p.handle, stop ? 0u : 1u);
+  if (threadIdx.x == 0) p.state[0].blocks_done = 0;
+  active = __syncthreads_or(active);
+  if (threadIdx.x == 0 && p.use_handle) cudaGraphSetConditional(p.handle, active ? 1u : 0u);
 }
+
 
 // ---------------------------------------------------------------------------
 // pipe_kernel: the Blackwell streaming path. Per CTA one producer warp moves
@@ -1877,6 +1909,12 @@ struct ddsolve_ctx {
   // solver state
   DevBuf d_sol, d_next, d_state, d_nonfinite, d_mags, d_settings;
   DevBuf d_chain;  // outputs of ddsolve_perform_iterations
+  // independent solution intervals (ddsolve_set_intervals): interval g owns
+  // channel blocks [group_first_cb[g], group_first_cb[g + 1])
+  uint32_t n_groups = 1;
+  std::vector<uint32_t> group_first_cb;
+  uint32_t mags_stride = 1;
+  DevBuf d_block_group, d_block_item0, d_block_item_end, d_group_blocks, d_cb_group;
   // graph
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -2407,8 +2445,8 @@ int BuildPlan(ddsolve_ctx* ctx) {
   // Pipelined kernel when the direction count, the correlation layout and the
   // shared memory allow it (and no lane groups were requested).
   ctx->use_pipe = false;
-  if (ctx->tune_ng == 0 && ctx->tune_pipe != 0 && (ctx->n_corr == 2 || ctx->n_corr == 4) &&
-      !std::getenv("DDSOLVE_NO_PIPE")) {
+  if (ctx->tune_ng == 0 && ctx->tune_pipe != 0 && ctx->n_groups == 1 &&
+      (ctx->n_corr == 2 || ctx->n_corr == 4) && !std::getenv("DDSOLVE_NO_PIPE")) {
     const KernelEntry* pe =
         FindPipeKernel(int(ctx->n_corr), int(ctx->n_pol), int(ctx->n_dir));
     const uint32_t acc_stride = OddAtLeast(ctx->n_dir * ctx->n_pol * 3);
@@ -2581,8 +2619,24 @@ int BuildPlan(ddsolve_ctx* ctx) {
   }
   fin_off[lists.size()] = uint32_t(fin_visits.size());
 
-  const uint32_t n_items = ctx->n_cb * ctx->n_ant * ctx->n_sub;
-  ctx->fin_blocks = (n_items + kThreads - 1) / kThreads;
+  // Finalisation blocks: each covers items (cb, antenna, sub-solution) of one
+  // interval only, so that its norm partial belongs to that interval.
+  const uint32_t per_cb_items = ctx->n_ant * ctx->n_sub;
+  std::vector<uint32_t> block_group, block_item0, block_item_end, group_blocks(1, 0);
+  std::vector<uint32_t> cb_group(ctx->n_cb, 0);
+  for (uint32_t g = 0; g < ctx->n_groups; ++g) {
+    const uint32_t cb0 = ctx->n_groups == 1 ? 0 : ctx->group_first_cb[g];
+    const uint32_t cb1 = ctx->n_groups == 1 ? ctx->n_cb : ctx->group_first_cb[g + 1];
+    for (uint32_t cb = cb0; cb < cb1; ++cb) cb_group[cb] = g;
+    const uint32_t i0 = cb0 * per_cb_items, i1 = cb1 * per_cb_items;
+    for (uint32_t i = i0; i < i1; i += kThreads) {
+      block_group.push_back(g);
+      block_item0.push_back(i);
+      block_item_end.push_back(std::min(i1, i + kThreads));
+    }
+    group_blocks.push_back(uint32_t(block_group.size()));
+  }
+  ctx->fin_blocks = uint32_t(block_group.size());
 
   auto upload = [&](DevBuf& b, const void* src, size_t bytes) -> int {
     DDS_CHECK_CUDA(ctx, b.Reserve(bytes));
@@ -2592,6 +2646,12 @@ int BuildPlan(ddsolve_ctx* ctx) {
     return DDSOLVE_OK;
   };
   int rc;
+  if ((rc = upload(ctx->d_block_group, block_group.data(), block_group.size() * 4))) return rc;
+  if ((rc = upload(ctx->d_block_item0, block_item0.data(), block_item0.size() * 4))) return rc;
+  if ((rc = upload(ctx->d_block_item_end, block_item_end.data(), block_item_end.size() * 4)))
+    return rc;
+  if ((rc = upload(ctx->d_group_blocks, group_blocks.data(), group_blocks.size() * 4))) return rc;
+  if ((rc = upload(ctx->d_cb_group, cb_group.data(), cb_group.size() * 4))) return rc;
   if ((rc = upload(ctx->d_slabs, descs.data(), descs.size() * sizeof(SlabDesc)))) return rc;
   if ((rc = upload(ctx->d_visits, visits.data(), visits.size() * sizeof(Visit)))) return rc;
   if ((rc = upload(ctx->d_cta_off, cta_off.data(), cta_off.size() * 4))) return rc;
@@ -2657,6 +2717,12 @@ FinParams MakeFinParams(ddsolve_ctx* ctx, bool host_mode) {
   f.step_magnitudes = ctx->d_mags.as<double>();
   f.handle = ctx->handle;
   f.use_handle = 0;
+  f.block_group = ctx->d_block_group.as<uint32_t>();
+  f.block_item0 = ctx->d_block_item0.as<uint32_t>();
+  f.block_item_end = ctx->d_block_item_end.as<uint32_t>();
+  f.group_blocks = ctx->d_group_blocks.as<uint32_t>();
+  f.n_groups = ctx->n_groups;
+  f.mags_stride = ctx->mags_stride;
   return f;
 }
 
@@ -2757,11 +2823,15 @@ int LaunchMakeFinite(ddsolve_ctx* ctx, bool use_handle) {
   if (ctx->n_pol == 2)
     make_finite_kernel<2><<<ctx->n_cb, kThreads, 0, ctx->stream>>>(
         ctx->d_sol.as<double2>(), ctx->d_nonfinite.as<uint32_t>(), per_cb,
-        ctx->handle, use_handle ? 1 : 0);
+        ctx->handle, use_handle ? 1 : 0,
+        ctx->n_groups > 1 ? ctx->d_cb_group.as<uint32_t>() : nullptr,
+        ctx->d_state.as<LoopState>());
   else
     make_finite_kernel<1><<<ctx->n_cb, kThreads, 0, ctx->stream>>>(
         ctx->d_sol.as<double2>(), ctx->d_nonfinite.as<uint32_t>(), per_cb,
-        ctx->handle, use_handle ? 1 : 0);
+        ctx->handle, use_handle ? 1 : 0,
+        ctx->n_groups > 1 ? ctx->d_cb_group.as<uint32_t>() : nullptr,
+        ctx->d_state.as<LoopState>());
   DDS_CHECK_CUDA(ctx, cudaGetLastError());
   return DDSOLVE_OK;
 }
@@ -2886,7 +2956,8 @@ int UploadSettings(ddsolve_ctx* ctx) {
   DDS_CHECK_CUDA(ctx, ctx->d_settings.Reserve(sizeof(DevSettings)));
   DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->d_settings.ptr, &ds, sizeof(ds),
                                       cudaMemcpyHostToDevice, ctx->stream));
-  DDS_CHECK_CUDA(ctx, ctx->d_mags.Reserve(size_t(ds.hard_cap) * 8));
+  ctx->mags_stride = ds.hard_cap;
+  DDS_CHECK_CUDA(ctx, ctx->d_mags.Reserve(size_t(ds.hard_cap) * ctx->n_groups * 8));
   // keep `ds` alive until the copy has been issued from pageable memory
   DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return DDSOLVE_OK;
@@ -3213,17 +3284,25 @@ int ddsolve_set_channel_block(ddsolve_ctx* ctx, uint32_t cbi, uint64_t n_vis,
   return UploadAndPack(ctx, cb, data, model);
 }
 
-int ddsolve_solve(ddsolve_ctx* ctx, double* solutions, ddsolve_result* result,
-                  double* step_magnitudes) {
-  if (!ctx || !solutions) return DDSOLVE_E_INVALID;
+}  // extern "C"
+
+namespace {
+
+// The solve of ddsolve_solve (one interval) and ddsolve_solve_batch (every
+// interval of the context): results[g] and step_magnitudes[g * cap] per
+// interval g.
+int SolveImpl(ddsolve_ctx* ctx, double* solutions, ddsolve_result* results,
+              double* step_magnitudes) {
   cudaSetDevice(ctx->device);
   int rc;
   bool solve_powers = false;
   if (ctx->plan_dirty && (rc = BuildPlan(ctx)) != DDSOLVE_OK) return rc;
+  const uint32_t n_groups = ctx->n_groups;
   const size_t n_sol = size_t(ctx->n_cb) * ctx->n_ant * ctx->n_sub * ctx->n_pol;
   DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->d_sol.ptr, solutions, n_sol * sizeof(double2),
                                       cudaMemcpyDefault, ctx->stream));
-  DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_state.ptr, 0, sizeof(LoopState), ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_state.ptr, 0, sizeof(LoopState) * n_groups,
+                                      ctx->stream));
   DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_nonfinite.ptr, 1, size_t(ctx->n_cb) * 4,
                                       ctx->stream));
   if (ctx->use_pipe) {
@@ -3252,11 +3331,12 @@ int ddsolve_solve(ddsolve_ctx* ctx, double* solutions, ddsolve_result* result,
     }
   }
   LoopState ls{};
+  std::vector<LoopState> states(n_groups);
   const size_t n_mags = std::max(std::max(ctx->settings.max_iterations,
                                           ctx->settings.min_iterations), 1u);
   DDS_CHECK_CUDA(ctx, ctx->ReserveStage(n_mags));
   bool staged = false;
-  if (ctx->graph_ok) {
+  if (ctx->graph_ok && n_groups == 1) {
     DDS_CHECK_CUDA(ctx, cudaGraphLaunch(ctx->graph_exec, ctx->stream));
     DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(&ctx->h_stage->ls, ctx->d_state.ptr, sizeof(ls),
                                         cudaMemcpyDeviceToHost, ctx->stream));
@@ -3265,46 +3345,104 @@ int ddsolve_solve(ddsolve_ctx* ctx, double* solutions, ddsolve_result* result,
                                           cudaMemcpyDeviceToHost, ctx->stream));
     if ((rc = StageCounters(ctx)) != DDSOLVE_OK) return rc;
     staged = true;
+  } else if (ctx->graph_ok) {
+    DDS_CHECK_CUDA(ctx, cudaGraphLaunch(ctx->graph_exec, ctx->stream));
   } else {
     const uint32_t cap = std::max(std::max(ctx->settings.max_iterations,
                                            ctx->settings.min_iterations), 1u);
     for (uint32_t it = 0; it < cap; ++it) {
       if ((rc = LaunchIteration(ctx, false, false, true)) != DDSOLVE_OK) return rc;
-      DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(&ls, ctx->d_state.ptr, sizeof(ls),
+      DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(states.data(), ctx->d_state.ptr,
+                                          sizeof(LoopState) * n_groups,
                                           cudaMemcpyDeviceToHost, ctx->stream));
       DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-      if (ls.done) break;
+      bool all_done = true;
+      for (const LoopState& st : states) all_done = all_done && st.done;
+      if (all_done) break;
     }
   }
   DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(solutions, ctx->d_sol.ptr, n_sol * sizeof(double2),
                                       cudaMemcpyDefault, ctx->stream));
   DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  if (staged) ls = ctx->h_stage->ls;
-  if (step_magnitudes && ls.iteration > 0) {
+  if (staged) {
+    states[0] = ctx->h_stage->ls;
+  } else {
+    DDS_CHECK_CUDA(ctx, cudaMemcpy(states.data(), ctx->d_state.ptr,
+                                   sizeof(LoopState) * n_groups, cudaMemcpyDeviceToHost));
+  }
+  uint32_t max_it = 0;
+  for (uint32_t g = 0; g < n_groups; ++g) {
+    const LoopState& st = states[g];
+    max_it = std::max(max_it, st.iteration);
+    if (!step_magnitudes || st.iteration == 0) continue;
+    const size_t n = std::min<size_t>(st.iteration, n_mags);
     if (staged) {
-      memcpy(step_magnitudes, ctx->h_stage->mags,
-             std::min<size_t>(ls.iteration, n_mags) * 8);
+      memcpy(step_magnitudes, ctx->h_stage->mags, n * 8);
     } else {
-      DDS_CHECK_CUDA(ctx, cudaMemcpy(step_magnitudes, ctx->d_mags.ptr,
-                                     size_t(ls.iteration) * 8, cudaMemcpyDeviceToHost));
+      DDS_CHECK_CUDA(ctx, cudaMemcpy(step_magnitudes + g * n_mags,
+                                     ctx->d_mags.as<double>() + size_t(g) * ctx->mags_stride,
+                                     n * 8, cudaMemcpyDeviceToHost));
     }
   }
   // pipe path: make_finite + build_tables (+ power_kernel) + one pipe_kernel
   // per iteration; else three kernels per iteration
-  ctx->last_launches = ctx->use_pipe
-                           ? uint64_t(ls.iteration) + 2 + (solve_powers ? 1 : 0)
-                           : uint64_t(ls.iteration) * 3;
+  ctx->last_launches = ctx->use_pipe ? uint64_t(max_it) + 2 + (solve_powers ? 1 : 0)
+                                     : uint64_t(max_it) * 3;
   // the model powers are fresh for one solve only (see LaunchPowers)
   ctx->powers_dirty = true;
   if ((rc = CheckDeviceError(ctx, staged)) != DDSOLVE_OK) return rc;
-  if (result) {
-    // SolverBase::MakeResult (SolverBase.cc:192-213), constraints satisfied.
-    result->iterations = ls.has_converged ? ls.iteration : ls.iteration + 1;
-    result->constraint_iterations = 0;
-    result->has_converged = ls.has_converged;
-    result->has_stalled = ls.has_stalled;
-  }
+  if (results)
+    for (uint32_t g = 0; g < n_groups; ++g) {
+      // SolverBase::MakeResult (SolverBase.cc:192-213), constraints satisfied.
+      const LoopState& st = states[g];
+      results[g].iterations = st.has_converged ? st.iteration : st.iteration + 1;
+      results[g].constraint_iterations = 0;
+      results[g].has_converged = st.has_converged;
+      results[g].has_stalled = st.has_stalled;
+    }
   return DDSOLVE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ddsolve_solve(ddsolve_ctx* ctx, double* solutions, ddsolve_result* result,
+                  double* step_magnitudes) {
+  if (!ctx || !solutions) return DDSOLVE_E_INVALID;
+  if (ctx->n_groups != 1)
+    return ctx->Fail(DDSOLVE_E_STATE,
+                     "the context holds several intervals: use ddsolve_solve_batch");
+  return SolveImpl(ctx, solutions, result, step_magnitudes);
+}
+
+int ddsolve_solve_batch(ddsolve_ctx* ctx, double* solutions, ddsolve_result* results,
+                        double* step_magnitudes) {
+  if (!ctx || !solutions) return DDSOLVE_E_INVALID;
+  return SolveImpl(ctx, solutions, results, step_magnitudes);
+}
+
+int ddsolve_set_intervals(ddsolve_ctx* ctx, uint32_t n_intervals,
+                          const uint32_t* first_channel_block) {
+  if (!ctx || n_intervals == 0) return DDSOLVE_E_INVALID;
+  if (n_intervals > 1) {
+    if (!first_channel_block || first_channel_block[0] != 0 ||
+        first_channel_block[n_intervals] != ctx->n_cb)
+      return ctx->Fail(DDSOLVE_E_INVALID, "intervals must cover channel blocks 0..n_cb");
+    for (uint32_t g = 0; g < n_intervals; ++g)
+      if (first_channel_block[g + 1] <= first_channel_block[g])
+        return ctx->Fail(DDSOLVE_E_INVALID, "every interval needs at least one channel block");
+  }
+  cudaSetDevice(ctx->device);
+  ctx->n_groups = n_intervals;
+  if (n_intervals > 1)
+    ctx->group_first_cb.assign(first_channel_block, first_channel_block + n_intervals + 1);
+  else
+    ctx->group_first_cb = {0u, ctx->n_cb};
+  DDS_CHECK_CUDA(ctx, ctx->d_state.Reserve(sizeof(LoopState) * n_intervals));
+  ctx->plan_dirty = true;
+  ctx->DestroyGraph();
+  return UploadSettings(ctx);
 }
 
 int ddsolve_perform_iteration(ddsolve_ctx* ctx, const double* solutions,

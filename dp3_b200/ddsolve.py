@@ -24,7 +24,7 @@ EXPORTED_SYMBOLS = (
     "ddsolve_set_tuning", "ddsolve_time_stream_kernel",
     "ddsolve_last_launch_count", "ddsolve_perform_iteration_noalloc",
     "ddsolve_perform_iterations", "ddsolve_get_tuning", "ddsolve_set_plan_tuning",
-    "ddsolve_autotune",
+    "ddsolve_autotune", "ddsolve_set_intervals", "ddsolve_solve_batch",
 )
 
 
@@ -94,6 +94,8 @@ def lib():
         L.ddsolve_solve.argtypes = [vp, vp, ctypes.POINTER(Result), vp]
         L.ddsolve_perform_iteration.argtypes = [vp, vp, vp]
         L.ddsolve_perform_iterations.argtypes = [vp, vp, u32, vp]
+        L.ddsolve_set_intervals.argtypes = [vp, u32, vp]
+        L.ddsolve_solve_batch.argtypes = [vp, vp, vp, vp]
         L.ddsolve_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
         L.ddsolve_set_plan_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
         L.ddsolve_autotune.argtypes = [vp, u32, ctypes.POINTER(Tuning),
@@ -230,6 +232,22 @@ class Context:
                                                     _addr(nxt)),
                     "ddsolve_perform_iteration")
         return nxt
+
+    def set_intervals(self, first_channel_block):
+        """Independent intervals: channel blocks [first[g], first[g+1])."""
+        f = np.ascontiguousarray(first_channel_block, np.uint32)
+        self._check(lib().ddsolve_set_intervals(self._h, len(f) - 1, _addr(f)),
+                    "ddsolve_set_intervals")
+        self.n_intervals = len(f) - 1
+
+    def solve_batch(self, solutions, step_magnitudes=None):
+        """Solves every interval; solutions [n_cb, ...] updated in place.
+        Returns the list of per-interval Results."""
+        n = getattr(self, "n_intervals", 1)
+        res = (Result * n)()
+        self._check(lib().ddsolve_solve_batch(self._h, _addr(solutions), res,
+                                              _addr(step_magnitudes)), "ddsolve_solve_batch")
+        return list(res)
 
     def perform_iterations(self, start, n_passes):
         """n_passes chained PerformIteration passes from `start`; returns

@@ -152,6 +152,25 @@ DDSOLVE_API int ddsolve_set_channel_block_regular(ddsolve_ctx* ctx, uint32_t cha
 DDSOLVE_API int ddsolve_solve(ddsolve_ctx* ctx, double* solutions, ddsolve_result* result,
                   double* step_magnitudes);
 
+/* Several independent solution intervals in one context (no counterpart in
+ * the reference, which solves one interval per Solve call): channel blocks
+ * [first_channel_block[g], first_channel_block[g + 1]) form interval g, for
+ * g < n_intervals (first_channel_block[0] = 0, first_channel_block[n] =
+ * n_channel_blocks; NULL with n_intervals = 1 restores one interval). Every
+ * interval has its own iteration count, convergence, stall detection and
+ * stopping, exactly as if solved alone; one streaming pass per iteration
+ * covers all intervals still iterating, and an interval that has stopped
+ * keeps its solutions. Batched contexts run on the stream_kernel path. */
+DDSOLVE_API int ddsolve_set_intervals(ddsolve_ctx* ctx, uint32_t n_intervals,
+                                      const uint32_t* first_channel_block);
+
+/* ddsolve_solve for every interval of the context: results[g] per interval,
+ * step_magnitudes (optional) [n_intervals][max(max_iterations,
+ * min_iterations, 1)]. ddsolve_solve refuses a context with several
+ * intervals. */
+DDSOLVE_API int ddsolve_solve_batch(ddsolve_ctx* ctx, double* solutions, ddsolve_result* results,
+                                    double* step_magnitudes);
+
 /* One direction-iterative pass over every channel block:
  * next_solutions = sum(num) / sum(den) per antenna, sub-solution and
  * polarization, NaN where the denominator is zero -- exactly the

@@ -404,3 +404,53 @@ def test_autotune_keeps_results_and_caches(built):
         err = np.abs(got - expect) / np.maximum(np.abs(expect), 1e-12)
         assert np.nanmax(err) < RTOL_PASS, t
         c.close()
+
+
+def test_batched_intervals_match_separate_solves(built):
+    """Three independent intervals in one context (ddsolve_set_intervals /
+    ddsolve_solve_batch) give each interval the iteration count and the
+    solutions of its own solve: intervals stop at different iterations and a
+    stopped interval keeps its solutions while the others go on."""
+    from dp3_b200 import ddsolve
+    obs_list = [synth.observe(synth.small_config(n_stations=12, n_directions=3, n_channels=8,
+                                                 n_cb=2, n_times=2, seed=seed))
+                for seed in (21, 22, 23)]
+    cfg = obs_list[0].cfg
+    n_sub = sum(cfg.nspd)
+    st = ddsolve.default_settings()
+    st.max_iterations, st.accuracy, st.step_size = 150, 1e-5, 0.2
+    singles = []
+    for obs in obs_list:
+        ctx = ddsolve.Context(cfg.n_stations, cfg.nspd, cfg.n_channel_blocks, 2, 2)
+        ctx.set_settings(st)
+        for cb, nc in enumerate(cfg.cb_channels):
+            ctx.set_channel_block_regular(cb, cfg.n_times, cfg.n_baselines, nc, obs.data[cb],
+                                          obs.model[cb], obs.antenna1, obs.antenna2)
+        sol = np.ones((cfg.n_channel_blocks, cfg.n_stations, n_sub, 2), np.complex128)
+        mags = np.zeros(150)
+        r = ctx.solve(sol, mags)
+        singles.append((r, sol, mags))
+        ctx.close()
+    n_cb = cfg.n_channel_blocks
+    ctx = ddsolve.Context(cfg.n_stations, cfg.nspd, 3 * n_cb, 2, 2)
+    ctx.set_settings(st)
+    ctx.set_intervals([0, n_cb, 2 * n_cb, 3 * n_cb])
+    for g, obs in enumerate(obs_list):
+        for cb, nc in enumerate(cfg.cb_channels):
+            ctx.set_channel_block_regular(g * n_cb + cb, cfg.n_times, cfg.n_baselines, nc,
+                                          obs.data[cb], obs.model[cb], obs.antenna1,
+                                          obs.antenna2)
+    sol = np.ones((3 * n_cb, cfg.n_stations, n_sub, 2), np.complex128)
+    mags = np.zeros((3, 150))
+    res = ctx.solve_batch(sol, mags)
+    with pytest.raises(RuntimeError):
+        ctx.solve(np.ones_like(sol))
+    ctx.close()
+    its = [r.iterations for r, _, _ in singles]
+    assert len(set(its)) > 1, its  # the intervals stop at different iterations
+    for g, (r, s1, m1) in enumerate(singles):
+        assert res[g].iterations == r.iterations
+        assert res[g].has_converged == r.has_converged
+        assert H.max_rel_diff(sol[g * n_cb:(g + 1) * n_cb], s1) < RTOL_SOLVE
+        n = min(r.iterations, 150)
+        np.testing.assert_allclose(mags[g, :n], m1[:n], rtol=1e-3, atol=1e-12)
