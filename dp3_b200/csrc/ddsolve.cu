@@ -3519,6 +3519,12 @@ int ddsolve_perform_iterations(ddsolve_ctx* ctx, const double* start, uint32_t n
   }
   DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(outputs, ctx->d_chain.ptr, bytes * n_passes,
                                       cudaMemcpyDefault, ctx->stream));
+  ctx->last_launches = launches;
+  cudaPointerAttributes attr{};
+  const bool dev_out = cudaPointerGetAttributes(&attr, outputs) == cudaSuccess &&
+                       (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged);
+  cudaGetLastError();
+  if (dev_out) return DDSOLVE_OK;  // device outputs: no wait (see the header)
   if ((rc = StageCounters(ctx)) != DDSOLVE_OK) return rc;
   DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   ctx->last_launches = launches;

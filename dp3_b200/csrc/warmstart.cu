@@ -502,8 +502,9 @@ struct ddwarm_ctx {
     err = m;
     return code;
   }
+  cudaStream_t own_stream = nullptr;  // created by the context; `stream` may be a caller's
   ~ddwarm_ctx() {
-    if (stream) cudaStreamDestroy(stream);
+    if (own_stream) cudaStreamDestroy(own_stream);
   }
 };
 
@@ -738,7 +739,9 @@ int ddwarm_create(uint32_t n_in, uint32_t n_hidden, uint32_t n_out, uint64_t see
     delete ctx;
     return code;
   };
-  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(2);
+  if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(2);
+  ctx->stream = ctx->own_stream;
   if (cudaFuncSetAttribute(gemm_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            int(GemmSmem<256>())) != cudaSuccess ||
       cudaFuncSetAttribute(gemm_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1004,9 +1007,19 @@ int ddwarm_predict_start(ddwarm_ctx* ctx, const ddwarm_layout* lay, uint32_t n_s
                                              lay->n_channel_blocks, lay->n_antennas, lay->n_sub,
                                              lay->n_pol, lay->scale, out);
   WARM_CHECK(ctx, cudaGetLastError());
-  if (!dev_out)
+  if (!dev_out) {
     WARM_CHECK(ctx, cudaMemcpyAsync(start, out, n_sol * 16, cudaMemcpyDeviceToHost, ctx->stream));
-  return CheckError(ctx);
+    return CheckError(ctx);
+  }
+  return 0;  // device output: no wait (see the header)
+}
+
+int ddwarm_set_stream(ddwarm_ctx* ctx, void* stream) {
+  if (!ctx) return 1;
+  cudaSetDevice(ctx->device);
+  WARM_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+  return 0;
 }
 
 }  // extern "C"

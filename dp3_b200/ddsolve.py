@@ -249,15 +249,18 @@ class Context:
                                               _addr(step_magnitudes)), "ddsolve_solve_batch")
         return list(res)
 
-    def perform_iterations(self, start, n_passes):
+    def perform_iterations(self, start, n_passes, out=None):
         """n_passes chained PerformIteration passes from `start`; returns
         [n_passes] + start.shape (pass k starts from pass k - 1's output).
-        A CUDA torch tensor in gives a CUDA tensor out (no host copies)."""
+        A CUDA torch tensor in gives a CUDA tensor out (no host copies, and
+        the call returns without waiting: the passes are ordered on this
+        context's stream); `out` may supply that tensor."""
         if _is_torch(start):
             import torch
             start = start.contiguous()
-            out = torch.empty((n_passes,) + tuple(start.shape), dtype=torch.complex128,
-                              device=start.device)
+            if out is None:
+                out = torch.empty((n_passes,) + tuple(start.shape), dtype=torch.complex128,
+                                  device=start.device)
         else:
             start = np.ascontiguousarray(start, dtype=np.complex128)
             out = np.empty((n_passes,) + start.shape, np.complex128)

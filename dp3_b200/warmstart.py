@@ -38,6 +38,7 @@ EXPORTED_SYMBOLS = (
     "ddwarm_create", "ddwarm_destroy", "ddwarm_last_error", "ddwarm_param_count",
     "ddwarm_get_params", "ddwarm_set_params", "ddwarm_predict",
     "ddwarm_gradients", "ddwarm_train", "ddwarm_features", "ddwarm_predict_start",
+    "ddwarm_set_stream",
 )
 
 _lib = None
@@ -68,6 +69,7 @@ def lib():
         L.ddwarm_train.argtypes = [vp, u32, vp, vp, u32, u32, f32, u64, vp]
         L.ddwarm_features.argtypes = [vp, vp, u32, vp, vp]
         L.ddwarm_predict_start.argtypes = [vp, vp, u32, vp, vp]
+        L.ddwarm_set_stream.argtypes = [vp, vp]
         _lib = L
     return _lib
 
@@ -199,12 +201,18 @@ class Stage:
         return self.mlp.train(np.concatenate(self.x), np.concatenate(self.t), epochs=epochs,
                               batch=batch, lr=lr, seed=seed)
 
-    def predict(self, sets):
-        """Initial solutions, on the device of sets[0] (numpy in, numpy out)."""
+    def set_stream(self, stream_ptr):
+        """Runs this network's work on a CUDA stream (e.g. the solver's)."""
+        self.mlp._check(lib().ddwarm_set_stream(self.mlp._h, ctypes.c_void_p(stream_ptr)))
+
+    def predict(self, sets, out=None):
+        """Initial solutions, on the device of sets[0] (numpy in, numpy out;
+        CUDA tensors in: a CUDA tensor out, `out` if given, and the call
+        returns without waiting)."""
         arrs, ptrs = _sets_arg(sets)
         if hasattr(arrs[0], "data_ptr"):
             import torch
-            start = torch.empty_like(arrs[0])
+            start = torch.empty_like(arrs[0]) if out is None else out
             out = ctypes.c_void_p(start.data_ptr())
         else:
             start = np.empty_like(arrs[0])
@@ -280,11 +288,36 @@ class LearnedWarmStart:
 
     def start(self, solver, history):
         """Initial solutions of the interval loaded in `solver`. With the
-        history as CUDA tensors every step stays on the GPU."""
-        z = solver.perform_iterations(history[0], self.k1)
-        g1 = self.stage1.predict(list(history[:self.HISTORY]) + list(z))
-        y = solver.perform_iterations(g1, self.k2)
-        return self.stage2.predict([g1] + list(y))
+        history as CUDA tensors every step stays on the GPU, on the solver's
+        stream, without host waits (the solve that follows orders after it);
+        the result is a new CUDA tensor whose pending work is on the solver's
+        stream: solve from it, or synchronize before dropping it."""
+        h1 = history[0]
+        if not (hasattr(h1, "is_cuda") and h1.is_cuda):
+            z = solver.perform_iterations(h1, self.k1)
+            g1 = self.stage1.predict(list(history[:self.HISTORY]) + list(z))
+            y = solver.perform_iterations(g1, self.k2)
+            return self.stage2.predict([g1] + list(y))
+        import torch
+        ptr = solver.stream_ptr()
+        if getattr(self, "_stream", None) != ptr:
+            for st in (self.stage1, self.stage2):
+                st.set_stream(ptr)
+            self._stream = ptr
+            # persistent work buffers: reused in stream order by later calls
+            self._z = torch.empty((self.k1,) + tuple(h1.shape), dtype=h1.dtype, device=h1.device)
+            self._y = torch.empty((self.k2,) + tuple(h1.shape), dtype=h1.dtype, device=h1.device)
+            self._g1 = torch.empty_like(h1)
+            self._torch_stream = torch.cuda.ExternalStream(ptr, device=h1.device)
+        z = solver.perform_iterations(h1, self.k1, out=self._z)
+        self.stage1.predict(list(history[:self.HISTORY]) + list(z), out=self._g1)
+        y = solver.perform_iterations(self._g1, self.k2, out=self._y)
+        g2 = torch.empty_like(h1)
+        # g2 is written on the solver's stream: order that stream after the
+        # allocating one. The caller uses g2 on the solver's stream (the solve)
+        # or waits for it before dropping it.
+        self._torch_stream.wait_stream(torch.cuda.current_stream(h1.device))
+        return self.stage2.predict([self._g1] + list(y), out=g2)
 
     def close(self):
         for st in (self.stage1, self.stage2, self._provisional):

@@ -190,7 +190,9 @@ DDSOLVE_API int ddsolve_perform_iteration(ddsolve_ctx* ctx, const double* soluti
  * pass costs one streaming pass over the data. Replaces a host loop of
  * ddsolve_perform_iteration calls; the learned warm start
  * (include/ddwarm_b200.h) uses these undamped passes as residual statistics
- * of the current interval. */
+ * of the current interval. With `outputs` in device memory the call only
+ * enqueues the passes on the context's stream (ddsolve_stream) and returns; a
+ * bounded-wait failure then surfaces at the next call that waits. */
 DDSOLVE_API int ddsolve_perform_iterations(ddsolve_ctx* ctx, const double* start,
                                            uint32_t n_passes, double* outputs);
 

@@ -96,9 +96,18 @@ DDSOLVE_API int ddwarm_features(ddwarm_ctx* ctx, const ddwarm_layout* layout, ui
  * not finite take the base value. Features, forward pass and the update run
  * on the GPU. `sets` and `start` may be host arrays or, with unified
  * addressing, device memory of the context's device (for example the outputs
- * of ddsolve_perform_iterations kept on the device), which is read in place. */
+ * of ddsolve_perform_iterations kept on the device), which is read in place.
+ * With `start` in device memory the call only enqueues the work on the
+ * context's stream and returns; a bounded-wait failure then surfaces at the
+ * context's next call that waits (a host `start`, ddwarm_features, ...). */
 DDSOLVE_API int ddwarm_predict_start(ddwarm_ctx* ctx, const ddwarm_layout* layout,
                                      uint32_t n_sets, const double* const* sets, double* start);
+
+/* Runs the context's work on `stream` (a cudaStream_t of the same device,
+ * e.g. ddsolve_stream() of the solver, so that the warm start and the solve
+ * are ordered without host waits); NULL restores the context's own stream.
+ * Waits for the work already enqueued. */
+DDSOLVE_API int ddwarm_set_stream(ddwarm_ctx* ctx, void* stream);
 
 #ifdef __cplusplus
 }

@@ -241,3 +241,34 @@ def test_learned_warm_start_saves_iterations(built):
     for w, p in zip(d_w, d_p):
         assert w < max(PASS_RTOL, 1.5 * p), (w, p)
     assert max(d_wp) < 3 * PASS_RTOL, max(d_wp)
+
+
+@pytest.mark.gpu
+def test_device_start_matches_host_start(built):
+    """The asynchronous device path of LearnedWarmStart.start (solver stream,
+    no host waits) gives the start of the host path."""
+    import torch
+    from dp3_b200 import ddsolve
+    obs = H.small_observation(n_stations=10, n_directions=2, n_channels=8, n_cb=2,
+                              n_times=2, seed=9)
+    cfg = obs.cfg
+    n_sub = sum(cfg.nspd)
+    ctx = ddsolve.Context(cfg.n_stations, cfg.nspd, cfg.n_channel_blocks, 2, 2)
+    for cb, nc in enumerate(cfg.cb_channels):
+        ctx.set_channel_block_regular(cb, cfg.n_times, cfg.n_baselines, nc, obs.data[cb],
+                                      obs.model[cb], obs.antenna1, obs.antenna2)
+    ws = warmstart.LearnedWarmStart(cfg.n_channel_blocks, cfg.n_stations, n_sub, 2,
+                                    passes=(2, 2), hidden=64)
+    rng = np.random.default_rng(4)
+    shape = (cfg.n_channel_blocks, cfg.n_stations, n_sub, 2)
+    hist = [np.exp(0.05 * (rng.normal(size=shape) + 1j * rng.normal(size=shape)))
+            for _ in range(4)]
+    host = ws.start(ctx, hist)
+    dev = ws.start(ctx, [torch.from_numpy(h).cuda() for h in hist])
+    got = dev.cpu().numpy()  # waits for the solver's stream through the copy
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(got, host, rtol=1e-12)
+    r = ctx.solve(dev)
+    assert r.iterations > 0
+    ws.close()
+    ctx.close()
