@@ -97,6 +97,90 @@ class SolveData:
         return cls(blocks, n_correlations)
 
 
+class Constraint:
+    """dp3::ddecal::Constraint (ddecal/constraints/Constraint.h:28-90): the
+    hooks SolverBase::ApplyConstraints calls on the host between iterations.
+    Apply() receives next_solutions as an ndarray [n_cb, n_ant, n_sub, n_pol]
+    (complex128) and modifies it in place."""
+
+    def Satisfied(self):
+        return True
+
+    def PrepareIteration(self, has_reached_precision, iteration, final_iter):
+        pass
+
+    def Apply(self, solutions, time):
+        raise NotImplementedError
+
+    def GetResult(self):
+        return None
+
+
+class AntennaConstraint(Constraint):
+    """AntennaConstraint (ddecal/constraints/AntennaConstraint.h:29-82): the
+    antennas of each set get the mean of their finite solutions, per channel
+    block, sub-solution and polarization."""
+
+    def __init__(self, antenna_sets):
+        self.antenna_sets = [sorted(set(a)) for a in antenna_sets]
+
+    def Apply(self, solutions, time):
+        for ants in self.antenna_sets:
+            sel = solutions[:, ants]  # [cb, |set|, sub, pol]
+            finite = np.isfinite(sel)
+            total = np.where(finite, sel, 0).sum(axis=1)
+            with np.errstate(all="ignore"):
+                mean = total / finite.sum(axis=1)
+            solutions[:, ants] = mean[:, None]
+
+
+def make_solutions_finite(arr, n_pol):
+    """SolverBase::MakeSolutionsFinite1Pol / 2Pol (SolverBase.cc:316-371) on
+    [n_cb, per_cb] complex128, in place; the 2-pol version averages |pol 0|
+    for both polarizations, as the reference does (SolverBase.cc:354)."""
+    for cb in range(arr.shape[0]):
+        v = arr[cb].reshape(-1, n_pol)
+        ok = np.all(np.isfinite(v), axis=1)
+        avg = np.abs(v[ok, 0]).mean() if ok.any() else 1.0
+        v[~ok] = avg
+
+
+def step(solutions, nxt, step_size, phase_only):
+    """SolverBase::Step (SolverBase.cc:88-158): returns the moved solutions."""
+    if not phase_only:
+        return solutions * (1.0 - step_size) + nxt * step_size
+    frm = np.angle(solutions)
+    dist = np.angle(nxt) - frm
+    dist = np.where(dist > np.pi, dist - 2 * np.pi, np.where(dist < -np.pi, dist + 2 * np.pi, dist))
+    return np.exp(1j * (frm + step_size * dist))
+
+
+def assign_solutions(solutions, nxt, n_pol, step_size, accuracy):
+    """SolverBase::AssignSolutions (SolverBase.cc:215-306) for 1 or 2
+    polarizations: appends nothing, returns (step magnitude, converged) and
+    copies nxt into solutions."""
+    total, n = 0.0, 0
+    with np.errstate(all="ignore"):
+        if n_pol == 1:
+            s = solutions.reshape(-1)
+            ns = nxt.reshape(-1)
+            nz = s != 0
+            a = np.abs((ns[nz] - s[nz]) / s[nz])
+            fin = np.isfinite(a)
+            total, n = a[fin].sum(), int(fin.sum())
+        else:
+            s = solutions.reshape(-1, 2)
+            ns = nxt.reshape(-1, 2)
+            inv = 1.0 / s
+            ok = np.all(np.isfinite(inv), axis=1)
+            d = np.abs((ns[ok] - s[ok]) * inv[ok]).sum(axis=1)
+            fin = np.isfinite(d)
+            total, n = d[fin].sum(), 2 * int(fin.sum())
+    solutions[...] = nxt
+    mag = 0.0 if n == 0 else total / step_size / n
+    return mag, mag <= accuracy
+
+
 class SolverBase:
     """Settings and dimensions of dp3::ddecal::SolverBase, with its defaults
     (SolverBase.cc:27-39)."""
@@ -263,8 +347,9 @@ class SolverBase:
         receives the result. stat_stream, when given, receives one line per
         iteration with the step magnitude."""
         if self.constraints:
-            raise NotImplementedError(
-                "host constraints: drive the loop with PerformIteration()")
+            ctx = self._upload(data)
+            return self._solve_with_constraints(
+                lambda sol: ctx.perform_iteration(sol), solutions, time, stat_stream)
         ctx = self._upload(data)
         ctx.set_settings(self._settings)
         arr = self._solutions_array(solutions)
@@ -279,6 +364,62 @@ class SolverBase:
         return SolveResult(res.iterations, res.constraint_iterations, [],
                            bool(res.has_converged), bool(res.has_stalled),
                            mags[:n_it].copy())
+
+    def _solve_with_constraints(self, perform, solutions, time, stat_stream):
+        """IterativeDiagonalSolver::Solve / IterativeScalarSolver::Solve with
+        constraints (IterativeDiagonalSolver.cc:38-97, SolverBase.cc:160-306):
+        the pass runs on the GPU (`perform`: [n_cb, n_ant, n_sub, n_pol] ->
+        next_solutions), MakeSolutionsFinite, Step, the constraints,
+        AssignSolutions and the stopping criterion on the host, as in the
+        reference."""
+        st = self._settings
+        n_pol = self.NSolutionPolarizations()
+        shape4 = (self.n_channel_blocks, self.n_antennas, self.NSubSolutions(), n_pol)
+        arr = self._solutions_array(solutions).reshape(self.n_channel_blocks, -1)
+        for c in self.constraints:  # PrepareConstraints (SolverBase.cc:160-164)
+            c.PrepareIteration(False, 0, False)
+        iteration, has_converged, has_prev, satisfied = 0, False, False, False
+        mags = []
+        n_var, mean, var = 0, 0.0, 0.0
+        while True:
+            make_solutions_finite(arr, n_pol)
+            nxt = np.asarray(perform(arr.reshape(shape4)), np.complex128).reshape(shape4)
+            nxt = step(arr.reshape(shape4), nxt, st.step_size, bool(st.phase_only))
+            satisfied = True  # ApplyConstraints (SolverBase.cc:174-190)
+            for c in self.constraints:
+                satisfied = c.Satisfied() and satisfied
+                c.PrepareIteration(has_prev, iteration, iteration + 1 >= st.max_iterations)
+                c.Apply(nxt, time)
+            acc = st.constraint_accuracy if not satisfied else st.accuracy
+            mag, has_converged = assign_solutions(arr, nxt.reshape(arr.shape), n_pol,
+                                                  st.step_size, acc)
+            mags.append(mag)
+            iteration += 1
+            has_prev = has_converged or has_prev
+            # ReachedStoppingCriterion / DetectStall (SolverBase.h:274-285,
+            # SolverBase.cc:63-86)
+            stalled = False
+            if st.detect_stalling and satisfied:
+                if iteration == 1:
+                    n_var, mean, var = 1, mag, 0.0
+                else:
+                    n_var += 1
+                    d1 = mag - mean
+                    mean += d1 / n_var
+                    var += d1 * (mag - mean)
+                stalled = iteration >= 30 and mean < st.step_diff_sigma * np.sqrt(var / n_var)
+            ready = (iteration >= st.max_iterations or (has_converged and satisfied) or stalled)
+            if iteration >= st.min_iterations and ready:
+                break
+        self._store(solutions, arr)
+        if stat_stream is not None:
+            for i, m in enumerate(mags):
+                stat_stream.write(f"{i + 1} {m!r}\n")
+        # MakeResult (SolverBase.cc:192-213)
+        its = iteration if (has_converged and satisfied) else iteration + 1
+        c_its = iteration + 1 if not satisfied else 0
+        return SolveResult(its, c_its, [c.GetResult() for c in self.constraints],
+                           bool(has_converged), bool(stalled), np.array(mags))
 
     def PerformIteration(self, data: SolveData, solutions):
         """next_solutions of one direction-iterative pass (num / den), as the
