@@ -1265,6 +1265,10 @@ __global__ void __launch_bounds__(kPipeRuns) power_kernel(const SlabDesc* __rest
 
 template <int NCORR, int NPOL, int DMAX>
 __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams p) {
+  // An unrolled graph body launches the kernel more than once per loop test:
+  // a launch after the loop has stopped does nothing.
+  if (!p.host_mode && p.use_handle && static_cast<volatile const LoopState*>(p.state)->done)
+    return;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + kPipeMaxStages;
@@ -1912,6 +1916,7 @@ struct ddsolve_ctx {
   // independent solution intervals (ddsolve_set_intervals): interval g owns
   // channel blocks [group_first_cb[g], group_first_cb[g + 1])
   uint32_t n_groups = 1;
+  uint32_t graph_unroll = 4;  // pipe_kernel launches per graph loop test
   std::vector<uint32_t> group_first_cb;
   uint32_t mags_stride = 1;
   DevBuf d_block_group, d_block_item0, d_block_item_end, d_group_blocks, d_cb_group;
@@ -2924,7 +2929,14 @@ int BuildGraph(ddsolve_ctx* ctx) {
   DDS_CHECK_CUDA(ctx, cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr,
                                                      nullptr, 0,
                                                      cudaStreamCaptureModeThreadLocal));
-  const int rc = LaunchIteration(ctx, false, true, true);
+  // pipe_kernel: several iterations per loop test (launches after the loop
+  // stopped return at once); one otherwise.
+  int rc = DDSOLVE_OK;
+  uint32_t unroll = ctx->use_pipe ? ctx->graph_unroll : 1u;
+  if (const char* e = std::getenv("DDSOLVE_GRAPH_UNROLL"))
+    if (ctx->use_pipe) unroll = uint32_t(std::max(1, std::atoi(e)));
+  for (uint32_t u = 0; u < unroll && rc == DDSOLVE_OK; ++u)
+    rc = LaunchIteration(ctx, false, true, true);
   cudaGraph_t captured = nullptr;
   const cudaError_t end = cudaStreamEndCapture(ctx->stream, &captured);
   if (rc != DDSOLVE_OK) return rc;
