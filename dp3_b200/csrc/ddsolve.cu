@@ -1098,7 +1098,24 @@ __device__ __noinline__ void FinalizeDistributed(const PipeParams& p, int ctid,
   ConsumerBarrier();
   if (!*s_last) return;
   __threadfence();
+  // Channel blocks with new non-finite solutions, checked by all consumer
+  // threads at once (the serial pass below runs only when there are some).
+  uint32_t any_bad = 0;
   if (!p.host_mode) {
+    ConsumerBarrier();  // every thread has read *s_last above
+    if (ctid == 0) *s_last = 0u;
+    ConsumerBarrier();
+    for (uint32_t cb = ctid; cb < p.n_cb; cb += kPipeRuns) {
+      const bool bad = reinterpret_cast<volatile uint32_t*>(p.cb_newflag)[cb] != 0;
+      if (!bad)
+        p.cb_flag[cb] = 0u;
+      else
+        atomicOr(s_last, 1u);
+    }
+    ConsumerBarrier();
+    any_bad = *s_last;
+  }
+  if (!p.host_mode && any_bad) {
     // Replacement values for channel blocks with new non-finite solutions:
     // mean |pol 0| over finite pairs; the gain tables take the replacement
     // now, the solutions when the next finalisation reads them.
@@ -1156,13 +1173,30 @@ __device__ __noinline__ void FinalizeDistributed(const PipeParams& p, int ctid,
       ConsumerBarrier();
     }
   }
-  if (ctid != 0) return;
-  double sum = 0.0;
-  uint64_t cnt = 0;
-  for (uint32_t b = 0; b < gridDim.x; ++b) {
-    sum += reinterpret_cast<volatile double*>(p.block_sum)[b];
-    cnt += reinterpret_cast<volatile uint32_t*>(p.block_cnt)[b];
+  // The per-CTA norm partials, summed by all consumer threads of the last CTA
+  // in a fixed tree order (a serial sum by one thread sat on the critical
+  // path of every iteration).
+  {
+    double sum_t = 0.0;
+    uint32_t cnt_t = 0;
+    for (uint32_t b = ctid; b < gridDim.x; b += kPipeRuns) {
+      sum_t += reinterpret_cast<volatile double*>(p.block_sum)[b];
+      cnt_t += reinterpret_cast<volatile uint32_t*>(p.block_cnt)[b];
+    }
+    s_sum[ctid] = sum_t;
+    s_cnt[ctid] = cnt_t;
+    ConsumerBarrier();
+    for (int w = 128; w > 0; w >>= 1) {
+      if (ctid < w && ctid + w < kPipeRuns) {
+        s_sum[ctid] += s_sum[ctid + w];
+        s_cnt[ctid] += s_cnt[ctid + w];
+      }
+      ConsumerBarrier();
+    }
   }
+  if (ctid != 0) return;
+  const double sum = s_sum[0];
+  const uint64_t cnt = s_cnt[0];
   p.counters[0] = 0;
   p.counters[2] = 0;
   if (p.host_mode) return;
