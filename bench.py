@@ -330,6 +330,66 @@ def run_mlp_only(args):
     return 0
 
 
+def run_fp64_check(args):
+    """Solution error of the GPU solver against the FP64 oracle on
+    configuration `args.config` (a numerical statement, not a timing): one
+    pass from a perturbed start (max relative error per element) and the full
+    solve from unit solutions (iteration counts; max relative difference after
+    antenna-0 phase referencing), plus the same for the oracle with the
+    reference's FP32 arithmetic."""
+    from dp3_b200 import build as native_build
+    from dp3_b200 import ddsolve, synth
+    from oracle import oracle_ffi as of
+    native_build.build_all()
+    of.build()
+    cfg = synth.benchmark_configs()[args.config]
+    obs = synth.observe(cfg)
+    ap, sm = obs.generic_arrays()
+    npol = args.npol
+    prob = dict(n_antennas=cfg.n_stations, n_correlations=2, n_pol=npol,
+                n_solutions_per_direction=list(cfg.nspd), data=obs.data, model=obs.model,
+                antenna_pairs=ap, solution_map=sm)
+    n_sub = sum(cfg.nspd)
+    shape = (cfg.n_channel_blocks, cfg.n_stations, n_sub, npol)
+    ctx = ddsolve.Context(cfg.n_stations, cfg.nspd, cfg.n_channel_blocks, 2, npol)
+    for cb, nc in enumerate(cfg.cb_channels):
+        ctx.set_channel_block_regular(cb, cfg.n_times, cfg.n_baselines, nc, obs.data[cb],
+                                      obs.model[cb], obs.antenna1, obs.antenna2)
+    st = ddsolve.default_settings()
+    st.max_iterations, st.accuracy, st.step_size = (cfg.max_iterations, cfg.tolerance,
+                                                    cfg.step_size)
+    ctx.set_settings(st)
+    rng = np.random.default_rng(3)
+    start = np.exp(0.1 * (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)))
+    got = ctx.perform_iteration(start)
+    ref = of.perform_iteration(prob, start, precision=64)
+    ref32 = of.perform_iteration(prob, start, precision=32)
+    with np.errstate(all="ignore"):
+        pass_err = float(np.nanmax(np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300)))
+        pass_err32 = float(np.nanmax(np.abs(ref32 - ref) / np.maximum(np.abs(ref), 1e-300)))
+        # relative to the block's typical gain magnitude instead of each element
+        scale = np.nanmedian(np.abs(ref), axis=(1, 2, 3), keepdims=True)
+        pass_err_scaled = float(np.nanmax(np.abs(got - ref) / scale))
+        pass_err32_scaled = float(np.nanmax(np.abs(ref32 - ref) / scale))
+    g = np.ones(shape, np.complex128)
+    r = ctx.solve(g)
+    ost = of.settings(max_iterations=cfg.max_iterations, accuracy=cfg.tolerance,
+                      step_size=cfg.step_size)
+    out = {"config": workload_name(cfg, args.config, npol), "pass_max_rel_err_vs_fp64": pass_err,
+           "pass_max_rel_err_oracle32_vs_fp64": pass_err32,
+           "pass_max_err_per_median_gain": pass_err_scaled,
+           "pass_max_err_per_median_gain_oracle32": pass_err32_scaled,
+           "gpu_iterations": int(r.iterations)}
+    for prec in (64, 32):
+        o = np.ones(shape, np.complex128)
+        ro, _ = of.solve(prob, o, ost, precision=prec)
+        out[f"oracle{prec}_iterations"] = int(ro.iterations)
+        out[f"solve_max_rel_diff_vs_oracle{prec}"] = _max_rel_diff(g, o)
+    print(json.dumps(out), flush=True)
+    ctx.close()
+    return 0
+
+
 def run_reference_arm(args):
     world, rank, local = _dist_setup()
     if rank != 0:
@@ -680,6 +740,8 @@ def main():
     ap.add_argument("--warm-tight", type=int, default=20,
                     help="evaluated intervals also solved to tolerance 1e-8 for accuracy")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--fp64-check", action="store_true",
+                    help="solution error against the FP64 oracle (no timing)")
     ap.add_argument("--batch", type=int, default=1,
                     help="independent intervals of --config solved in one context")
     ap.add_argument("--mlp-only", action="store_true",
@@ -695,6 +757,8 @@ def main():
         return run_reference_arm(args)
     if args.mlp_only:
         return run_mlp_only(args)
+    if args.fp64_check:
+        return run_fp64_check(args)
     if args.batch > 1:
         return run_batch(args)
     return run_gpu_arm(args)
