@@ -1297,8 +1297,14 @@ __global__ void __launch_bounds__(kPipeRuns) power_kernel(const SlabDesc* __rest
   for (int c = 0; c < NCORR; ++c) out[c * kPipeRuns + r] = float(q[c]);
 }
 
-template <int NCORR, int NPOL, int DMAX>
+// NG lanes per run (1, 2 or 4): a tile has kPipeRuns / NG runs and lane g of a
+// run owns directions g, g + NG, ... (DMAX of them); the residual is the sum
+// over the run's lanes (warp shuffles). NG = 1: one run per lane, exactly DMAX
+// directions.
+template <int NCORR, int NPOL, int DMAX, int NG>
 __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams p) {
+  static_assert(kPipeRuns % NG == 0 && 32 % NG == 0, "lanes per run must divide a warp");
+  constexpr int RUNS = kPipeRuns / NG;  // runs per tile
   // An unrolled graph body launches the kernel more than once per loop test:
   // a launch after the loop has stopped does nothing.
   if (!p.host_mode && p.use_handle && static_cast<volatile const LoopState*>(p.state)->done)
@@ -1323,11 +1329,12 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
   char* stages = reinterpret_cast<char*>(smem + p.off_stages);
   constexpr uint32_t E = NCORR * 8;  // bytes per visibility
   const uint32_t acc_n = p.acc_floats;
-  // Each instantiation serves exactly DMAX directions (no padded ones).
-  constexpr uint32_t n_dir = DMAX;
+  // NG = 1: each instantiation serves exactly DMAX directions (no padded
+  // ones); NG > 1: up to NG * DMAX.
+  const uint32_t n_dir = NG == 1 ? uint32_t(DMAX) : p.n_dir;
   // stage: [run antennas of the fragment, first row only][data][model 0..]
-  constexpr uint32_t kRunsBytes = kPipeRuns * 4;
-  const uint32_t stage_bytes = kRunsBytes + (1 + n_dir) * kPipeRuns * E;
+  constexpr uint32_t kRunsBytes = RUNS * 4;
+  const uint32_t stage_bytes = kRunsBytes + (1 + n_dir) * RUNS * E;
   const uint32_t table_bytes = p.table_f2 * 8;
   const uint32_t S = p.stages;
 
@@ -1397,7 +1404,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
         BulkCopyG2S(dst, dsrc, seg, &full[st]);
         const char* m = msrc;
         for (uint32_t d = 0; d < n_dir; ++d, m += dir_step)
-          BulkCopyG2S(dst + size_t(1 + d) * kPipeRuns * E, m, seg, &full[st]);
+          BulkCopyG2S(dst + size_t(1 + d) * RUNS * E, m, seg, &full[st]);
         dsrc += row_step;
         msrc += row_step;
         if (++st == S) {
@@ -1405,7 +1412,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
           ph ^= 1u;
         }
       }
-      if (ok && (f.flags & kFragPower)) {
+      if (NG == 1 && ok && (f.flags & kFragPower)) {
         // one more stage: the tile's model powers [dir][corr][run]
         if (row >= S && !PipeWait(&empty[st], ph ^ 1u, s_err, &p.counters[1])) {
           ok = false;
@@ -1436,7 +1443,9 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
 
   // ---------------- consumer warps ----------------
   const int ctid = tid;  // 0 .. kPipeRuns - 1
-  const bool powers_pre = p.powers != nullptr;
+  const int run = ctid / NG;  // the lane's run within the tile
+  const int g = ctid % NG;    // the lane's first direction
+  const bool powers_pre = NG == 1 && p.powers != nullptr;
   uint32_t nvis = 0, cur_visit = 0xFFFFFFFFu;
   uint32_t st = 0, ph = 0;  // stage of the next row and the parity of its use
   const float2* gtab = gtab_buf;
@@ -1468,8 +1477,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
       ++nvis;
       ConsumerBarrier();
     }
-    const bool active = uint32_t(ctid) < f.n_runs;
-    const bool warp_busy = uint32_t(warp) * 32u < f.n_runs;
+    const bool active = uint32_t(run) < f.n_runs;
+    const bool warp_busy = uint32_t(warp) * (32u / NG) < f.n_runs;
     uint32_t a1 = 0, a2 = 0;
     float2 G[DMAX][NCORR];
     float2 P[DMAX][NCORR];
@@ -1493,7 +1502,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
         if (rr == f.row_lo) {
           // first row of the fragment: run antennas and the run's gain products
           const uint32_t ap =
-              active ? reinterpret_cast<const uint32_t*>(stages + size_t(s) * stage_bytes)[ctid] : 0u;
+              active ? reinterpret_cast<const uint32_t*>(stages + size_t(s) * stage_bytes)[run] : 0u;
           a1 = ap & 0xFFFFu;
           a2 = ap >> 16;
 #pragma unroll
@@ -1503,9 +1512,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
             for (int q = 0; q < NPOL; ++q) {
               ga[q] = make_float2(0.f, 0.f);
               gb[q] = make_float2(0.f, 0.f);
-              if (k < int(n_dir)) {
-                ga[q] = gtab[a1 * p.gain_stride + k * NPOL + q];
-                gb[q] = gtab[a2 * p.gain_stride + k * NPOL + q];
+              const uint32_t d = g + k * NG;
+              if (d < n_dir) {
+                ga[q] = gtab[a1 * p.gain_stride + d * NPOL + q];
+                gb[q] = gtab[a2 * p.gain_stride + d * NPOL + q];
               }
             }
 #pragma unroll
@@ -1524,16 +1534,23 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
           constexpr bool kKeepM = kQ ? DMAX * NCORR <= 12 : DMAX * NCORR <= 20;
           // The residual is summed in two halves (even and odd directions) to
           // halve its chain of dependent multiply-adds.
+          // With NG > 1 each lane sums its own directions' terms and the
+          // run's lanes then add theirs up (shuffles) before D is added.
           float2 Rv[NCORR], Ro[NCORR];
-          LoadVisShared<NCORR>(base, ctid, Rv);
+          if constexpr (NG == 1) {
+            LoadVisShared<NCORR>(base, run, Rv);
+          } else {
+#pragma unroll
+            for (int c = 0; c < NCORR; ++c) Rv[c] = make_float2(0.f, 0.f);
+          }
 #pragma unroll
           for (int c = 0; c < NCORR; ++c) Ro[c] = make_float2(0.f, 0.f);
           float2 Mk[kKeepM ? DMAX : 1][NCORR];
 #pragma unroll
           for (int k = 0; k < DMAX; ++k) {
             float2 M[NCORR];
-            if (k < int(n_dir)) {
-              LoadVisShared<NCORR>(base + size_t(1 + k) * kPipeRuns * E, ctid, M);
+            if (g + k * NG < int(n_dir)) {
+              LoadVisShared<NCORR>(base + size_t(1 + g + k * NG) * RUNS * E, run, M);
             } else {
 #pragma unroll
               for (int c = 0; c < NCORR; ++c) M[c] = make_float2(0.f, 0.f);
@@ -1556,14 +1573,30 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
             Rv[c].x += Ro[c].x;
             Rv[c].y += Ro[c].y;
           }
+          if constexpr (NG > 1) {
+#pragma unroll
+            for (int m = 1; m < NG; m <<= 1)
+#pragma unroll
+              for (int c = 0; c < NCORR; ++c) {
+                Rv[c].x += __shfl_xor_sync(0xFFFFFFFFu, Rv[c].x, m);
+                Rv[c].y += __shfl_xor_sync(0xFFFFFFFFu, Rv[c].y, m);
+              }
+            float2 D[NCORR];
+            LoadVisShared<NCORR>(base, run, D);
+#pragma unroll
+            for (int c = 0; c < NCORR; ++c) {
+              Rv[c].x += D[c].x;
+              Rv[c].y += D[c].y;
+            }
+          }
 #pragma unroll
           for (int k = 0; k < DMAX; ++k) {
             float2 M[NCORR];
             if constexpr (kKeepM) {
 #pragma unroll
               for (int c = 0; c < NCORR; ++c) M[c] = Mk[k][c];
-            } else if (k < int(n_dir)) {
-              LoadVisShared<NCORR>(base + size_t(1 + k) * kPipeRuns * E, ctid, M);
+            } else if (g + k * NG < int(n_dir)) {
+              LoadVisShared<NCORR>(base + size_t(1 + g + k * NG) * RUNS * E, run, M);
             } else {
 #pragma unroll
               for (int c = 0; c < NCORR; ++c) M[c] = make_float2(0.f, 0.f);
@@ -1589,7 +1622,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
       __syncwarp();
       if (lane == 0) MbarArrive(&empty[s]);
     }
-    if (f.flags & kFragPower) {
+    if (NG == 1 && (f.flags & kFragPower)) {
       // the tile's precomputed model powers, in the stage after its rows
       const uint32_t s = st;
       PipeWait(&full[s], ph, s_err, &p.counters[1]);
@@ -1618,9 +1651,9 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
       const uint32_t n_groups_t = (f.flags >> 8) & 0xFu;
       uint32_t my_group = 0;
 #pragma unroll
-      for (int g = 0; g < int(kMaxGroups) - 1; ++g)
-        my_group += uint32_t(ctid) >= ((f.group_end[g >> 2] >> ((g & 3) * 8)) & 0xFFu) &&
-                    uint32_t(g + 1) < n_groups_t;
+      for (int gi = 0; gi < int(kMaxGroups) - 1; ++gi)
+        my_group += uint32_t(run) >= ((f.group_end[gi >> 2] >> ((gi & 3) * 8)) & 0xFFu) &&
+                    uint32_t(gi + 1) < n_groups_t;
       for (uint32_t phase = 0; phase < 2 * n_groups_t; ++phase) {
         const int side = int(phase & 1u);
         if (phase > 0) ConsumerBarrier();
@@ -1629,11 +1662,12 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
           const uint32_t b = side == 0 ? a2 : a1;
 #pragma unroll
           for (int k = 0; k < DMAX; ++k) {
-            if (k < int(n_dir)) {
+            const uint32_t d = g + k * NG;
+            if (d < n_dir) {
               float2 gb[NPOL];
 #pragma unroll
-              for (int q = 0; q < NPOL; ++q) gb[q] = gtab[b * p.gain_stride + k * NPOL + q];
-              float* x = acc + a * p.acc_stride + k * NPOL * 3;
+              for (int q = 0; q < NPOL; ++q) gb[q] = gtab[b * p.gain_stride + d * NPOL + q];
+              float* x = acc + a * p.acc_stride + d * NPOL * 3;
 #pragma unroll
               for (int q = 0; q < NPOL; ++q) {
                 float2 n = make_float2(0.f, 0.f);
@@ -1665,6 +1699,11 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
       }
       continue;
     }
+    if constexpr (NG > 1) {
+      // the plan gives lane-group kernels direct tiles only
+      if (ctid == 0) atomicExch(&p.counters[1], 1u);
+      continue;
+    } else {
     // Sorted reduction: stage the run's P/Q, counting-sort the (run, side)
     // pairs by antenna, then (antenna, direction group) owner threads add
     // them up; each accumulator entry has exactly one writer.
@@ -1790,6 +1829,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
         }
       }
     }
+    }  // NG == 1
   }
   if (cur_visit != 0xFFFFFFFFu) end_visit();
   // Grid barrier: every CTA has flushed every partial slot (the launch is
@@ -1932,6 +1972,7 @@ struct ddsolve_ctx {
   const void* pipe_fn = nullptr;
   size_t pipe_smem = 0;
   uint32_t pipe_stages = 0, acc_stride = 0, gain_stride = 0;
+  uint32_t pipe_ng = 1;  // lanes per run of the chosen pipe_kernel
   DevBuf d_cb_done /* new non-finite flags */, d_cb_flag, d_cb_avg, d_counters;
   DevBuf d_frags, d_cta_frag_off, d_tables, d_tab_cb, d_tab_sol, d_tab_off, d_tab_ent;
   uint32_t n_tables = 0, table_f2 = 0, owner_groups = 1, n_gbuf = 2;
@@ -2007,6 +2048,7 @@ namespace {
 struct KernelEntry {
   int ncorr, npol, dmax;
   const void* fn;
+  int ng = 1;  // pipe_kernel: lanes per run
 };
 
 template <int NC, int NP, int DM>
@@ -2041,7 +2083,14 @@ const KernelEntry* FindKernel(int ncorr, int npol, int need) {
 template <int NC, int NP, int DM>
 constexpr KernelEntry PipeEntry() {
   return KernelEntry{NC, NP, DM,
-                     reinterpret_cast<const void*>(&pipe_kernel<NC, NP, DM>)};
+                     reinterpret_cast<const void*>(&pipe_kernel<NC, NP, DM, 1>), 1};
+}
+
+// Lane-group variant: up to 4 * DM directions.
+template <int NC, int NP, int DM>
+constexpr KernelEntry PipeEntry4() {
+  return KernelEntry{NC, NP, DM,
+                     reinterpret_cast<const void*>(&pipe_kernel<NC, NP, DM, 4>), 4};
 }
 
 const std::vector<KernelEntry>& PipeKernels() {
@@ -2060,6 +2109,11 @@ const std::vector<KernelEntry>& PipeKernels() {
       PipeEntry<4, 2, 4>(),
       PipeEntry<4, 1, 1>(), PipeEntry<4, 1, 2>(), PipeEntry<4, 1, 3>(),
       PipeEntry<4, 1, 4>(),
+      // 13..48 directions (XX/YY): four lanes per run
+      PipeEntry4<2, 2, 4>(), PipeEntry4<2, 2, 6>(), PipeEntry4<2, 2, 8>(),
+      PipeEntry4<2, 2, 10>(), PipeEntry4<2, 2, 12>(),
+      PipeEntry4<2, 1, 4>(), PipeEntry4<2, 1, 6>(), PipeEntry4<2, 1, 8>(),
+      PipeEntry4<2, 1, 10>(), PipeEntry4<2, 1, 12>(),
   };
   return k;
 }
@@ -2067,7 +2121,14 @@ const std::vector<KernelEntry>& PipeKernels() {
 const KernelEntry* FindPipeKernel(int ncorr, int npol, int n_dir) {
   const KernelEntry* best = nullptr;
   for (const KernelEntry& e : PipeKernels())
-    if (e.ncorr == ncorr && e.npol == npol && e.dmax == n_dir) best = &e;
+    if (e.ng == 1 && e.ncorr == ncorr && e.npol == npol && e.dmax == n_dir) best = &e;
+  if (best || std::getenv("DDSOLVE_NO_LANE_GROUPS")) return best;
+  // more directions than one lane holds: four lanes per run, the smallest
+  // instantiation with 4 * dmax >= n_dir
+  for (const KernelEntry& e : PipeKernels())
+    if (e.ng == 4 && e.ncorr == ncorr && e.npol == npol && 4 * e.dmax >= n_dir &&
+        (!best || e.dmax < best->dmax))
+      best = &e;
   return best;
 }
 
@@ -2076,7 +2137,8 @@ uint32_t OddAtLeast(uint32_t x) { return x | 1u; }
 // One pipeline stage of pipe_kernel: the fragment's run antennas (first row
 // only), then one row of data and of every direction's model.
 size_t PipeStageBytes(const ddsolve_ctx* ctx) {
-  return size_t(kPipeRuns) * 4 + size_t(1 + ctx->n_dir) * kPipeRuns * ctx->elem_bytes;
+  const size_t runs = kPipeRuns / ctx->pipe_ng;
+  return runs * 4 + size_t(1 + ctx->n_dir) * runs * ctx->elem_bytes;
 }
 
 // Shared memory of pipe_kernel for `stages` stages, with one gain-table
@@ -2090,8 +2152,10 @@ size_t PipeSmemBytes(const ddsolve_ctx* ctx, uint32_t stages, uint32_t acc_strid
   size_t off = align(256 + size_t(kPipeRuns) * 12, 16);
   off += align(size_t(ctx->n_ant) * acc_stride * 4, 16);
   off += table_f2 * 8;
-  off += size_t(3) * ctx->n_corr * ctx->n_dir * kPipeRuns * 4 + 2 * n_ant4 * 4 +
-         size_t(kPipeRuns) * 4 + size_t(kPipeRuns) * 4 + 128;
+  if (ctx->pipe_ng == 1)  // the sorted tile reduction (one run per lane only)
+    off += size_t(3) * ctx->n_corr * ctx->n_dir * kPipeRuns * 4 + 2 * n_ant4 * 4 +
+           size_t(kPipeRuns) * 4 + size_t(kPipeRuns) * 4;
+  off += 128;
   off = align(off, 128);
   return off + size_t(stages) * PipeStageBytes(ctx);
 }
@@ -2192,6 +2256,8 @@ int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const float* data,
   return DDSOLVE_OK;
 }
 
+constexpr int kPlanNoPipe = -1;  // BuildPipePlan: use the stream_kernel path
+
 // Plan of the pipelined path: tiles of up to kPipeRuns runs (flagged direct
 // when their first antennas are distinct and their second antennas are
 // distinct), split along their (time, channel) rows into fragments so that
@@ -2245,9 +2311,10 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
     // Equal tiles (a multiple of 4 runs, so that each tile's run antennas
     // start on a 16-byte boundary): a short remainder tile would stream its
     // rows at a fraction of the bytes per pipeline stage.
-    const uint32_t n_tiles_slab = (sd.R + kPipeRuns - 1) / kPipeRuns;
+    const uint32_t max_runs = kPipeRuns / ctx->pipe_ng;
+    const uint32_t n_tiles_slab = (sd.R + max_runs - 1) / max_runs;
     const uint32_t tile_runs =
-        n_tiles_slab ? ((sd.R + n_tiles_slab - 1) / n_tiles_slab + 3u) & ~3u : kPipeRuns;
+        n_tiles_slab ? ((sd.R + n_tiles_slab - 1) / n_tiles_slab + 3u) & ~3u : max_runs;
     for (uint32_t r0 = 0; r0 < sd.R; r0 += tile_runs) {
       const uint32_t n = std::min<uint32_t>(tile_runs, sd.R - r0);
       // Greedy split into consecutive groups whose first antennas are
@@ -2291,8 +2358,9 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
     run_rows += uint64_t(t.n) * t.rows;
     n_runs_all += t.n;
   }
+  if (ctx->pipe_ng > 1 && any_sorted) return kPlanNoPipe;
   const bool use_powers =
-      !std::getenv("DDSOLVE_NO_POWERS") && n_runs_all > 0 &&
+      ctx->pipe_ng == 1 && !std::getenv("DDSOLVE_NO_POWERS") && n_runs_all > 0 &&
       (ctx->tune_powers == 1 || (ctx->tune_powers < 0 && run_rows >= 16 * n_runs_all));
   // ---- fragments: rows balanced over the CTAs ----
   uint64_t total_rows = 0;
@@ -2472,7 +2540,7 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
 
 // Builds the streaming plan: kernel choice, CTA work split, partial slots and
 // the finalisation lists.
-int BuildPlan(ddsolve_ctx* ctx) {
+int BuildPlanImpl(ddsolve_ctx* ctx, bool allow_pipe) {
   for (uint32_t c = 0; c < ctx->n_cb; ++c)
     if (!ctx->cbs[c].set)
       return ctx->Fail(DDSOLVE_E_STATE,
@@ -2484,10 +2552,12 @@ int BuildPlan(ddsolve_ctx* ctx) {
   // Pipelined kernel when the direction count, the correlation layout and the
   // shared memory allow it (and no lane groups were requested).
   ctx->use_pipe = false;
-  if (ctx->tune_ng == 0 && ctx->tune_pipe != 0 && ctx->n_groups == 1 &&
+  ctx->pipe_ng = 1;
+  if (allow_pipe && ctx->tune_ng == 0 && ctx->tune_pipe != 0 && ctx->n_groups == 1 &&
       (ctx->n_corr == 2 || ctx->n_corr == 4) && !std::getenv("DDSOLVE_NO_PIPE")) {
     const KernelEntry* pe =
         FindPipeKernel(int(ctx->n_corr), int(ctx->n_pol), int(ctx->n_dir));
+    if (pe) ctx->pipe_ng = uint32_t(pe->ng);
     const uint32_t acc_stride = OddAtLeast(ctx->n_dir * ctx->n_pol * 3);
     const uint32_t gain_stride = OddAtLeast(ctx->n_dir * ctx->n_pol);
     uint32_t stages = 0;
@@ -2599,6 +2669,7 @@ int BuildPlan(ddsolve_ctx* ctx) {
     }
   }
   if (ctx->use_pipe) return BuildPipePlan(ctx, descs, slab_sol, max_optin);
+  ctx->pipe_ng = 1;
   const uint32_t max_ctas = uint32_t(ctx->n_sm) * uint32_t(occ);
   uint32_t n_ctas = std::max<uint32_t>(1, std::min<uint32_t>(max_ctas, uint32_t(steps.size())));
   double total_w = 0;
@@ -2718,6 +2789,15 @@ int BuildPlan(ddsolve_ctx* ctx) {
   ctx->plan_dirty = false;
   ctx->DestroyGraph();
   return DDSOLVE_OK;
+}
+
+// The pipelined plan when it applies (a lane-group pipe_kernel needs every
+// tile to take the direct reduction), else the stream_kernel plan.
+int BuildPlan(ddsolve_ctx* ctx) {
+  const int rc = BuildPlanImpl(ctx, true);
+  if (rc != kPlanNoPipe) return rc;
+  ctx->use_pipe = false;
+  return BuildPlanImpl(ctx, false);
 }
 
 StreamParams MakeStreamParams(ddsolve_ctx* ctx) {

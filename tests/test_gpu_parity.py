@@ -454,3 +454,32 @@ def test_batched_intervals_match_separate_solves(built):
         assert H.max_rel_diff(sol[g * n_cb:(g + 1) * n_cb], s1) < RTOL_SOLVE
         n = min(r.iterations, 150)
         np.testing.assert_allclose(mags[g, :n], m1[:n], rtol=1e-3, atol=1e-12)
+
+
+@pytest.mark.parametrize("n_dir,npol", [(13, 2), (16, 1), (40, 2)])
+def test_lane_group_pipe_kernel(built, n_dir, npol):
+    """More directions than one lane holds: pipe_kernel with four lanes per
+    run (the residual summed across the run's lanes), against the FP64
+    oracle for one pass and the FP32 oracle for a 20-iteration solve, and
+    against the stream_kernel path."""
+    obs = H.small_observation(n_stations=30, n_directions=n_dir, n_channels=8, n_cb=2,
+                              n_times=2, seed=31 + n_dir, n_sources=2)
+    prob = H.problem_from_observation(obs, 2, npol)
+    sol0 = _perturbed_start(obs, prob, scale=0.1)
+    solver = H.make_solver(prob, max_iterations=20)
+    got = solver.PerformIteration(obs.solve_data(), sol0)
+    assert solver._ctx.tuning()["use_pipe"] == -1
+    ref = of.perform_iteration(prob, sol0, precision=64)
+    err = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-12)
+    assert np.nanmax(err) < RTOL_PASS, np.nanmax(err)
+    v1 = H.make_solver(prob, max_iterations=20)
+    v1.SetTuning(direction_groups=4)
+    got_v1 = v1.PerformIteration(obs.solve_data(), sol0)
+    np.testing.assert_allclose(got, got_v1, rtol=1e-4)
+    st = of.settings(max_iterations=20, accuracy=1e-5, step_size=0.2)
+    ref32 = sol0.copy()
+    r, _ = of.solve(prob, ref32, st, precision=32)
+    g = sol0.copy()
+    res = solver.Solve(obs.solve_data(), g, 0.0)
+    assert res.iterations == r.iterations
+    assert H.max_rel_diff(g, ref32) < RTOL_SOLVE
