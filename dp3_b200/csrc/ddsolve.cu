@@ -949,7 +949,7 @@ __device__ __forceinline__ void WriteTables(const PipeParams& p, uint32_t cb,
 // MakeSolutionsFinite{1,2}Pol (SolverBase.cc:316-371) for channel blocks that
 // got non-finite solutions.
 template <int NPOL>
-__device__ __noinline__ void FinalizeDistributed(const PipeParams& p, int ctid,
+__device__ __forceinline__ void FinalizeDistributed(const PipeParams& p, int ctid,
                                                  double* s_sum, uint32_t* s_cnt,
                                                  uint32_t* s_last) {
   const DevSettings st = *p.settings;
@@ -1304,6 +1304,7 @@ __global__ void __launch_bounds__(kPipeRuns) power_kernel(const SlabDesc* __rest
 template <int NCORR, int NPOL, int DMAX, int NG>
 __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams p) {
   static_assert(kPipeRuns % NG == 0 && 32 % NG == 0, "lanes per run must divide a warp");
+  static_assert(NG == 1 || NCORR == 2, "lane groups are laid out for two correlations");
   constexpr int RUNS = kPipeRuns / NG;  // runs per tile
   // An unrolled graph body launches the kernel more than once per loop test:
   // a launch after the loop has stopped does nothing.
@@ -1334,7 +1335,13 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
   const uint32_t n_dir = NG == 1 ? uint32_t(DMAX) : p.n_dir;
   // stage: [run antennas of the fragment, first row only][data][model 0..]
   constexpr uint32_t kRunsBytes = RUNS * 4;
-  const uint32_t stage_bytes = kRunsBytes + (1 + n_dir) * RUNS * E;
+  // Row pitch inside a stage. A 16-byte shared load is served per quarter
+  // warp (8 lanes); with NG lanes per run those are 8 / NG runs reading NG
+  // different direction rows. A pitch of whole 128-byte bank lines plus
+  // 128 / NG bytes puts the 8 loads in distinct banks (without the pad,
+  // NG = 4 is a 4-way bank conflict). Two correlations (E = 16) only.
+  constexpr uint32_t RP = RUNS * E + (NG > 1 ? 128u / NG : 0u);
+  const uint32_t stage_bytes = kRunsBytes + (1 + n_dir) * RP;
   const uint32_t table_bytes = p.table_f2 * 8;
   const uint32_t S = p.stages;
 
@@ -1404,7 +1411,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
         BulkCopyG2S(dst, dsrc, seg, &full[st]);
         const char* m = msrc;
         for (uint32_t d = 0; d < n_dir; ++d, m += dir_step)
-          BulkCopyG2S(dst + size_t(1 + d) * RUNS * E, m, seg, &full[st]);
+          BulkCopyG2S(dst + size_t(1 + d) * RP, m, seg, &full[st]);
         dsrc += row_step;
         msrc += row_step;
         if (++st == S) {
@@ -1550,7 +1557,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
           for (int k = 0; k < DMAX; ++k) {
             float2 M[NCORR];
             if (g + k * NG < int(n_dir)) {
-              LoadVisShared<NCORR>(base + size_t(1 + g + k * NG) * RUNS * E, run, M);
+              LoadVisShared<NCORR>(base + size_t(1 + g + k * NG) * RP, run, M);
             } else {
 #pragma unroll
               for (int c = 0; c < NCORR; ++c) M[c] = make_float2(0.f, 0.f);
@@ -1596,7 +1603,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
 #pragma unroll
               for (int c = 0; c < NCORR; ++c) M[c] = Mk[k][c];
             } else if (g + k * NG < int(n_dir)) {
-              LoadVisShared<NCORR>(base + size_t(1 + g + k * NG) * RUNS * E, run, M);
+              LoadVisShared<NCORR>(base + size_t(1 + g + k * NG) * RP, run, M);
             } else {
 #pragma unroll
               for (int c = 0; c < NCORR; ++c) M[c] = make_float2(0.f, 0.f);
@@ -2138,7 +2145,8 @@ uint32_t OddAtLeast(uint32_t x) { return x | 1u; }
 // only), then one row of data and of every direction's model.
 size_t PipeStageBytes(const ddsolve_ctx* ctx) {
   const size_t runs = kPipeRuns / ctx->pipe_ng;
-  return runs * 4 + size_t(1 + ctx->n_dir) * runs * ctx->elem_bytes;
+  const size_t pitch = runs * ctx->elem_bytes + (ctx->pipe_ng > 1 ? 128 / ctx->pipe_ng : 0);
+  return runs * 4 + size_t(1 + ctx->n_dir) * pitch;
 }
 
 // Shared memory of pipe_kernel for `stages` stages, with one gain-table
