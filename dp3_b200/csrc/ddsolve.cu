@@ -64,14 +64,30 @@ constexpr uint32_t kMaxAntennas = 65535;
 // ---------------------------------------------------------------------------
 // Device-side plan structures
 // ---------------------------------------------------------------------------
+// A slab's visibilities, packed tile by tile: for every (time, channel) row,
+// its runs are cut into tiles of W runs (the last one shorter), and a tile
+// holds the data and then every direction's model for its runs,
+//   [T][L][tile][1 + n_dir][runs of the tile],
+// so that one row of one tile, with all its directions, is one contiguous
+// block (one bulk copy of the pipelined kernel).
 struct SlabDesc {
-  const void* data;         // [T][L][R] elements
-  const void* model;        // [n_dir][T][L][R] elements
+  const void* vis;          // data and model, packed as above
   const uint32_t* run_ant;  // [R] antenna1 | antenna2 << 16
   uint32_t cb, T, L, R;
+  uint32_t W;        // runs per tile (a multiple of 4)
   uint32_t sol_off;  // first of n_dir entries in slab_sol
   uint32_t table;    // gain table of the slab (pipe_kernel)
 };
+
+// Element index in a packed slab of run r, row (t * L + l), and j = 0 for the
+// data or 1 + d for direction d's model; nd1 = 1 + n_dir.
+__host__ __device__ __forceinline__ uint64_t SlabElem(uint32_t R, uint32_t W, uint32_t nd1,
+                                                      uint64_t row, uint32_t j, uint32_t r) {
+  const uint32_t k = r / W;
+  const uint32_t base = k * W;
+  const uint32_t w = R - base < W ? R - base : W;
+  return row * R * nd1 + uint64_t(base) * nd1 + uint64_t(j) * w + (r - base);
+}
 
 // pipe_kernel work item: rows [row_lo, row_hi) of the (t, channel) rows of
 // the tile of runs [r0, r0 + n_runs) of a slab; fragments of one CTA that
@@ -215,10 +231,10 @@ __device__ __forceinline__ void LoadVis(const void* base, size_t idx,
 constexpr uint32_t kRunFlipped = 0x80000000u;
 
 struct PackSlab {
-  uint64_t dst_elem_off;  // into the cb's packed data buffer
+  uint64_t dst_elem_off;  // into the cb's packed buffer, in units of 1 + n_dir elements
   uint64_t src_base;
   uint64_t tstride;
-  uint32_t T, L, R, run_off;
+  uint32_t T, L, R, run_off, W;
 };
 
 template <int NCORR>
@@ -246,8 +262,7 @@ __global__ void pack_kernel(const PackSlab* __restrict__ slabs, uint32_t slab,
                             const uint32_t* __restrict__ run_len,
                             const float2* __restrict__ src_data,
                             const float2* __restrict__ src_model, uint64_t n_vis,
-                            uint32_t n_dir, float2* __restrict__ dst_data,
-                            float2* __restrict__ dst_model) {
+                            uint32_t n_dir, float2* __restrict__ dst_vis) {
   const PackSlab s = slabs[slab];
   const uint64_t tlr = uint64_t(s.T) * s.L * s.R;
   for (uint64_t e = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; e < tlr;
@@ -260,14 +275,12 @@ __global__ void pack_kernel(const PackSlab* __restrict__ slabs, uint32_t slab,
     const bool flip = (len & kRunFlipped) != 0;
     const bool valid = ch < (len & ~kRunFlipped);
     const uint64_t v = valid ? s.src_base + t * s.tstride + run_src[s.run_off + r] + ch : 0;
-    const uint64_t dst = s.dst_elem_off + e;
-    CopyVis<NCORR>(src_data + v * NCORR, dst_data + dst * NCORR, valid, flip);
-    // model block of the slab: [n_dir][T][L][R] starting at n_dir * dst_elem_off
-    for (uint32_t d = 0; d < n_dir; ++d) {
-      const uint64_t md = uint64_t(n_dir) * s.dst_elem_off + d * tlr + e;
-      CopyVis<NCORR>(src_model + (d * n_vis + v) * NCORR, dst_model + md * NCORR,
-                     valid, flip);
-    }
+    float2* dst = dst_vis + (uint64_t(1 + n_dir) * s.dst_elem_off) * NCORR;
+    CopyVis<NCORR>(src_data + v * NCORR,
+                   dst + SlabElem(s.R, s.W, 1 + n_dir, tl, 0, r) * NCORR, valid, flip);
+    for (uint32_t d = 0; d < n_dir; ++d)
+      CopyVis<NCORR>(src_model + (d * n_vis + v) * NCORR,
+                     dst + SlabElem(s.R, s.W, 1 + n_dir, tl, 1 + d, r) * NCORR, valid, flip);
   }
 }
 
@@ -378,11 +391,15 @@ __global__ void __launch_bounds__(kThreads)
       gtab[i] = make_float2(float(gv.x), float(gv.y));
     }
     __syncthreads();
-    const size_t tlr = size_t(sl.T) * sl.L * sl.R;
+    const uint32_t nd1 = 1 + n_dir;
+    const size_t row_elems = size_t(sl.R) * nd1;
 
     for (uint32_t run0 = vis.run_lo; run0 < vis.run_hi; run0 += runs_per_block) {
       const uint32_t run = run0 + slot;
       const bool active = run < vis.run_hi;
+      // the run's data in row 0, and the distance between its directions
+      const size_t e0 = active ? SlabElem(sl.R, sl.W, nd1, 0, 0, run) : 0;
+      const size_t jstep = active ? SlabElem(sl.R, sl.W, nd1, 0, 1, run) - e0 : 0;
       uint32_t a1 = 0, a2 = 0;
       if (active) {
         const uint32_t ap = sl.run_ant[run];
@@ -424,16 +441,16 @@ __global__ void __launch_bounds__(kThreads)
 
       for (uint32_t t = 0; t < sl.T; ++t) {
         for (uint32_t ch = 0; ch < sl.L; ++ch) {
-          const size_t e = (size_t(t) * sl.L + ch) * sl.R + run;
+          const size_t e = (size_t(t) * sl.L + ch) * row_elems + e0;
           float2 Rv[NCORR];
 #pragma unroll
           for (int c = 0; c < NCORR; ++c) Rv[c] = make_float2(0.f, 0.f);
-          if (active && g == 0) LoadVis<NCORR>(sl.data, e, Rv);
+          if (active && g == 0) LoadVis<NCORR>(sl.vis, e, Rv);
           float2 M[DMAX][NCORR];
 #pragma unroll
           for (int k = 0; k < DMAX; ++k) {
             if (active && k < nd) {
-              LoadVis<NCORR>(sl.model, size_t(g + k * ng) * tlr + e, M[k]);
+              LoadVis<NCORR>(sl.vis, e + size_t(1 + g + k * ng) * jstep, M[k]);
             } else {
 #pragma unroll
               for (int c = 0; c < NCORR; ++c) M[k][c] = make_float2(0.f, 0.f);
@@ -1282,9 +1299,10 @@ __global__ void __launch_bounds__(kPipeRuns) power_kernel(const SlabDesc* __rest
   for (int c = 0; c < NCORR; ++c) q[c] = 0.0;
   if (r < t.n) {
     const size_t rows = size_t(sl.T) * sl.L;
-    const float2* m = static_cast<const float2*>(sl.model) +
-                      ((size_t(k) * rows) * sl.R + t.r0 + r) * NCORR;
-    for (size_t row = 0; row < rows; ++row, m += size_t(sl.R) * NCORR) {
+    const uint32_t nd1 = 1 + n_dir;
+    const float2* m = static_cast<const float2*>(sl.vis) +
+                      SlabElem(sl.R, sl.W, nd1, 0, 1 + k, t.r0 + r) * NCORR;
+    for (size_t row = 0; row < rows; ++row, m += size_t(sl.R) * nd1 * NCORR) {
 #pragma unroll
       for (int c = 0; c < NCORR; ++c) {
         const float2 v = __ldcs(m + c);
@@ -1335,13 +1353,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
   const uint32_t n_dir = NG == 1 ? uint32_t(DMAX) : p.n_dir;
   // stage: [run antennas of the fragment, first row only][data][model 0..]
   constexpr uint32_t kRunsBytes = RUNS * 4;
-  // Row pitch inside a stage. A 16-byte shared load is served per quarter
-  // warp (8 lanes); with NG lanes per run those are 8 / NG runs reading NG
-  // different direction rows. A pitch of whole 128-byte bank lines plus
-  // 128 / NG bytes puts the 8 loads in distinct banks (without the pad,
-  // NG = 4 is a 4-way bank conflict). Two correlations (E = 16) only.
-  constexpr uint32_t RP = RUNS * E + (NG > 1 ? 128u / NG : 0u);
-  const uint32_t stage_bytes = kRunsBytes + (1 + n_dir) * RP;
+  const uint32_t stage_bytes = kRunsBytes + (1 + n_dir) * RUNS * E;
   const uint32_t table_bytes = p.table_f2 * 8;
   const uint32_t S = p.stages;
 
@@ -1388,14 +1400,12 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
         cur_visit = f.visit;
         ++nvis;
       }
-      const size_t tlr = size_t(sl.T) * sl.L * sl.R;
-      const uint32_t seg = f.n_runs * E;
-      const char* dsrc = static_cast<const char*>(sl.data) +
-                         (size_t(f.row_lo) * sl.R + f.r0) * E;
-      const char* msrc = static_cast<const char*>(sl.model) +
-                         (size_t(f.row_lo) * sl.R + f.r0) * E;
-      const size_t row_step = size_t(sl.R) * E;
-      const size_t dir_step = tlr * E;
+      // The fragment's tile is one tile of the packed slab: a row of it,
+      // data and all directions, is one contiguous block.
+      const uint32_t seg = (1 + n_dir) * f.n_runs * E;
+      const size_t row_step = size_t(sl.R) * (1 + n_dir) * E;
+      const char* src = static_cast<const char*>(sl.vis) + size_t(f.row_lo) * row_step +
+                        size_t(f.r0) * (1 + n_dir) * E;
       for (uint32_t rr = f.row_lo; rr < f.row_hi; ++rr, ++row) {
         if (row >= S && !PipeWait(&empty[st], ph ^ 1u, s_err, &p.counters[1])) {
           ok = false;
@@ -1404,16 +1414,11 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
         // The fragment's run antennas travel with its first row (the run
         // arrays are padded to whole 16-byte groups).
         const uint32_t runs_bytes = rr == f.row_lo ? ((f.n_runs + 3u) & ~3u) * 4u : 0u;
-        MbarArriveExpectTx(&full[st], seg * (1 + n_dir) + runs_bytes);
+        MbarArriveExpectTx(&full[st], seg + runs_bytes);
         char* dst = stages + size_t(st) * stage_bytes;
         if (runs_bytes) BulkCopyG2S(dst, sl.run_ant + f.r0, runs_bytes, &full[st]);
-        dst += kRunsBytes;
-        BulkCopyG2S(dst, dsrc, seg, &full[st]);
-        const char* m = msrc;
-        for (uint32_t d = 0; d < n_dir; ++d, m += dir_step)
-          BulkCopyG2S(dst + size_t(1 + d) * RP, m, seg, &full[st]);
-        dsrc += row_step;
-        msrc += row_step;
+        BulkCopyG2S(dst + kRunsBytes, src, seg, &full[st]);
+        src += row_step;
         if (++st == S) {
           st = 0;
           ph ^= 1u;
@@ -1450,8 +1455,12 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
 
   // ---------------- consumer warps ----------------
   const int ctid = tid;  // 0 .. kPipeRuns - 1
-  const int run = ctid / NG;  // the lane's run within the tile
-  const int g = ctid % NG;    // the lane's first direction
+  // A warp holds 32 / NG runs; lane g * (32 / NG) + i serves run i of the
+  // warp for directions g, g + NG, ...: the 8 lanes of a quarter warp read 8
+  // consecutive runs of one direction row (distinct shared-memory banks).
+  constexpr int kRunsPerWarp = 32 / NG;
+  const int run = warp * kRunsPerWarp + lane % kRunsPerWarp;  // run within the tile
+  const int g = lane / kRunsPerWarp;  // the lane's first direction
   const bool powers_pre = NG == 1 && p.powers != nullptr;
   uint32_t nvis = 0, cur_visit = 0xFFFFFFFFu;
   uint32_t st = 0, ph = 0;  // stage of the next row and the parity of its use
@@ -1485,6 +1494,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
       ConsumerBarrier();
     }
     const bool active = uint32_t(run) < f.n_runs;
+    const uint32_t pitch = f.n_runs * E;  // bytes per direction row in a stage
     const bool warp_busy = uint32_t(warp) * (32u / NG) < f.n_runs;
     uint32_t a1 = 0, a2 = 0;
     float2 G[DMAX][NCORR];
@@ -1557,7 +1567,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
           for (int k = 0; k < DMAX; ++k) {
             float2 M[NCORR];
             if (g + k * NG < int(n_dir)) {
-              LoadVisShared<NCORR>(base + size_t(1 + g + k * NG) * RP, run, M);
+              LoadVisShared<NCORR>(base + size_t(1 + g + k * NG) * pitch, run, M);
             } else {
 #pragma unroll
               for (int c = 0; c < NCORR; ++c) M[c] = make_float2(0.f, 0.f);
@@ -1582,7 +1592,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
           }
           if constexpr (NG > 1) {
 #pragma unroll
-            for (int m = 1; m < NG; m <<= 1)
+            for (int m = kRunsPerWarp; m < 32; m <<= 1)
 #pragma unroll
               for (int c = 0; c < NCORR; ++c) {
                 Rv[c].x += __shfl_xor_sync(0xFFFFFFFFu, Rv[c].x, m);
@@ -1603,7 +1613,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
 #pragma unroll
               for (int c = 0; c < NCORR; ++c) M[c] = Mk[k][c];
             } else if (g + k * NG < int(n_dir)) {
-              LoadVisShared<NCORR>(base + size_t(1 + g + k * NG) * RP, run, M);
+              LoadVisShared<NCORR>(base + size_t(1 + g + k * NG) * pitch, run, M);
             } else {
 #pragma unroll
               for (int c = 0; c < NCORR; ++c) M[c] = make_float2(0.f, 0.f);
@@ -1909,7 +1919,8 @@ struct DevBuf {
 
 struct HostSlab {
   uint32_t T, L, R;
-  uint64_t elem_off;  // within the channel block's packed buffer
+  uint32_t W = 0;     // runs per tile of the packed layout
+  uint64_t elem_off;  // within the channel block's packed buffer, in 1 + n_dir units
   uint64_t src_base, tstride;
   uint32_t run_off;
   std::vector<uint32_t> sol;  // [n_dir]
@@ -1918,7 +1929,7 @@ struct HostSlab {
 bool SameLayout(const std::vector<HostSlab>& a, const std::vector<HostSlab>& b) {
   if (a.size() != b.size()) return false;
   for (size_t i = 0; i < a.size(); ++i)
-    if (a[i].T != b[i].T || a[i].L != b[i].L || a[i].R != b[i].R ||
+    if (a[i].T != b[i].T || a[i].L != b[i].L || a[i].R != b[i].R || a[i].W != b[i].W ||
         a[i].elem_off != b[i].elem_off || a[i].run_off != b[i].run_off ||
         a[i].sol != b[i].sol)
       return false;
@@ -1931,7 +1942,7 @@ struct ChannelBlockStore {
   uint64_t n_elems = 0;
   std::vector<HostSlab> slabs;
   std::vector<uint32_t> run_ant, run_src, run_len;
-  DevBuf data, model, run_ant_dev;
+  DevBuf vis, run_ant_dev;  // packed slabs (data and model), run antennas
   // Layout of the previous upload; an upload with the same layout into the
   // same buffers keeps the streaming plan (and its CUDA graph) valid.
   std::vector<HostSlab> prev_slabs;
@@ -2145,8 +2156,7 @@ uint32_t OddAtLeast(uint32_t x) { return x | 1u; }
 // only), then one row of data and of every direction's model.
 size_t PipeStageBytes(const ddsolve_ctx* ctx) {
   const size_t runs = kPipeRuns / ctx->pipe_ng;
-  const size_t pitch = runs * ctx->elem_bytes + (ctx->pipe_ng > 1 ? 128 / ctx->pipe_ng : 0);
-  return runs * 4 + size_t(1 + ctx->n_dir) * pitch;
+  return runs * 4 + size_t(1 + ctx->n_dir) * runs * ctx->elem_bytes;
 }
 
 // Shared memory of pipe_kernel for `stages` stages, with one gain-table
@@ -2188,22 +2198,35 @@ int CheckDims(const ddsolve_dims* dims) {
   return DDSOLVE_OK;
 }
 
+// Runs per tile of the packed layout: the tile of the pipelined kernel that
+// the context's correlations and direction count select (equal tiles of at
+// most kPipeRuns / NG runs, a multiple of 4, so that a tile's run antennas
+// start on a 16-byte boundary; a short remainder tile would stream its rows
+// at a fraction of the bytes per pipeline stage).
+uint32_t LayoutTileRuns(const ddsolve_ctx* ctx, uint32_t R) {
+  const KernelEntry* e = FindPipeKernel(int(ctx->n_corr), int(ctx->n_pol), int(ctx->n_dir));
+  const uint32_t max_runs = kPipeRuns / (e ? uint32_t(e->ng) : 1u);
+  if (R == 0) return max_runs;
+  const uint32_t n_tiles = (R + max_runs - 1) / max_runs;
+  return ((R + n_tiles - 1) / n_tiles + 3u) & ~3u;
+}
+
 // Uploads the staged reference-layout block and packs it into slabs.
 int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const float* data,
                   const float* model) {
   const size_t E = ctx->elem_bytes;
   const size_t src_bytes = size_t(cb.n_vis) * E * (1 + ctx->n_dir);
   DDS_CHECK_CUDA(ctx, ctx->staging.Reserve(src_bytes));
-  cb.data.realloc_flag = cb.model.realloc_flag = cb.run_ant_dev.realloc_flag = false;
-  DDS_CHECK_CUDA(ctx, cb.data.Reserve(cb.n_elems * E));
-  DDS_CHECK_CUDA(ctx, cb.model.Reserve(cb.n_elems * E * ctx->n_dir));
+  cb.vis.realloc_flag = cb.run_ant_dev.realloc_flag = false;
+  DDS_CHECK_CUDA(ctx, cb.vis.Reserve(cb.n_elems * E * (1 + ctx->n_dir)));
   DDS_CHECK_CUDA(ctx, cb.run_ant_dev.Reserve(cb.run_ant.size() * 4));
   DDS_CHECK_CUDA(ctx, ctx->run_src_dev.Reserve(cb.run_src.size() * 4));
   DDS_CHECK_CUDA(ctx, ctx->run_len_dev.Reserve(cb.run_len.size() * 4));
   std::vector<PackSlab> ps(cb.slabs.size());
   for (size_t i = 0; i < cb.slabs.size(); ++i) {
-    const HostSlab& s = cb.slabs[i];
-    ps[i] = PackSlab{s.elem_off, s.src_base, s.tstride, s.T, s.L, s.R, s.run_off};
+    HostSlab& s = cb.slabs[i];
+    s.W = LayoutTileRuns(ctx, s.R);
+    ps[i] = PackSlab{s.elem_off, s.src_base, s.tstride, s.T, s.L, s.R, s.run_off, s.W};
   }
   DDS_CHECK_CUDA(ctx, ctx->pack_desc.Reserve(ps.size() * sizeof(PackSlab)));
   char* st = ctx->staging.as<char>();
@@ -2233,26 +2256,25 @@ int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const float* data,
         uint32_t(std::min<uint64_t>((tlr + 255) / 256, uint64_t(ctx->n_sm) * 8));
     const float2* src_d = reinterpret_cast<const float2*>(st);
     const float2* src_m = reinterpret_cast<const float2*>(st + size_t(cb.n_vis) * E);
-    float2* dst_d = cb.data.as<float2>();
-    float2* dst_m = cb.model.as<float2>();
+    float2* dst = cb.vis.as<float2>();
     if (E == 8)
       pack_kernel<1><<<blocks, 256, 0, ctx->stream>>>(
           ctx->pack_desc.as<PackSlab>(), uint32_t(i), ctx->run_src_dev.as<uint32_t>(),
-          ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir, dst_d, dst_m);
+          ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir, dst);
     else if (E == 16)
       pack_kernel<2><<<blocks, 256, 0, ctx->stream>>>(
           ctx->pack_desc.as<PackSlab>(), uint32_t(i), ctx->run_src_dev.as<uint32_t>(),
-          ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir, dst_d, dst_m);
+          ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir, dst);
     else
       pack_kernel<4><<<blocks, 256, 0, ctx->stream>>>(
           ctx->pack_desc.as<PackSlab>(), uint32_t(i), ctx->run_src_dev.as<uint32_t>(),
-          ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir, dst_d, dst_m);
+          ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir, dst);
     DDS_CHECK_CUDA(ctx, cudaGetLastError());
   }
   // The staging and run arrays are reused by the next upload: keep the
   // stream order (a later upload's copies follow these kernels).
   const bool moved =
-      cb.data.realloc_flag || cb.model.realloc_flag || cb.run_ant_dev.realloc_flag;
+      cb.vis.realloc_flag || cb.run_ant_dev.realloc_flag;
   if (!cb.set || moved || !SameLayout(cb.slabs, cb.prev_slabs) ||
       cb.run_ant != cb.prev_run_ant) {
     ctx->plan_dirty = true;
@@ -2316,13 +2338,11 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
     const SlabDesc& sd = descs[gi];
     const ChannelBlockStore& cbs = ctx->cbs[sd.cb];
     const uint32_t run_off = uint32_t(sd.run_ant - cbs.run_ant_dev.as<uint32_t>());
-    // Equal tiles (a multiple of 4 runs, so that each tile's run antennas
-    // start on a 16-byte boundary): a short remainder tile would stream its
-    // rows at a fraction of the bytes per pipeline stage.
+    // The tiles of the packed layout (LayoutTileRuns): a row of a tile is
+    // one bulk copy.
     const uint32_t max_runs = kPipeRuns / ctx->pipe_ng;
-    const uint32_t n_tiles_slab = (sd.R + max_runs - 1) / max_runs;
-    const uint32_t tile_runs =
-        n_tiles_slab ? ((sd.R + n_tiles_slab - 1) / n_tiles_slab + 3u) & ~3u : max_runs;
+    const uint32_t tile_runs = sd.W;
+    if (tile_runs == 0 || tile_runs > max_runs || (tile_runs & 3u)) return kPlanNoPipe;
     for (uint32_t r0 = 0; r0 < sd.R; r0 += tile_runs) {
       const uint32_t n = std::min<uint32_t>(tile_runs, sd.R - r0);
       // Greedy split into consecutive groups whose first antennas are
@@ -2658,8 +2678,8 @@ int BuildPlanImpl(ddsolve_ctx* ctx, bool allow_pipe) {
     for (uint32_t i = 0; i < cb.slabs.size(); ++i) {
       const HostSlab& s = cb.slabs[i];
       SlabDesc sd{};
-      sd.data = cb.data.as<char>() + s.elem_off * ctx->elem_bytes;
-      sd.model = cb.model.as<char>() + s.elem_off * ctx->n_dir * ctx->elem_bytes;
+      sd.vis = cb.vis.as<char>() + s.elem_off * (1 + ctx->n_dir) * ctx->elem_bytes;
+      sd.W = s.W;
       sd.run_ant = cb.run_ant_dev.as<uint32_t>() + s.run_off;
       sd.cb = c;
       sd.T = s.T;

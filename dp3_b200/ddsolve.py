@@ -159,6 +159,7 @@ class Context:
         if getattr(self, "_h", None):
             lib().ddsolve_destroy(self._h)
             self._h = None
+            self._tstream = None  # wrapped the destroyed stream
 
     def __del__(self):
         try:
@@ -177,6 +178,18 @@ class Context:
 
     def stream_ptr(self):
         return lib().ddsolve_stream(self._h)
+
+    def _after_current_stream(self, t):
+        """Orders this context's stream after torch's current stream on the
+        device of CUDA tensor `t` (which may have pending writes there), and
+        returns (this stream, the current stream) as torch streams."""
+        import torch
+        ts = getattr(self, "_tstream", None)
+        if ts is None:
+            ts = self._tstream = torch.cuda.ExternalStream(self.stream_ptr(), device=t.device)
+        cur = torch.cuda.current_stream(t.device)
+        ts.wait_stream(cur)
+        return ts, cur
 
     def set_settings(self, settings):
         self._check(lib().ddsolve_set_settings(self._h, ctypes.byref(settings)),
@@ -217,6 +230,8 @@ class Context:
         if _is_torch(solutions):
             import torch
             assert solutions.dtype == torch.complex128 and solutions.is_contiguous()
+            if solutions.is_cuda:  # the solve returns after its own stream
+                self._after_current_stream(solutions)
         else:
             assert solutions.dtype == np.complex128 and solutions.flags.c_contiguous
         res = Result()
@@ -253,20 +268,26 @@ class Context:
         """n_passes chained PerformIteration passes from `start`; returns
         [n_passes] + start.shape (pass k starts from pass k - 1's output).
         A CUDA torch tensor in gives a CUDA tensor out (no host copies, and
-        the call returns without waiting: the passes are ordered on this
-        context's stream); `out` may supply that tensor."""
+        the call returns without waiting: the passes run on this context's
+        stream, ordered after torch's current stream, and the current stream
+        is ordered after them); `out` may supply that tensor."""
+        streams = None
         if _is_torch(start):
             import torch
             start = start.contiguous()
             if out is None:
                 out = torch.empty((n_passes,) + tuple(start.shape), dtype=torch.complex128,
                                   device=start.device)
+            if start.is_cuda:
+                streams = self._after_current_stream(start)
         else:
             start = np.ascontiguousarray(start, dtype=np.complex128)
             out = np.empty((n_passes,) + start.shape, np.complex128)
         self._check(lib().ddsolve_perform_iterations(self._h, _addr(start), n_passes,
                                                      _addr(out)),
                     "ddsolve_perform_iterations")
+        if streams is not None:
+            streams[1].wait_stream(streams[0])
         return out
 
     def autotune(self, launches=5):

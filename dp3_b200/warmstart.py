@@ -289,9 +289,10 @@ class LearnedWarmStart:
     def start(self, solver, history):
         """Initial solutions of the interval loaded in `solver`. With the
         history as CUDA tensors every step stays on the GPU, on the solver's
-        stream, without host waits (the solve that follows orders after it);
-        the result is a new CUDA tensor whose pending work is on the solver's
-        stream: solve from it, or synchronize before dropping it."""
+        stream, without host waits: the solver's stream first waits for the
+        caller's current stream (which wrote the history), and the current
+        stream then waits for the solver's stream, so the returned CUDA tensor
+        is ready in the caller's stream order (and in the solver's)."""
         h1 = history[0]
         if not (hasattr(h1, "is_cuda") and h1.is_cuda):
             z = solver.perform_iterations(h1, self.k1)
@@ -309,15 +310,18 @@ class LearnedWarmStart:
             self._y = torch.empty((self.k2,) + tuple(h1.shape), dtype=h1.dtype, device=h1.device)
             self._g1 = torch.empty_like(h1)
             self._torch_stream = torch.cuda.ExternalStream(ptr, device=h1.device)
+        cur = torch.cuda.current_stream(h1.device)
+        g2 = torch.empty_like(h1)
+        # the history and g2's allocation are in the current stream's order
+        self._torch_stream.wait_stream(cur)
         z = solver.perform_iterations(h1, self.k1, out=self._z)
         self.stage1.predict(list(history[:self.HISTORY]) + list(z), out=self._g1)
         y = solver.perform_iterations(self._g1, self.k2, out=self._y)
-        g2 = torch.empty_like(h1)
-        # g2 is written on the solver's stream: order that stream after the
-        # allocating one. The caller uses g2 on the solver's stream (the solve)
-        # or waits for it before dropping it.
-        self._torch_stream.wait_stream(torch.cuda.current_stream(h1.device))
-        return self.stage2.predict([self._g1] + list(y), out=g2)
+        self.stage2.predict([self._g1] + list(y), out=g2)
+        # g2 (written on the solver's stream) is used and freed in the
+        # current stream's order
+        cur.wait_stream(self._torch_stream)
+        return g2
 
     def close(self):
         for st in (self.stage1, self.stage2, self._provisional):
