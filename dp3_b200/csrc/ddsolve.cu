@@ -899,8 +899,12 @@ __device__ __forceinline__ uint64_t GlobalTimerNs() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+// Named barrier of the consumer warps. The non-aligned form counts threads,
+// not warps: it stays correct after lane-divergent code (a lane that spins
+// on the grid barrier while the rest of its warp has gone ahead), where the
+// warp-aligned `bar.sync` would let the warp's other lanes complete it.
 __device__ __forceinline__ void ConsumerBarrier() {
-  asm volatile("bar.sync 1, %0;" ::"n"(kPipeRuns) : "memory");
+  asm volatile("barrier.sync 1, %0;" ::"n"(kPipeRuns) : "memory");
 }
 
 // Bounded wait on an mbarrier phase. Returns false on timeout (or when the CTA
@@ -2391,11 +2395,19 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
       ctx->pipe_ng == 1 && !std::getenv("DDSOLVE_NO_POWERS") && n_runs_all > 0 &&
       (ctx->tune_powers == 1 || (ctx->tune_powers < 0 && run_rows >= 16 * n_runs_all));
   // ---- fragments: rows balanced over the CTAs ----
+  // A row weighs its runs plus a fixed cost; a tile adds the cost of its
+  // reduction, about 1.25 rows per barrier phase (two per direct group; the
+  // sorted reduction as 16 phases), so that CTAs with many short tiles get
+  // fewer rows.
+  auto tile_cost = [](const Tile& t) {
+    const uint32_t phases = (t.flags & kFragDirect) ? 2u * ((t.flags >> 8) & 0xFu) : 16u;
+    return 1.25 * phases * double(t.n + 32);
+  };
   uint64_t total_rows = 0;
   double total_w = 0.0;
   for (const Tile& t : tiles) {
     total_rows += t.rows;
-    total_w += double(t.rows) * double(t.n + 32);
+    total_w += double(t.rows) * double(t.n + 32) + tile_cost(t);
   }
   const uint32_t max_ctas = uint32_t(ctx->n_sm);
   const uint32_t n_ctas = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(max_ctas, total_rows)));
@@ -2406,6 +2418,7 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
     uint32_t cur_cta = 0;
     for (const Tile& t : tiles) {
       const double w = double(t.n + 32);
+      cum += tile_cost(t);
       uint32_t lo = 0;
       while (lo < t.rows) {
         // last row of this tile that stays on cur_cta
