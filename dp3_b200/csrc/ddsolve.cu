@@ -827,8 +827,8 @@ struct PipeParams {
   const uint32_t* tab_off;  // finalisation: (cb, s) -> [tab_off, tab_off+1)
   const uint32_t* tab_ent;  //   entries table * 256 + direction
   uint32_t n_ant, n_dir, n_sub, n_cb;
-  uint32_t acc_stride;    // floats per antenna in the accumulator table (odd)
-  uint32_t gain_stride;   // float2 per antenna in a gain table (odd)
+  uint32_t acc_stride;    // floats per antenna in the accumulator table (PipeAccStride)
+  uint32_t gain_stride;   // float2 per antenna in a gain table (PipeGainStride)
   uint32_t stages;
   uint32_t acc_floats;    // n_ant * acc_stride = one partial slot
   uint32_t owner_groups;  // direction groups per antenna in the sorted reduction
@@ -899,12 +899,15 @@ __device__ __forceinline__ uint64_t GlobalTimerNs() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-// Named barrier of the consumer warps. The non-aligned form counts threads,
-// not warps: it stays correct after lane-divergent code (a lane that spins
-// on the grid barrier while the rest of its warp has gone ahead), where the
-// warp-aligned `bar.sync` would let the warp's other lanes complete it.
+// Named barrier of the consumer warps: the warp-aligned form, entered by
+// whole warps (__syncwarp first, so lane-divergent code before it is
+// reconverged), at the same place by every consumer warp. Measured on B200:
+// the non-aligned `barrier.sync 1, 224` let six waiting warps through while
+// the seventh was still busy, and so did `bar.sync` after a loop that only
+// one warp ran; waits of that kind are done by every warp instead.
 __device__ __forceinline__ void ConsumerBarrier() {
-  asm volatile("barrier.sync 1, %0;" ::"n"(kPipeRuns) : "memory");
+  __syncwarp();
+  asm volatile("bar.sync 1, %0;" ::"n"(kPipeRuns) : "memory");
 }
 
 // Bounded wait on an mbarrier phase. Returns false on timeout (or when the CTA
@@ -938,6 +941,60 @@ __device__ __forceinline__ void LoadVisShared(const char* base, uint32_t idx,
     v[1] = make_float2(x.z, x.w);
     v[2] = make_float2(y.x, y.y);
     v[3] = make_float2(y.z, y.w);
+  }
+}
+
+// Accumulator table of pipe_kernel, per antenna `stride` floats: the
+// numerators of every direction (NPOL complex values each), then the
+// denominators (NPOL real values each), so that one direction's update is
+// one vector read-modify-write of each (stride = 4 mod 8: distinct
+// shared-memory banks for consecutive antennas).
+template <int NPOL>
+__device__ __forceinline__ void AccAdd(float* acc, uint32_t a, uint32_t stride, uint32_t n_dir,
+                                       uint32_t d, const float2 (&num)[NPOL],
+                                       const float (&den)[NPOL]) {
+  float* row = acc + size_t(a) * stride;
+  if constexpr (NPOL == 2) {
+    float4* pn = reinterpret_cast<float4*>(row) + d;
+    float4 v = *pn;
+    v.x += num[0].x;
+    v.y += num[0].y;
+    v.z += num[1].x;
+    v.w += num[1].y;
+    *pn = v;
+    float2* pd = reinterpret_cast<float2*>(row + 4 * n_dir) + d;
+    float2 w = *pd;
+    w.x += den[0];
+    w.y += den[1];
+    *pd = w;
+  } else {
+    float2* pn = reinterpret_cast<float2*>(row) + d;
+    float2 v = *pn;
+    v.x += num[0].x;
+    v.y += num[0].y;
+    *pn = v;
+    row[2 * n_dir + d] += den[0];
+  }
+}
+__host__ __device__ constexpr uint32_t AccNumOffset(uint32_t npol, uint32_t d, uint32_t q) {
+  return (d * npol + q) * 2;
+}
+__host__ __device__ constexpr uint32_t AccDenOffset(uint32_t npol, uint32_t n_dir, uint32_t d,
+                                                    uint32_t q) {
+  return 2 * npol * n_dir + d * npol + q;
+}
+
+// Gains of antenna `ant`, direction d from a gain table (NPOL float2 per
+// direction; for two polarizations one 16-byte load: stride = 2 mod 4).
+template <int NPOL>
+__device__ __forceinline__ void LoadGains(const float2* gtab, uint32_t ant, uint32_t stride,
+                                          uint32_t d, float2 (&g)[NPOL]) {
+  if constexpr (NPOL == 2) {
+    const float4 v = *reinterpret_cast<const float4*>(gtab + size_t(ant) * stride + 2 * d);
+    g[0] = make_float2(v.x, v.y);
+    g[1] = make_float2(v.z, v.w);
+  } else {
+    g[0] = gtab[size_t(ant) * stride + d];
   }
 }
 
@@ -988,32 +1045,36 @@ __device__ __forceinline__ void FinalizeDistributed(const PipeParams& p, int cti
     NeumaierSum nr[NPOL], ni[NPOL], dn[NPOL];
     const uint32_t j0 = p.fin_off[cb * p.n_sub + s];
     const uint32_t j1 = p.fin_off[cb * p.n_sub + s + 1];
-    const size_t off = size_t(ant) * p.acc_stride + d * NPOL * 3;
+    // the item's numerators and denominators in a partial slot (AccAdd)
+    const size_t off_n = size_t(ant) * p.acc_stride + AccNumOffset(NPOL, d, 0);
+    const size_t off_d = size_t(ant) * p.acc_stride + AccDenOffset(NPOL, p.n_dir, d, 0);
     uint32_t j = j0;
     for (; j + 4 <= j1; j += 4) {  // four slots in flight
       float v[4][NPOL * 3];
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        const float* a = p.partials + size_t(p.fin_visits[j + u]) * p.acc_floats + off;
+        const float* a = p.partials + size_t(p.fin_visits[j + u]) * p.acc_floats;
 #pragma unroll
-        for (int e = 0; e < NPOL * 3; ++e) v[u][e] = __ldcg(a + e);
+        for (int e = 0; e < NPOL * 2; ++e) v[u][e] = __ldcg(a + off_n + e);
+#pragma unroll
+        for (int q = 0; q < NPOL; ++q) v[u][NPOL * 2 + q] = __ldcg(a + off_d + q);
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u)
 #pragma unroll
         for (int q = 0; q < NPOL; ++q) {
-          nr[q].Add(v[u][q * 3 + 0]);
-          ni[q].Add(v[u][q * 3 + 1]);
-          dn[q].Add(v[u][q * 3 + 2]);
+          nr[q].Add(v[u][q * 2 + 0]);
+          ni[q].Add(v[u][q * 2 + 1]);
+          dn[q].Add(v[u][NPOL * 2 + q]);
         }
     }
     for (; j < j1; ++j) {
-      const float* a = p.partials + size_t(p.fin_visits[j]) * p.acc_floats + off;
+      const float* a = p.partials + size_t(p.fin_visits[j]) * p.acc_floats;
 #pragma unroll
       for (int q = 0; q < NPOL; ++q) {
-        nr[q].Add(__ldcg(a + q * 3 + 0));
-        ni[q].Add(__ldcg(a + q * 3 + 1));
-        dn[q].Add(__ldcg(a + q * 3 + 2));
+        nr[q].Add(__ldcg(a + off_n + q * 2 + 0));
+        ni[q].Add(__ldcg(a + off_n + q * 2 + 1));
+        dn[q].Add(__ldcg(a + off_d + q));
       }
     }
     double2* sol = p.solutions + size_t(item) * NPOL;
@@ -1374,6 +1435,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
       MbarInit(&gfree[b], kPipeConsumerWarps);
     }
     *s_err = 0;
+    *s_last = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     if (p.use_handle && blockIdx.x == 0) cudaGraphSetConditional(p.handle, 0);
   }
@@ -1533,11 +1595,11 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
             for (int q = 0; q < NPOL; ++q) {
               ga[q] = make_float2(0.f, 0.f);
               gb[q] = make_float2(0.f, 0.f);
-              const uint32_t d = g + k * NG;
-              if (d < n_dir) {
-                ga[q] = gtab[a1 * p.gain_stride + d * NPOL + q];
-                gb[q] = gtab[a2 * p.gain_stride + d * NPOL + q];
-              }
+            }
+            const uint32_t d = g + k * NG;
+            if (d < n_dir) {
+              LoadGains<NPOL>(gtab, a1, p.gain_stride, d, ga);
+              LoadGains<NPOL>(gtab, a2, p.gain_stride, d, gb);
             }
 #pragma unroll
             for (int c = 0; c < NCORR; ++c)
@@ -1686,9 +1748,9 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
             const uint32_t d = g + k * NG;
             if (d < n_dir) {
               float2 gb[NPOL];
-#pragma unroll
-              for (int q = 0; q < NPOL; ++q) gb[q] = gtab[b * p.gain_stride + d * NPOL + q];
-              float* x = acc + a * p.acc_stride + d * NPOL * 3;
+              LoadGains<NPOL>(gtab, b, p.gain_stride, d, gb);
+              float2 num[NPOL];
+              float den[NPOL];
 #pragma unroll
               for (int q = 0; q < NPOL; ++q) {
                 float2 n = make_float2(0.f, 0.f);
@@ -1710,10 +1772,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
                     dd += cnorm(gb[rp]) * Q[k][c];
                   }
                 }
-                x[q * 3 + 0] += n.x;
-                x[q * 3 + 1] += n.y;
-                x[q * 3 + 2] += dd;
+                num[q] = n;
+                den[q] = dd;
               }
+              AccAdd<NPOL>(acc, a, p.acc_stride, n_dir, d, num, den);
             }
           }
         }
@@ -1803,8 +1865,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
           const uint32_t k = grp + i * n_groups;
           if (k < n_dir) {
             float2 gb[NPOL];
-#pragma unroll
-            for (int q = 0; q < NPOL; ++q) gb[q] = gtab[b * p.gain_stride + k * NPOL + q];
+            LoadGains<NPOL>(gtab, b, p.gain_stride, k, gb);
             float2 Pc[NCORR];
             float Qc[NCORR];
 #pragma unroll
@@ -1840,13 +1901,14 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
       for (int i = 0; i < DMAX; ++i) {
         const uint32_t k = grp + i * n_groups;
         if (k < n_dir) {
-          float* x = acc + a * p.acc_stride + k * NPOL * 3;
+          float2 num[NPOL];
+          float den[NPOL];
 #pragma unroll
           for (int q = 0; q < NPOL; ++q) {
-            x[q * 3 + 0] += sum[i][q][0];
-            x[q * 3 + 1] += sum[i][q][1];
-            x[q * 3 + 2] += sum[i][q][2];
+            num[q] = make_float2(sum[i][q][0], sum[i][q][1]);
+            den[q] = sum[i][q][2];
           }
+          AccAdd<NPOL>(acc, a, p.acc_stride, n_dir, k, num, den);
         }
       }
     }
@@ -1854,25 +1916,32 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
   }
   if (cur_visit != 0xFFFFFFFFu) end_visit();
   // Grid barrier: every CTA has flushed every partial slot (the launch is
-  // cooperative, so all CTAs are resident). Bounded: a timeout flags an error
-  // and the finalisation goes ahead on whatever is there.
+  // cooperative, so all CTAs are resident). Every consumer warp waits on the
+  // arrival count itself (lane 0 polls, the warp follows): a named barrier
+  // after one warp's polling loop was measured to let the other warps
+  // through early. Bounded: a timeout flags an error and the finalisation
+  // goes ahead on whatever is there.
   __threadfence();
-  ConsumerBarrier();
-  if (ctid == 0) {
-    atomicAdd(&p.counters[2], 1u);
+  ConsumerBarrier();  // this CTA's slots are written
+  if (ctid == 0) atomicAdd(&p.counters[2], 1u);
+  {
     volatile uint32_t* arrived = &p.counters[2];
-    if (*arrived < gridDim.x) {
-      const uint64_t t0 = GlobalTimerNs();
-      for (uint32_t n = 1; *arrived < gridDim.x; ++n) {
-        if ((n & 63u) == 0 && GlobalTimerNs() - t0 > kWaitBudgetNs) {
+    const uint64_t t0 = GlobalTimerNs();
+    for (uint32_t n = 1;; ++n) {
+      // lane 0 decides (all arrived, or out of time) and the warp follows
+      uint32_t stop = 0;
+      if (lane == 0) {
+        stop = *arrived >= gridDim.x ? 1u : 0u;
+        if (!stop && (n & 63u) == 0 && GlobalTimerNs() - t0 > kWaitBudgetNs) {
           atomicExch(&p.counters[1], 1u);
-          break;
+          stop = 1u;
         }
       }
+      if (__shfl_sync(0xFFFFFFFFu, stop, 0)) break;
+      __nanosleep(64);
     }
     __threadfence();
   }
-  ConsumerBarrier();
   FinalizeDistributed<NPOL>(p, ctid, s_sum, s_cnt, s_last);
 }
 
@@ -2155,6 +2224,23 @@ const KernelEntry* FindPipeKernel(int ncorr, int npol, int n_dir) {
 }
 
 uint32_t OddAtLeast(uint32_t x) { return x | 1u; }
+
+// Strides of pipe_kernel's accumulator rows (floats; 4 mod 8, see AccAdd)
+// and gain-table rows (float2; 2 mod 4 for two polarizations, see
+// LoadGains, else odd).
+uint32_t PipeAccStride(uint32_t n_dir, uint32_t n_pol) {
+  uint32_t s = n_dir * n_pol * 3;
+  while (s % 8 != 4) ++s;
+  return s;
+}
+uint32_t PipeGainStride(uint32_t n_dir, uint32_t n_pol) {
+  uint32_t s = n_dir * n_pol;
+  if (n_pol == 2) {
+    while (s % 4 != 2) ++s;
+    return s;
+  }
+  return OddAtLeast(s);
+}
 
 // One pipeline stage of pipe_kernel: the fragment's run antennas (first row
 // only), then one row of data and of every direction's model.
@@ -2599,8 +2685,8 @@ int BuildPlanImpl(ddsolve_ctx* ctx, bool allow_pipe) {
     const KernelEntry* pe =
         FindPipeKernel(int(ctx->n_corr), int(ctx->n_pol), int(ctx->n_dir));
     if (pe) ctx->pipe_ng = uint32_t(pe->ng);
-    const uint32_t acc_stride = OddAtLeast(ctx->n_dir * ctx->n_pol * 3);
-    const uint32_t gain_stride = OddAtLeast(ctx->n_dir * ctx->n_pol);
+    const uint32_t acc_stride = PipeAccStride(ctx->n_dir, ctx->n_pol);
+    const uint32_t gain_stride = PipeGainStride(ctx->n_dir, ctx->n_pol);
     uint32_t stages = 0;
     for (uint32_t st = kPipeMaxStages; st >= 2 && pe; --st)
       if (PipeSmemBytes(ctx, st, acc_stride, gain_stride) <= size_t(max_optin)) {
