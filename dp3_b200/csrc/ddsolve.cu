@@ -841,6 +841,7 @@ struct PipeParams {
       off_wsum, off_stages;
   const uint32_t* fin_off;
   const uint32_t* fin_visits;
+  const uint32_t* fin_first;  // first visit of each list when all lists are ranges, else null
   const uint32_t* dir_of_sub;
   uint32_t* cb_flag;     // channel block holds non-finite solutions
   double* cb_avg;        // replacement value for them (MakeSolutionsFinite)
@@ -1035,54 +1036,17 @@ __device__ __forceinline__ void FinalizeDistributed(const PipeParams& p, int cti
   const uint32_t n_items = p.n_cb * n_items_cb;
   double nsum = 0.0;
   uint32_t ncnt = 0;
-  for (uint32_t item = blockIdx.x * kPipeRuns + ctid; item < n_items;
-       item += gridDim.x * kPipeRuns) {
-    const uint32_t cb = item / n_items_cb;
-    const uint32_t it = item - cb * n_items_cb;
-    const uint32_t ant = it / p.n_sub;
-    const uint32_t s = it - ant * p.n_sub;
-    const uint32_t d = p.dir_of_sub[s];
-    NeumaierSum nr[NPOL], ni[NPOL], dn[NPOL];
-    const uint32_t j0 = p.fin_off[cb * p.n_sub + s];
-    const uint32_t j1 = p.fin_off[cb * p.n_sub + s + 1];
-    // the item's numerators and denominators in a partial slot (AccAdd)
-    const size_t off_n = size_t(ant) * p.acc_stride + AccNumOffset(NPOL, d, 0);
-    const size_t off_d = size_t(ant) * p.acc_stride + AccDenOffset(NPOL, p.n_dir, d, 0);
-    uint32_t j = j0;
-    for (; j + 4 <= j1; j += 4) {  // four slots in flight
-      float v[4][NPOL * 3];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const float* a = p.partials + size_t(p.fin_visits[j + u]) * p.acc_floats;
-#pragma unroll
-        for (int e = 0; e < NPOL * 2; ++e) v[u][e] = __ldcg(a + off_n + e);
-#pragma unroll
-        for (int q = 0; q < NPOL; ++q) v[u][NPOL * 2 + q] = __ldcg(a + off_d + q);
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int q = 0; q < NPOL; ++q) {
-          nr[q].Add(v[u][q * 2 + 0]);
-          ni[q].Add(v[u][q * 2 + 1]);
-          dn[q].Add(v[u][NPOL * 2 + q]);
-        }
-    }
-    for (; j < j1; ++j) {
-      const float* a = p.partials + size_t(p.fin_visits[j]) * p.acc_floats;
-#pragma unroll
-      for (int q = 0; q < NPOL; ++q) {
-        nr[q].Add(__ldcg(a + off_n + q * 2 + 0));
-        ni[q].Add(__ldcg(a + off_n + q * 2 + 1));
-        dn[q].Add(__ldcg(a + off_d + q));
-      }
-    }
+  // One item: the merged sums and the old solutions in, the next solutions,
+  // their norm terms, the gain tables and the non-finite flag out.
+  auto finish = [&](uint32_t item, uint32_t cb, uint32_t ant, uint32_t s,
+                    const double2 (&old_in)[NPOL], const NeumaierSum (&nr)[NPOL],
+                    const NeumaierSum (&ni)[NPOL], const NeumaierSum (&dn)[NPOL]) {
     double2* sol = p.solutions + size_t(item) * NPOL;
     double2 old[NPOL], nxt[NPOL];
     bool pair_ok = true;
 #pragma unroll
     for (int q = 0; q < NPOL; ++q) {
-      old[q] = sol[q];
+      old[q] = old_in[q];
       pair_ok = pair_ok && dfinite(old[q]);
     }
     if (!pair_ok && p.cb_flag[cb]) {
@@ -1105,7 +1069,7 @@ __device__ __forceinline__ void FinalizeDistributed(const PipeParams& p, int cti
       double2* out = p.next_out + size_t(item) * NPOL;
 #pragma unroll
       for (int q = 0; q < NPOL; ++q) out[q] = nxt[q];
-      continue;
+      return;
     }
 #pragma unroll
     for (int q = 0; q < NPOL; ++q) {
@@ -1158,6 +1122,91 @@ __device__ __forceinline__ void FinalizeDistributed(const PipeParams& p, int cti
     }
     WriteTables<NPOL>(p, cb, ant, s, nxt);
     if (!all_finite) p.cb_newflag[cb] = 1u;
+  };
+  // A thread's items, kFinBatch at a time: their index, slot-list and
+  // solution reads are issued together and their partial slots merged in
+  // rounds, so that the chains of dependent L2 reads of the items overlap
+  // (each item's slots are still added in slot order).
+  constexpr int kFinBatch = 4;
+  const uint32_t item_step = gridDim.x * kPipeRuns;
+  for (uint32_t item0 = blockIdx.x * kPipeRuns + ctid; item0 < n_items;
+       item0 += kFinBatch * item_step) {
+    uint32_t cbv[kFinBatch], antv[kFinBatch], sv[kFinBatch], dv[kFinBatch];
+    uint32_t j0v[kFinBatch], j1v[kFinBatch], v0v[kFinBatch];
+    double2 oldv[kFinBatch][NPOL];
+#pragma unroll
+    for (int b = 0; b < kFinBatch; ++b) {
+      const uint32_t item = item0 + b * item_step;
+      cbv[b] = antv[b] = sv[b] = dv[b] = 0;
+      j0v[b] = j1v[b] = v0v[b] = 0;
+#pragma unroll
+      for (int q = 0; q < NPOL; ++q) oldv[b][q] = make_double2(0.0, 0.0);
+      if (item < n_items) {
+        const uint32_t cb = item / n_items_cb;
+        const uint32_t it = item - cb * n_items_cb;
+        const uint32_t ant = it / p.n_sub;
+        const uint32_t s = it - ant * p.n_sub;
+        cbv[b] = cb;
+        antv[b] = ant;
+        sv[b] = s;
+        dv[b] = p.dir_of_sub[s];
+        j0v[b] = p.fin_off[cb * p.n_sub + s];
+        j1v[b] = p.fin_off[cb * p.n_sub + s + 1];
+        if (p.fin_first) v0v[b] = p.fin_first[cb * p.n_sub + s];
+        const double2* sol = p.solutions + size_t(item) * NPOL;
+#pragma unroll
+        for (int q = 0; q < NPOL; ++q) oldv[b][q] = sol[q];
+      }
+    }
+    uint32_t n_rounds = 0;
+#pragma unroll
+    for (int b = 0; b < kFinBatch; ++b) n_rounds = max(n_rounds, j1v[b] - j0v[b]);
+    NeumaierSum nr[kFinBatch][NPOL], ni[kFinBatch][NPOL], dn[kFinBatch][NPOL];
+    constexpr int kR = 4;  // slots per item and round
+    for (uint32_t k = 0; k < n_rounds; k += kR) {
+      uint32_t vis[kFinBatch][kR];
+#pragma unroll
+      for (int b = 0; b < kFinBatch; ++b)
+#pragma unroll
+        for (int u = 0; u < kR; ++u)
+          vis[b][u] = j0v[b] + k + u >= j1v[b] ? 0xFFFFFFFFu
+                      : p.fin_first            ? v0v[b] + k + u
+                                               : p.fin_visits[j0v[b] + k + u];
+      float v[kFinBatch][kR][NPOL * 3];
+#pragma unroll
+      for (int b = 0; b < kFinBatch; ++b) {
+        // the item's numerators and denominators in a partial slot (AccAdd)
+        const size_t off_n = size_t(antv[b]) * p.acc_stride + AccNumOffset(NPOL, dv[b], 0);
+        const size_t off_d =
+            size_t(antv[b]) * p.acc_stride + AccDenOffset(NPOL, p.n_dir, dv[b], 0);
+#pragma unroll
+        for (int u = 0; u < kR; ++u) {
+          if (vis[b][u] == 0xFFFFFFFFu) continue;
+          const float* a = p.partials + size_t(vis[b][u]) * p.acc_floats;
+#pragma unroll
+          for (int e = 0; e < NPOL * 2; ++e) v[b][u][e] = __ldcg(a + off_n + e);
+#pragma unroll
+          for (int q = 0; q < NPOL; ++q) v[b][u][NPOL * 2 + q] = __ldcg(a + off_d + q);
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < kFinBatch; ++b)
+#pragma unroll
+        for (int u = 0; u < kR; ++u) {
+          if (vis[b][u] == 0xFFFFFFFFu) continue;
+#pragma unroll
+          for (int q = 0; q < NPOL; ++q) {
+            nr[b][q].Add(v[b][u][q * 2 + 0]);
+            ni[b][q].Add(v[b][u][q * 2 + 1]);
+            dn[b][q].Add(v[b][u][NPOL * 2 + q]);
+          }
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < kFinBatch; ++b) {
+      const uint32_t item = item0 + b * item_step;
+      if (item < n_items) finish(item, cbv[b], antv[b], sv[b], oldv[b], nr[b], ni[b], dn[b]);
+    }
   }
   // Per-CTA norm partial, then the last CTA finishes the iteration.
   s_sum[ctid] = nsum;
@@ -2075,7 +2124,8 @@ struct ddsolve_ctx {
   uint32_t n_power_tiles = 0, power_floats = 0;
   DevBuf d_power_tiles, d_powers;
   DevBuf d_slabs, d_visits, d_cta_off, d_slab_sol, d_partials, d_fin_off,
-      d_fin_visits, d_dir_of_sub, d_block_sum, d_block_cnt;
+      d_fin_visits, d_fin_first, d_dir_of_sub, d_block_sum, d_block_cnt;
+  bool fin_ranges = false;  // pipe plan: every finalisation list is a visit range
   // solver state
   DevBuf d_sol, d_next, d_state, d_nonfinite, d_mags, d_settings;
   DevBuf d_chain;  // outputs of ddsolve_perform_iterations
@@ -2562,6 +2612,17 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
     fin_visits.insert(fin_visits.end(), lists[i].begin(), lists[i].end());
   }
   fin_off[lists.size()] = uint32_t(fin_visits.size());
+  // Visits are numbered in CTA order and CTAs take the slabs in order, so a
+  // (channel block, sub-solution) whose slabs are consecutive has a range of
+  // visits: the finalisation then needs its first visit only.
+  bool ranges = true;
+  std::vector<uint32_t> fin_first(lists.size(), 0);
+  for (size_t i = 0; i < lists.size() && ranges; ++i) {
+    for (size_t k = 1; k < lists[i].size() && ranges; ++k)
+      ranges = lists[i][k] == lists[i][k - 1] + 1;
+    if (!lists[i].empty()) fin_first[i] = lists[i][0];
+  }
+  ctx->fin_ranges = ranges;
 
   // ---- shared-memory layout ----
   auto align = [](size_t x, size_t a) { return (x + a - 1) / a * a; };
@@ -2629,6 +2690,7 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
   if ((rc = upload(ctx->d_slab_sol, slab_sol.data(), slab_sol.size() * 4))) return rc;
   if ((rc = upload(ctx->d_fin_off, fin_off.data(), fin_off.size() * 4))) return rc;
   if ((rc = upload(ctx->d_fin_visits, fin_visits.data(), fin_visits.size() * 4))) return rc;
+  if ((rc = upload(ctx->d_fin_first, fin_first.data(), fin_first.size() * 4))) return rc;
   if ((rc = upload(ctx->d_dir_of_sub, ctx->dir_of_sub.data(), ctx->dir_of_sub.size() * 4)))
     return rc;
   if ((rc = upload(ctx->d_tab_cb, tab_cb.data(), tab_cb.size() * 4))) return rc;
@@ -3007,6 +3069,7 @@ PipeParams MakePipeParams(ddsolve_ctx* ctx, bool host_mode, bool use_handle) {
   p.off_stages = ctx->off_stages;
   p.fin_off = ctx->d_fin_off.as<uint32_t>();
   p.fin_visits = ctx->d_fin_visits.as<uint32_t>();
+  p.fin_first = ctx->fin_ranges ? ctx->d_fin_first.as<uint32_t>() : nullptr;
   p.dir_of_sub = ctx->d_dir_of_sub.as<uint32_t>();
   p.cb_flag = ctx->d_cb_flag.as<uint32_t>();
   p.cb_avg = ctx->d_cb_avg.as<double>();
