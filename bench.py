@@ -666,6 +666,10 @@ def run_gpu_arm(args):
     alg_bytes = cfg.n_vis * 16 * (1 + cfg.n_directions)
     peak, peak_kind = _peaks()
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+    # the kernel of the autotuned plan (the default plan prefers pipe_kernel)
+    use_pipe = (tuning or {}).get("use_pipe", -1)
+    kernel_name = ("stream_kernel" if use_pipe == 0 else
+                   "pipe_kernel" if use_pipe == 1 else "default plan (pipe_kernel where it applies)")
     traffic = None
     prof = os.path.join(ROOT, "profiles", f"pipe_kernel_c{args.config}_traffic.json")
     if os.path.exists(prof):
@@ -696,7 +700,7 @@ def run_gpu_arm(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "pipe_kernel" if cfg.n_directions <= 12 else "stream_kernel",
+                     "kernel": kernel_name,
                      "kernel_ms": kernel_ms,
                      "algorithmic_bytes_per_launch": alg_bytes},
         "gpu_launches": int(launches),
