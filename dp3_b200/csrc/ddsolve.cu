@@ -1069,6 +1069,9 @@ __device__ __forceinline__ void FinalizeDistributed(const PipeParams& p, int cti
       double2* out = p.next_out + size_t(item) * NPOL;
 #pragma unroll
       for (int q = 0; q < NPOL; ++q) out[q] = nxt[q];
+      // the gain tables of a chained next pass, which starts from `nxt`
+      // (every other launch rebuilds them from its own solutions first)
+      WriteTables<NPOL>(p, cb, ant, s, nxt);
       return;
     }
 #pragma unroll
@@ -3800,9 +3803,28 @@ int ddsolve_perform_iterations(ddsolve_ctx* ctx, const double* start, uint32_t n
   if (ctx->plan_dirty && (rc = BuildPlan(ctx)) != DDSOLVE_OK) return rc;
   const size_t n_sol = size_t(ctx->n_cb) * ctx->n_ant * ctx->n_sub * ctx->n_pol;
   const size_t bytes = n_sol * sizeof(double2);
-  DDS_CHECK_CUDA(ctx, ctx->d_chain.Reserve(bytes * n_passes));
-  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->d_sol.ptr, start, bytes, cudaMemcpyDefault,
-                                      ctx->stream));
+  auto on_device = [&](const void* ptr) {
+    cudaPointerAttributes attr{};
+    const bool dev = cudaPointerGetAttributes(&attr, ptr) == cudaSuccess &&
+                     (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged) &&
+                     attr.device == ctx->device;
+    cudaGetLastError();  // unregistered host memory is not an error here
+    return dev;
+  };
+  const bool dev_out = on_device(outputs);
+  // Device arrays on this GPU are used in place: the first pass reads `start`
+  // (passes never write their input) and every pass writes its slot of
+  // `outputs`, unless the two overlap.
+  const char* s0 = reinterpret_cast<const char*>(start);
+  const char* o0 = reinterpret_cast<const char*>(outputs);
+  const bool overlap = s0 < o0 + bytes * n_passes && o0 < s0 + bytes;
+  const bool dev_in = !overlap && on_device(start);
+  const bool in_place_out = dev_out && !overlap;
+  if (!in_place_out) DDS_CHECK_CUDA(ctx, ctx->d_chain.Reserve(bytes * n_passes));
+  char* chain = in_place_out ? reinterpret_cast<char*>(outputs) : ctx->d_chain.as<char>();
+  if (!dev_in)
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->d_sol.ptr, start, bytes, cudaMemcpyDefault,
+                                        ctx->stream));
   uint64_t launches = 0;
   // Pass k reads its solutions from the previous pass's slot of the chain
   // buffer and writes its own slot: the solver's solution buffers are
@@ -3815,31 +3837,37 @@ int ddsolve_perform_iterations(ddsolve_ctx* ctx, const double* start, uint32_t n
       c->d_next.ptr = next;
     }
   } restore{ctx, ctx->d_sol.ptr, ctx->d_next.ptr};
+  if (ctx->use_pipe) {
+    // Once per call: no replacement values from an earlier solve apply
+    // (next-solutions passes neither read nor write the new-non-finite flags,
+    // which every solve clears itself), and every pipe_kernel launch leaves
+    // its counters at zero.
+    DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_flag.ptr, 0, size_t(ctx->n_cb) * 4,
+                                        ctx->stream));
+    DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.ptr, 0, 16, ctx->stream));
+  }
+  if (dev_in) ctx->d_sol.ptr = const_cast<double*>(start);
   for (uint32_t k = 0; k < n_passes; ++k) {
-    if (k > 0) ctx->d_sol.ptr = ctx->d_chain.as<char>() + bytes * (k - 1);
-    ctx->d_next.ptr = ctx->d_chain.as<char>() + bytes * k;
+    if (k > 0) ctx->d_sol.ptr = chain + bytes * (k - 1);
+    ctx->d_next.ptr = chain + bytes * k;
     if (ctx->use_pipe) {
-      DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_flag.ptr, 0, size_t(ctx->n_cb) * 4,
-                                          ctx->stream));
-      DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_done.ptr, 0, size_t(ctx->n_cb) * 4,
-                                          ctx->stream));
-      DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.ptr, 0, 16, ctx->stream));
-      if ((rc = LaunchBuildTables(ctx)) != DDSOLVE_OK) return rc;
-      if (ctx->use_powers && ctx->powers_dirty) ++launches;
-      if ((rc = LaunchPowers(ctx, false)) != DDSOLVE_OK) return rc;
-      launches += 2;
+      // pass k > 0 uses the gain tables that pass k - 1 wrote from its output
+      if (k == 0) {
+        if ((rc = LaunchBuildTables(ctx)) != DDSOLVE_OK) return rc;
+        if (ctx->use_powers && ctx->powers_dirty) ++launches;
+        if ((rc = LaunchPowers(ctx, false)) != DDSOLVE_OK) return rc;
+        ++launches;
+      }
+      ++launches;
     } else {
       launches += 2;
     }
     if ((rc = LaunchIteration(ctx, true, false, false)) != DDSOLVE_OK) return rc;
   }
-  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(outputs, ctx->d_chain.ptr, bytes * n_passes,
-                                      cudaMemcpyDefault, ctx->stream));
+  if (!in_place_out)
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(outputs, ctx->d_chain.ptr, bytes * n_passes,
+                                        cudaMemcpyDefault, ctx->stream));
   ctx->last_launches = launches;
-  cudaPointerAttributes attr{};
-  const bool dev_out = cudaPointerGetAttributes(&attr, outputs) == cudaSuccess &&
-                       (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged);
-  cudaGetLastError();
   if (dev_out) return DDSOLVE_OK;  // device outputs: no wait (see the header)
   if ((rc = StageCounters(ctx)) != DDSOLVE_OK) return rc;
   DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
