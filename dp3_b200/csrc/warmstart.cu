@@ -116,15 +116,20 @@ __host__ __device__ constexpr uint32_t InstrDesc(int m, int n) {
 // 16-byte groups are loaded into registers before any is stored, so that
 // their global-memory latencies overlap.
 template <int R>
-__device__ __forceinline__ void LoadChunk(unsigned char* dst, const uint16_t* src, int ld,
-                                          int trans, int rows, int K, int row0, int k0) {
-  constexpr int kGroups = R * (kKChunk / 8);
-  constexpr int kPerThread = kGroups / kGemmThreads;
-  static_assert(kGroups % kGemmThreads == 0, "chunk groups must split evenly");
-  uint4 q[kPerThread];
+__host__ __device__ constexpr int ChunkGroups() {
+  return R * (kKChunk / 8) / kGemmThreads;  // 16-byte groups per thread
+}
+
+// Global reads of a chunk (R rows x kKChunk of K) into registers, all of a
+// thread's 16-byte groups issued before any is used.
+template <int R>
+__device__ __forceinline__ void LoadChunkRegs(uint4 (&q)[ChunkGroups<R>()], const uint16_t* src,
+                                              int ld, int trans, int rows, int K, int row0,
+                                              int k0) {
+  static_assert((R * (kKChunk / 8)) % kGemmThreads == 0, "chunk groups must split evenly");
   const bool fast = !trans && (ld & 7) == 0;
 #pragma unroll
-  for (int i = 0; i < kPerThread; ++i) {
+  for (int i = 0; i < ChunkGroups<R>(); ++i) {
     const int g = threadIdx.x + i * kGemmThreads;
     const int r = g >> 3, kc = g & 7;
     const int row = row0 + r, k = k0 + kc * 8;
@@ -140,8 +145,16 @@ __device__ __forceinline__ void LoadChunk(unsigned char* dst, const uint16_t* sr
       memcpy(&q[i], v, 16);
     }
   }
+}
+
+// The chunk into shared memory in the canonical K-major no-swizzle layout:
+// 8x8 core matrices of 128 contiguous bytes, K-adjacent cores 128 B apart,
+// 8-row groups 1024 B apart.
+template <int R>
+__device__ __forceinline__ void StoreChunkRegs(unsigned char* dst,
+                                               const uint4 (&q)[ChunkGroups<R>()]) {
 #pragma unroll
-  for (int i = 0; i < kPerThread; ++i) {
+  for (int i = 0; i < ChunkGroups<R>(); ++i) {
     const int g = threadIdx.x + i * kGemmThreads;
     const int r = g >> 3, kc = g & 7;
     *reinterpret_cast<uint4*>(dst + ((r >> 3) * 8 + kc) * 128 + (r & 7) * 16) = q[i];
@@ -189,17 +202,26 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmParams p) 
   const uint32_t tmem = *tmem_slot;
 
   const int n_chunks = (p.K + kKChunk - 1) / kKChunk;
-  uint32_t waits[2] = {0u, 0u};  // completed waits per buffer = parity of the next
-  uint32_t commits[2] = {0u, 0u};
+  // Chunk c uses buffer c & 1; its MMAs commit to mbar[c & 1], whose phase
+  // (c >> 1) & 1 completes when they are done. Every commit is waited for
+  // exactly once: before chunk c + 2 reuses the buffer, or after the loop.
   constexpr uint32_t kIdesc = InstrDesc(kMTile, NT);
+  // Chunk c + 1's global reads are issued before chunk c's MMAs, so that their
+  // latency overlaps the barrier, the MMA issue and the buffer wait.
+  uint4 qa[ChunkGroups<kMTile>()], qb[ChunkGroups<NT>()];
+  if (n_chunks > 0) {
+    LoadChunkRegs<kMTile>(qa, p.a, p.lda, p.a_trans, p.M, p.K, m0, 0);
+    LoadChunkRegs<NT>(qb, p.b, p.ldb, p.b_trans, p.N, p.K, n0, 0);
+  }
   for (int c = 0; c < n_chunks; ++c) {
     const int b = c & 1;
-    if (commits[b] > waits[b]) {  // the MMAs of chunk c - 2 still read buffer b
-      MbarWait(&mbar[b], waits[b] & 1u, p.error);
-      ++waits[b];
+    if (c >= 2) MbarWait(&mbar[b], uint32_t((c - 2) >> 1) & 1u, p.error);  // chunk c - 2
+    StoreChunkRegs<kMTile>(a_buf + b * kABytes, qa);
+    StoreChunkRegs<NT>(b_buf + b * kBBytes, qb);
+    if (c + 1 < n_chunks) {
+      LoadChunkRegs<kMTile>(qa, p.a, p.lda, p.a_trans, p.M, p.K, m0, (c + 1) * kKChunk);
+      LoadChunkRegs<NT>(qb, p.b, p.ldb, p.b_trans, p.N, p.K, n0, (c + 1) * kKChunk);
     }
-    LoadChunk<kMTile>(a_buf + b * kABytes, p.a, p.lda, p.a_trans, p.M, p.K, m0, c * kKChunk);
-    LoadChunk<NT>(b_buf + b * kBBytes, p.b, p.ldb, p.b_trans, p.N, p.K, n0, c * kKChunk);
     // generic-proxy shared-memory writes -> visible to the tensor core (async proxy)
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
@@ -224,18 +246,22 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmParams p) 
               SmemAddr(&mbar[b]))
           : "memory");
     }
-    ++commits[b];  // every thread tracks the commit count
   }
   // All MMAs done (also before freeing tensor memory after a timeout).
-  for (int b = 0; b < 2; ++b)
-    while (commits[b] > waits[b]) {
-      MbarWait(&mbar[b], waits[b] & 1u, p.error);
-      ++waits[b];
-    }
+  for (int c = n_chunks >= 2 ? n_chunks - 2 : 0; c < n_chunks; ++c)
+    MbarWait(&mbar[c & 1], uint32_t(c >> 1) & 1u, p.error);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
   // Epilogue: warp w reads TMEM lanes 32w..32w+31 = rows m0 + 32w + lane.
+  // 16-byte output (and mask) accesses where every row start is 16-byte
+  // aligned: column groups start at multiples of 32 elements.
   const int row = m0 + warp * 32 + lane;
+  const int esz = p.epilogue == kEpiF32 ? 4 : 2;
+  const bool vec_out = (reinterpret_cast<uintptr_t>(p.c) & 15u) == 0 &&
+                       (size_t(p.ldc) * esz) % 16 == 0;
+  const bool vec_mask = p.epilogue == kEpiBf16Mask &&
+                        (reinterpret_cast<uintptr_t>(p.mask) & 15u) == 0 &&
+                        (size_t(p.ldc) * 2) % 16 == 0;
   for (int col = 0; col < NT; col += 32) {
     uint32_t r[32];
     const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + uint32_t(col);
@@ -252,21 +278,66 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmParams p) 
         : "r"(taddr)
         : "memory");
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    if (row >= p.M) continue;
+    // The group's biases (and masks) are read before any output is written,
+    // so that the reads are not serialised behind the stores.
+    const int nb = n0 + col;
+    float v[32];
 #pragma unroll
-    for (int j = 0; j < 32; ++j) {
-      const int n = n0 + col + j;
-      if (n >= p.N) break;
-      float v = __uint_as_float(r[j]);
-      if (p.bias) v += p.bias[n];
-      const size_t o = size_t(row) * p.ldc + n;
-      if (p.epilogue == kEpiF32) {
-        static_cast<float*>(p.c)[o] = v;
-      } else if (p.epilogue == kEpiBf16Relu) {
-        static_cast<uint16_t*>(p.c)[o] = ToBf16(fmaxf(v, 0.f));
+    for (int j = 0; j < 32; ++j)
+      v[j] = __uint_as_float(r[j]) + (p.bias && nb + j < p.N ? __ldg(p.bias + nb + j) : 0.f);
+    if (row >= p.M) continue;
+    const size_t o0 = size_t(row) * p.ldc + nb;
+    const bool full = vec_out && nb + 32 <= p.N;
+    if (p.epilogue == kEpiF32) {
+      float* out = static_cast<float*>(p.c) + o0;
+      if (full) {
+#pragma unroll
+        for (int j = 0; j < 32; j += 4)
+          *reinterpret_cast<float4*>(out + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
       } else {
-        static_cast<uint16_t*>(p.c)[o] = ToBf16(FromBf16(p.mask[o]) > 0.f ? v : 0.f);
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          if (nb + j < p.N) out[j] = v[j];
       }
+      continue;
+    }
+    if (p.epilogue == kEpiBf16Mask) {  // v = 0 where the mask (ReLU output) is not > 0
+      const uint16_t* mk = p.mask + o0;
+      if (vec_mask && nb + 32 <= p.N) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const uint4 mv = __ldg(reinterpret_cast<const uint4*>(mk) + q);
+          const uint32_t w[4] = {mv.x, mv.y, mv.z, mv.w};
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const uint16_t m = uint16_t(w[e >> 1] >> (16 * (e & 1)));
+            if (!(FromBf16(m) > 0.f)) v[q * 8 + e] = 0.f;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          if (!(nb + j < p.N && FromBf16(mk[j]) > 0.f)) v[j] = 0.f;
+      }
+    } else {  // kEpiBf16Relu
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = fmaxf(v[j], 0.f);
+    }
+    uint16_t* out = static_cast<uint16_t*>(p.c) + o0;
+    if (full) {
+#pragma unroll
+      for (int j = 0; j < 32; j += 8) {
+        uint4 w;
+        w.x = uint32_t(ToBf16(v[j + 0])) | (uint32_t(ToBf16(v[j + 1])) << 16);
+        w.y = uint32_t(ToBf16(v[j + 2])) | (uint32_t(ToBf16(v[j + 3])) << 16);
+        w.z = uint32_t(ToBf16(v[j + 4])) | (uint32_t(ToBf16(v[j + 5])) << 16);
+        w.w = uint32_t(ToBf16(v[j + 6])) | (uint32_t(ToBf16(v[j + 7])) << 16);
+        *reinterpret_cast<uint4*>(out + j) = w;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (nb + j < p.N) out[j] = ToBf16(v[j]);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
