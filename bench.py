@@ -510,7 +510,8 @@ def run_batch(args):
                 "d2h_bytes_per_step": int(sols.nbytes)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                     "kernel": "stream_kernel", "kernel_ms": kernel_ms,
+                     "kernel": "stream_kernel" if tuning.get("use_pipe") == 0 else "pipe_kernel",
+                     "kernel_ms": kernel_ms,
                      "algorithmic_bytes_per_launch": alg_bytes},
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),

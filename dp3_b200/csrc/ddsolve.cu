@@ -856,7 +856,23 @@ struct PipeParams {
   double* step_magnitudes;
   cudaGraphConditionalHandle handle;
   int32_t use_handle;
+  // Independent intervals (batched solve): interval g owns channel blocks
+  // [group_cb[g], group_cb[g + 1]) (cb_group[cb] = g), its loop state
+  // state[g], step magnitudes step_magnitudes[g * mags_stride] and norm
+  // partials block_sum[g * gridDim.x + CTA]. One interval: n_groups = 1.
+  uint32_t n_groups;
+  const uint32_t* cb_group;
+  const uint32_t* group_cb;
+  uint32_t mags_stride;
 };
+
+// A fragment of an interval that has stopped: skipped by the producer and the
+// consumers alike (the loop states do not change during a launch).
+__device__ __forceinline__ bool FragFrozen(const PipeParams& p, uint32_t slab) {
+  if (p.n_groups <= 1 || p.host_mode) return false;
+  const uint32_t g = p.cb_group[p.slabs[slab].cb];
+  return static_cast<volatile const LoopState*>(p.state)[g].done != 0;
+}
 
 __device__ __forceinline__ uint32_t SmemAddr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -1130,101 +1146,115 @@ __device__ __forceinline__ void FinalizeDistributed(const PipeParams& p, int cti
   // solution reads are issued together and their partial slots merged in
   // rounds, so that the chains of dependent L2 reads of the items overlap
   // (each item's slots are still added in slot order).
-  constexpr int kFinBatch = 4;
-  const uint32_t item_step = gridDim.x * kPipeRuns;
-  for (uint32_t item0 = blockIdx.x * kPipeRuns + ctid; item0 < n_items;
-       item0 += kFinBatch * item_step) {
-    uint32_t cbv[kFinBatch], antv[kFinBatch], sv[kFinBatch], dv[kFinBatch];
-    uint32_t j0v[kFinBatch], j1v[kFinBatch], v0v[kFinBatch];
-    double2 oldv[kFinBatch][NPOL];
-#pragma unroll
-    for (int b = 0; b < kFinBatch; ++b) {
-      const uint32_t item = item0 + b * item_step;
-      cbv[b] = antv[b] = sv[b] = dv[b] = 0;
-      j0v[b] = j1v[b] = v0v[b] = 0;
-#pragma unroll
-      for (int q = 0; q < NPOL; ++q) oldv[b][q] = make_double2(0.0, 0.0);
-      if (item < n_items) {
-        const uint32_t cb = item / n_items_cb;
-        const uint32_t it = item - cb * n_items_cb;
-        const uint32_t ant = it / p.n_sub;
-        const uint32_t s = it - ant * p.n_sub;
-        cbv[b] = cb;
-        antv[b] = ant;
-        sv[b] = s;
-        dv[b] = p.dir_of_sub[s];
-        j0v[b] = p.fin_off[cb * p.n_sub + s];
-        j1v[b] = p.fin_off[cb * p.n_sub + s + 1];
-        if (p.fin_first) v0v[b] = p.fin_first[cb * p.n_sub + s];
-        const double2* sol = p.solutions + size_t(item) * NPOL;
-#pragma unroll
-        for (int q = 0; q < NPOL; ++q) oldv[b][q] = sol[q];
-      }
-    }
-    uint32_t n_rounds = 0;
-#pragma unroll
-    for (int b = 0; b < kFinBatch; ++b) n_rounds = max(n_rounds, j1v[b] - j0v[b]);
-    NeumaierSum nr[kFinBatch][NPOL], ni[kFinBatch][NPOL], dn[kFinBatch][NPOL];
-    constexpr int kR = 4;  // slots per item and round
-    for (uint32_t k = 0; k < n_rounds; k += kR) {
-      uint32_t vis[kFinBatch][kR];
-#pragma unroll
-      for (int b = 0; b < kFinBatch; ++b)
-#pragma unroll
-        for (int u = 0; u < kR; ++u)
-          vis[b][u] = j0v[b] + k + u >= j1v[b] ? 0xFFFFFFFFu
-                      : p.fin_first            ? v0v[b] + k + u
-                                               : p.fin_visits[j0v[b] + k + u];
-      float v[kFinBatch][kR][NPOL * 3];
-#pragma unroll
+  // Interval by interval (one round for a single interval): its items spread
+  // over all CTAs, its norm partial per CTA. An interval that has stopped
+  // keeps its solutions.
+  for (uint32_t g = 0; g < p.n_groups; ++g) {
+    nsum = 0.0;
+    ncnt = 0;
+    const bool frozen = p.n_groups > 1 && !p.host_mode &&
+                        static_cast<volatile const LoopState*>(p.state)[g].done != 0;
+    const uint32_t i_lo = p.n_groups > 1 ? p.group_cb[g] * n_items_cb : 0u;
+    const uint32_t i_hi = frozen ? i_lo : p.n_groups > 1 ? p.group_cb[g + 1] * n_items_cb : n_items;
+    constexpr int kFinBatch = 4;
+    const uint32_t item_step = gridDim.x * kPipeRuns;
+    for (uint32_t item0 = i_lo + blockIdx.x * kPipeRuns + ctid; item0 < i_hi;
+         item0 += kFinBatch * item_step) {
+      uint32_t cbv[kFinBatch], antv[kFinBatch], sv[kFinBatch], dv[kFinBatch];
+      uint32_t j0v[kFinBatch], j1v[kFinBatch], v0v[kFinBatch];
+      double2 oldv[kFinBatch][NPOL];
+  #pragma unroll
       for (int b = 0; b < kFinBatch; ++b) {
-        // the item's numerators and denominators in a partial slot (AccAdd)
-        const size_t off_n = size_t(antv[b]) * p.acc_stride + AccNumOffset(NPOL, dv[b], 0);
-        const size_t off_d =
-            size_t(antv[b]) * p.acc_stride + AccDenOffset(NPOL, p.n_dir, dv[b], 0);
-#pragma unroll
-        for (int u = 0; u < kR; ++u) {
-          if (vis[b][u] == 0xFFFFFFFFu) continue;
-          const float* a = p.partials + size_t(vis[b][u]) * p.acc_floats;
-#pragma unroll
-          for (int e = 0; e < NPOL * 2; ++e) v[b][u][e] = __ldcg(a + off_n + e);
-#pragma unroll
-          for (int q = 0; q < NPOL; ++q) v[b][u][NPOL * 2 + q] = __ldcg(a + off_d + q);
+        const uint32_t item = item0 + b * item_step;
+        cbv[b] = antv[b] = sv[b] = dv[b] = 0;
+        j0v[b] = j1v[b] = v0v[b] = 0;
+  #pragma unroll
+        for (int q = 0; q < NPOL; ++q) oldv[b][q] = make_double2(0.0, 0.0);
+        if (item < i_hi) {
+          const uint32_t cb = item / n_items_cb;
+          const uint32_t it = item - cb * n_items_cb;
+          const uint32_t ant = it / p.n_sub;
+          const uint32_t s = it - ant * p.n_sub;
+          cbv[b] = cb;
+          antv[b] = ant;
+          sv[b] = s;
+          dv[b] = p.dir_of_sub[s];
+          j0v[b] = p.fin_off[cb * p.n_sub + s];
+          j1v[b] = p.fin_off[cb * p.n_sub + s + 1];
+          if (p.fin_first) v0v[b] = p.fin_first[cb * p.n_sub + s];
+          const double2* sol = p.solutions + size_t(item) * NPOL;
+  #pragma unroll
+          for (int q = 0; q < NPOL; ++q) oldv[b][q] = sol[q];
         }
       }
-#pragma unroll
-      for (int b = 0; b < kFinBatch; ++b)
-#pragma unroll
-        for (int u = 0; u < kR; ++u) {
-          if (vis[b][u] == 0xFFFFFFFFu) continue;
-#pragma unroll
-          for (int q = 0; q < NPOL; ++q) {
-            nr[b][q].Add(v[b][u][q * 2 + 0]);
-            ni[b][q].Add(v[b][u][q * 2 + 1]);
-            dn[b][q].Add(v[b][u][NPOL * 2 + q]);
+      uint32_t n_rounds = 0;
+  #pragma unroll
+      for (int b = 0; b < kFinBatch; ++b) n_rounds = max(n_rounds, j1v[b] - j0v[b]);
+      NeumaierSum nr[kFinBatch][NPOL], ni[kFinBatch][NPOL], dn[kFinBatch][NPOL];
+      constexpr int kR = 4;  // slots per item and round
+      for (uint32_t k = 0; k < n_rounds; k += kR) {
+        uint32_t vis[kFinBatch][kR];
+  #pragma unroll
+        for (int b = 0; b < kFinBatch; ++b)
+  #pragma unroll
+          for (int u = 0; u < kR; ++u)
+            vis[b][u] = j0v[b] + k + u >= j1v[b] ? 0xFFFFFFFFu
+                        : p.fin_first            ? v0v[b] + k + u
+                                                 : p.fin_visits[j0v[b] + k + u];
+        float v[kFinBatch][kR][NPOL * 3];
+  #pragma unroll
+        for (int b = 0; b < kFinBatch; ++b) {
+          // the item's numerators and denominators in a partial slot (AccAdd)
+          const size_t off_n = size_t(antv[b]) * p.acc_stride + AccNumOffset(NPOL, dv[b], 0);
+          const size_t off_d =
+              size_t(antv[b]) * p.acc_stride + AccDenOffset(NPOL, p.n_dir, dv[b], 0);
+  #pragma unroll
+          for (int u = 0; u < kR; ++u) {
+            if (vis[b][u] == 0xFFFFFFFFu) continue;
+            const float* a = p.partials + size_t(vis[b][u]) * p.acc_floats;
+  #pragma unroll
+            for (int e = 0; e < NPOL * 2; ++e) v[b][u][e] = __ldcg(a + off_n + e);
+  #pragma unroll
+            for (int q = 0; q < NPOL; ++q) v[b][u][NPOL * 2 + q] = __ldcg(a + off_d + q);
           }
         }
+  #pragma unroll
+        for (int b = 0; b < kFinBatch; ++b)
+  #pragma unroll
+          for (int u = 0; u < kR; ++u) {
+            if (vis[b][u] == 0xFFFFFFFFu) continue;
+  #pragma unroll
+            for (int q = 0; q < NPOL; ++q) {
+              nr[b][q].Add(v[b][u][q * 2 + 0]);
+              ni[b][q].Add(v[b][u][q * 2 + 1]);
+              dn[b][q].Add(v[b][u][NPOL * 2 + q]);
+            }
+          }
+      }
+  #pragma unroll
+      for (int b = 0; b < kFinBatch; ++b) {
+        const uint32_t item = item0 + b * item_step;
+        if (item < i_hi) finish(item, cbv[b], antv[b], sv[b], oldv[b], nr[b], ni[b], dn[b]);
+      }
     }
-#pragma unroll
-    for (int b = 0; b < kFinBatch; ++b) {
-      const uint32_t item = item0 + b * item_step;
-      if (item < n_items) finish(item, cbv[b], antv[b], sv[b], oldv[b], nr[b], ni[b], dn[b]);
-    }
-  }
-  // Per-CTA norm partial, then the last CTA finishes the iteration.
-  s_sum[ctid] = nsum;
-  s_cnt[ctid] = ncnt;
-  ConsumerBarrier();
-  for (int w = 128; w > 0; w >>= 1) {
-    if (ctid < w && ctid + w < kPipeRuns) {
-      s_sum[ctid] += s_sum[ctid + w];
-      s_cnt[ctid] += s_cnt[ctid + w];
-    }
+    s_sum[ctid] = nsum;
+    s_cnt[ctid] = ncnt;
     ConsumerBarrier();
+    for (int w = 128; w > 0; w >>= 1) {
+      if (ctid < w && ctid + w < kPipeRuns) {
+        s_sum[ctid] += s_sum[ctid + w];
+        s_cnt[ctid] += s_cnt[ctid + w];
+      }
+      ConsumerBarrier();
+    }
+    if (ctid == 0) {
+      p.block_sum[size_t(g) * gridDim.x + blockIdx.x] = s_sum[0];
+      p.block_cnt[size_t(g) * gridDim.x + blockIdx.x] = s_cnt[0];
+    }
+    ConsumerBarrier();  // s_sum is reused by the next interval
   }
+  // The last CTA finishes the iteration.
   if (ctid == 0) {
-    p.block_sum[blockIdx.x] = s_sum[0];
-    p.block_cnt[blockIdx.x] = s_cnt[0];
     __threadfence();
     const uint32_t prev = atomicAdd(&p.counters[0], 1u);
     *s_last = (prev == gridDim.x - 1) ? 1u : 0u;
@@ -1306,6 +1336,38 @@ __device__ __forceinline__ void FinalizeDistributed(const PipeParams& p, int cti
       }
       ConsumerBarrier();
     }
+  }
+  if (p.n_groups > 1 && !p.host_mode) {
+    // Several intervals: one thread per interval still going sums its norm
+    // partials in CTA order and runs its control step; the loop goes on while
+    // any interval does.
+    ConsumerBarrier();  // every thread has read *s_last
+    if (ctid == 0) *s_last = 0u;
+    ConsumerBarrier();
+    const bool error = reinterpret_cast<volatile uint32_t*>(p.counters)[1] != 0;
+    for (uint32_t g = ctid; g < p.n_groups; g += kPipeRuns) {
+      LoopState& ls = p.state[g];
+      if (ls.done) continue;
+      double sum = 0.0;
+      uint64_t cnt = 0;
+      for (uint32_t b = 0; b < gridDim.x; ++b) {
+        sum += reinterpret_cast<volatile double*>(p.block_sum)[size_t(g) * gridDim.x + b];
+        cnt += reinterpret_cast<volatile uint32_t*>(p.block_cnt)[size_t(g) * gridDim.x + b];
+      }
+      bool stop = ControlStep(ls, st, sum, cnt, p.step_magnitudes + size_t(g) * p.mags_stride);
+      if (error) {
+        ls.done = 1;
+        stop = true;
+      }
+      if (!stop) atomicOr(s_last, 1u);
+    }
+    ConsumerBarrier();
+    if (ctid == 0) {
+      p.counters[0] = 0;
+      p.counters[2] = 0;
+      if (p.use_handle) cudaGraphSetConditional(p.handle, *s_last ? 1u : 0u);
+    }
+    return;
   }
   // The per-CTA norm partials, summed by all consumer threads of the last CTA
   // in a fixed tree order (a serial sum by one thread sat on the critical
@@ -1443,8 +1505,12 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
   constexpr int RUNS = kPipeRuns / NG;  // runs per tile
   // An unrolled graph body launches the kernel more than once per loop test:
   // a launch after the loop has stopped does nothing.
-  if (!p.host_mode && p.use_handle && static_cast<volatile const LoopState*>(p.state)->done)
-    return;
+  if (!p.host_mode && p.use_handle) {
+    bool all_done = true;
+    for (uint32_t g = 0; g < p.n_groups && all_done; ++g)
+      all_done = static_cast<volatile const LoopState*>(p.state)[g].done != 0;
+    if (all_done) return;
+  }
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + kPipeMaxStages;
@@ -1504,6 +1570,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
     bool ok = true;
     for (uint32_t fi = f_begin; fi < f_end && ok; ++fi) {
       const Frag f = p.frags[fi];
+      if (FragFrozen(p, f.slab)) continue;
       const SlabDesc sl = p.slabs[f.slab];
       if (f.visit != cur_visit) {  // new visit: its gain table first
         const uint32_t b = nvis % p.n_gbuf;
@@ -1601,6 +1668,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
   for (uint32_t fi = f_begin; fi < f_end; ++fi) {
     const Frag f = nf;
     if (fi + 1 < f_end) nf = p.frags[fi + 1];
+    if (FragFrozen(p, f.slab)) continue;
     if (f.visit != cur_visit) {
       if (cur_visit != 0xFFFFFFFFu) end_visit();
       for (uint32_t i = ctid; i < acc_n; i += kPipeRuns) acc[i] = 0.f;
@@ -2139,6 +2207,7 @@ struct ddsolve_ctx {
   std::vector<uint32_t> group_first_cb;
   uint32_t mags_stride = 1;
   DevBuf d_block_group, d_block_item0, d_block_item_end, d_group_blocks, d_cb_group;
+  DevBuf d_group_cb;  // pipe plan: first channel block of each interval, and n_cb
   // graph
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -2715,8 +2784,20 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
                                       ctx->stream));
   DDS_CHECK_CUDA(ctx, ctx->d_partials.Reserve(
                           std::max<size_t>(1, size_t(n_visits) * n_ant * ctx->acc_stride) * 4));
-  DDS_CHECK_CUDA(ctx, ctx->d_block_sum.Reserve(size_t(std::max(n_ctas, ctx->fin_blocks)) * 8));
-  DDS_CHECK_CUDA(ctx, ctx->d_block_cnt.Reserve(size_t(std::max(n_ctas, ctx->fin_blocks)) * 4));
+  // norm partials per (interval, CTA)
+  {
+    const size_t n_part = std::max<size_t>(size_t(n_ctas) * ctx->n_groups, ctx->fin_blocks);
+    DDS_CHECK_CUDA(ctx, ctx->d_block_sum.Reserve(n_part * 8));
+    DDS_CHECK_CUDA(ctx, ctx->d_block_cnt.Reserve(n_part * 4));
+    std::vector<uint32_t> cb_group(ctx->n_cb, 0), group_cb(ctx->n_groups + 1, 0);
+    for (uint32_t g = 0; g < ctx->n_groups; ++g) {
+      group_cb[g] = ctx->n_groups == 1 ? 0u : ctx->group_first_cb[g];
+      group_cb[g + 1] = ctx->n_groups == 1 ? ctx->n_cb : ctx->group_first_cb[g + 1];
+      for (uint32_t cb = group_cb[g]; cb < group_cb[g + 1]; ++cb) cb_group[cb] = g;
+    }
+    if ((rc = upload(ctx->d_cb_group, cb_group.data(), cb_group.size() * 4))) return rc;
+    if ((rc = upload(ctx->d_group_cb, group_cb.data(), group_cb.size() * 4))) return rc;
+  }
   DDS_CHECK_CUDA(ctx, ctx->d_cb_done.Reserve(size_t(ctx->n_cb) * 4));
   DDS_CHECK_CUDA(ctx, ctx->d_cb_flag.Reserve(size_t(ctx->n_cb) * 4));
   DDS_CHECK_CUDA(ctx, ctx->d_cb_avg.Reserve(size_t(ctx->n_cb) * 8));
@@ -2745,7 +2826,7 @@ int BuildPlanImpl(ddsolve_ctx* ctx, bool allow_pipe) {
   // shared memory allow it (and no lane groups were requested).
   ctx->use_pipe = false;
   ctx->pipe_ng = 1;
-  if (allow_pipe && ctx->tune_ng == 0 && ctx->tune_pipe != 0 && ctx->n_groups == 1 &&
+  if (allow_pipe && ctx->tune_ng == 0 && ctx->tune_pipe != 0 &&
       (ctx->n_corr == 2 || ctx->n_corr == 4) && !std::getenv("DDSOLVE_NO_PIPE")) {
     const KernelEntry* pe =
         FindPipeKernel(int(ctx->n_corr), int(ctx->n_pol), int(ctx->n_dir));
@@ -3073,6 +3154,10 @@ PipeParams MakePipeParams(ddsolve_ctx* ctx, bool host_mode, bool use_handle) {
   p.fin_off = ctx->d_fin_off.as<uint32_t>();
   p.fin_visits = ctx->d_fin_visits.as<uint32_t>();
   p.fin_first = ctx->fin_ranges ? ctx->d_fin_first.as<uint32_t>() : nullptr;
+  p.n_groups = ctx->n_groups;
+  p.cb_group = ctx->d_cb_group.as<uint32_t>();
+  p.group_cb = ctx->d_group_cb.as<uint32_t>();
+  p.mags_stride = ctx->mags_stride;
   p.dir_of_sub = ctx->d_dir_of_sub.as<uint32_t>();
   p.cb_flag = ctx->d_cb_flag.as<uint32_t>();
   p.cb_avg = ctx->d_cb_avg.as<double>();

@@ -406,11 +406,14 @@ def test_autotune_keeps_results_and_caches(built):
         c.close()
 
 
-def test_batched_intervals_match_separate_solves(built):
+@pytest.mark.parametrize("use_pipe", [-1, 0])
+def test_batched_intervals_match_separate_solves(built, use_pipe):
     """Three independent intervals in one context (ddsolve_set_intervals /
     ddsolve_solve_batch) give each interval the iteration count and the
     solutions of its own solve: intervals stop at different iterations and a
-    stopped interval keeps its solutions while the others go on."""
+    stopped interval keeps its solutions while the others go on. Default plan
+    (pipe_kernel, per-interval control in its fused finalisation) and the
+    stream_kernel plan."""
     from dp3_b200 import ddsolve
     obs_list = [synth.observe(synth.small_config(n_stations=12, n_directions=3, n_channels=8,
                                                  n_cb=2, n_times=2, seed=seed))
@@ -435,6 +438,7 @@ def test_batched_intervals_match_separate_solves(built):
     ctx = ddsolve.Context(cfg.n_stations, cfg.nspd, 3 * n_cb, 2, 2)
     ctx.set_settings(st)
     ctx.set_intervals([0, n_cb, 2 * n_cb, 3 * n_cb])
+    ctx.set_plan_tuning(use_pipe=use_pipe)
     for g, obs in enumerate(obs_list):
         for cb, nc in enumerate(cfg.cb_channels):
             ctx.set_channel_block_regular(g * n_cb + cb, cfg.n_times, cfg.n_baselines, nc,
@@ -443,6 +447,13 @@ def test_batched_intervals_match_separate_solves(built):
     sol = np.ones((3 * n_cb, cfg.n_stations, n_sub, 2), np.complex128)
     mags = np.zeros((3, 150))
     res = ctx.solve_batch(sol, mags)
+    # which path ran: one pipe_kernel per iteration (plus make-finite, gain
+    # tables and model powers once per solve), or three kernels per iteration
+    max_it = max(r.iterations for r in res)
+    if use_pipe == -1:
+        assert ctx.last_launch_count() <= max_it + 3, (ctx.last_launch_count(), max_it)
+    else:
+        assert ctx.last_launch_count() >= 3 * (max_it - 1), (ctx.last_launch_count(), max_it)
     with pytest.raises(RuntimeError):
         ctx.solve(np.ones_like(sol))
     ctx.close()
