@@ -789,21 +789,23 @@ __global__ void __launch_bounds__(kThreads) finalize_kernel(const FinParams p) {
 
 
 // ---------------------------------------------------------------------------
-// pipe_kernel: the Blackwell streaming path. Per CTA one producer warp moves
-// the (time, channel) rows of each tile (224 runs) from HBM into a ring of
-// shared-memory stages with 1-D bulk copies (cp.async.bulk, completion on an
-// mbarrier, no multicast); seven consumer warps (one run per lane) compute
-// the residual and the per-direction P/Q sums from shared memory. Runs are
-// stored in baseline-diagonal order, so within a warp the 32 first antennas
-// are distinct and so are the 32 second antennas: every shared-memory atomic
-// of the antenna reduction is conflict-free and no warp shuffles are needed.
-// The accumulator and gain tables use an odd per-antenna stride, so the 32
-// lanes of one atomic hit 32 different banks.
+// pipe_kernel: the Blackwell streaming path. Per CTA one producer thread
+// moves the (time, channel) rows of each tile from HBM into a ring of
+// shared-memory stages, one 1-D bulk copy per row (cp.async.bulk, completion
+// on an mbarrier, no multicast; the tile-packed slab layout makes a row of a
+// tile, data and every direction, contiguous). Seven consumer warps compute
+// the residual and the per-direction P/Q sums from shared memory, one lane per
+// run (or four lanes per run for 13-48 directions), and reduce each tile into
+// the CTA's shared-memory antenna accumulators in barrier-separated phases
+// over groups of runs with distinct antennas (runs are stored in
+// cyclic-diagonal order), or by a counting sort where a tile has no such
+// grouping. No shared-memory float atomics.
 //
-// The finalisation is fused: the CTA that flushes the last partial slot of a
-// channel block finalises that block (merge, FP64 update, step, norm,
-// non-finite detection for the lazy MakeSolutionsFinite), and the CTA that
-// finalises the last channel block runs the iteration control. One launch per
+// The finalisation is fused: after a grid-wide arrival count, every CTA
+// finalises a slice of the (channel block, antenna, sub-solution) items (merge
+// of the partial slots, FP64 update, step, norm, non-finite detection for the
+// lazy MakeSolutionsFinite), interval by interval, and the last CTA to finish
+// runs the iteration control of every interval still going. One launch per
 // iteration. Every wait is bounded by a 4 s device timer; a timeout sets an
 // error flag that the host reports as DDSOLVE_E_TIMEOUT, and all later waits
 // of that CTA return at once so that the kernel still ends.
@@ -1034,12 +1036,13 @@ __device__ __forceinline__ void WriteTables(const PipeParams& p, uint32_t cb,
 
 // Grid-wide finalisation of pipe_kernel, after the grid barrier: the
 // consumer threads of all CTAs take (channel block, antenna, sub-solution)
-// items in a grid-stride loop: fixed-order compensated merge of the item's
+// items in a grid-stride loop, one round per independent interval (one round
+// for a single interval): fixed-order compensated merge of the item's
 // partial slots, FP64 add-back and division (IterativeDiagonalSolver.cc:206-221,
 // IterativeScalarSolver.cc:184-194), SolverBase::Step (SolverBase.cc:88-158),
 // the AssignSolutions norm (SolverBase.cc:234-285), and the FP32 gain tables
-// of the next iteration. The last CTA to finish sums the per-CTA norms in CTA
-// order, runs ReachedStoppingCriterion / DetectStall (SolverBase.h:274-285,
+// of the next iteration. The last CTA to finish sums each interval's per-CTA
+// norms in CTA order, runs ReachedStoppingCriterion / DetectStall (SolverBase.h:274-285,
 // SolverBase.cc:63-86), and prepares the next iteration's
 // MakeSolutionsFinite{1,2}Pol (SolverBase.cc:316-371) for channel blocks that
 // got non-finite solutions.
@@ -1065,7 +1068,9 @@ __device__ __forceinline__ void FinalizeDistributed(const PipeParams& p, int cti
       old[q] = old_in[q];
       pair_ok = pair_ok && dfinite(old[q]);
     }
-    if (!pair_ok && p.cb_flag[cb]) {
+    // the lazy MakeSolutionsFinite of a solve (next-solutions passes use the
+    // solutions they are given, as PerformIteration does)
+    if (!pair_ok && !p.host_mode && p.cb_flag[cb]) {
       const double rv = p.cb_avg[cb];
 #pragma unroll
       for (int q = 0; q < NPOL; ++q) old[q] = make_double2(rv, 0.0);
@@ -3923,12 +3928,8 @@ int ddsolve_perform_iterations(ddsolve_ctx* ctx, const double* start, uint32_t n
     }
   } restore{ctx, ctx->d_sol.ptr, ctx->d_next.ptr};
   if (ctx->use_pipe) {
-    // Once per call: no replacement values from an earlier solve apply
-    // (next-solutions passes neither read nor write the new-non-finite flags,
-    // which every solve clears itself), and every pipe_kernel launch leaves
-    // its counters at zero.
-    DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_flag.ptr, 0, size_t(ctx->n_cb) * 4,
-                                        ctx->stream));
+    // Once per call (every pipe_kernel launch leaves its counters at zero;
+    // next-solutions passes use none of the solve's non-finite flags).
     DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_counters.ptr, 0, 16, ctx->stream));
   }
   if (dev_in) ctx->d_sol.ptr = const_cast<double*>(start);
