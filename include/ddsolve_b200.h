@@ -159,8 +159,9 @@ DDSOLVE_API int ddsolve_solve(ddsolve_ctx* ctx, double* solutions, ddsolve_resul
  * n_channel_blocks; NULL with n_intervals = 1 restores one interval). Every
  * interval has its own iteration count, convergence, stall detection and
  * stopping, exactly as if solved alone; one streaming pass per iteration
- * covers all intervals still iterating, and an interval that has stopped
- * keeps its solutions. Batched contexts run on the stream_kernel path. */
+ * covers all intervals still iterating (the data of intervals that have
+ * stopped is skipped on the pipelined path), and an interval that has stopped
+ * keeps its solutions. */
 DDSOLVE_API int ddsolve_set_intervals(ddsolve_ctx* ctx, uint32_t n_intervals,
                                       const uint32_t* first_channel_block);
 
@@ -192,7 +193,12 @@ DDSOLVE_API int ddsolve_perform_iteration(ddsolve_ctx* ctx, const double* soluti
  * (include/ddwarm_b200.h) uses these undamped passes as residual statistics
  * of the current interval. With `outputs` in device memory the call only
  * enqueues the passes on the context's stream (ddsolve_stream) and returns; a
- * bounded-wait failure then surfaces at the next call that waits. */
+ * bounded-wait failure then surfaces at the next call that waits. Device
+ * arrays on the context's GPU are used in place (the first pass reads `start`,
+ * every pass writes its slice of `outputs`, no staging copies) unless the two
+ * overlap; they must stay allocated and unmodified until the passes have run
+ * in stream order. Non-finite input solutions are used as given (no
+ * MakeSolutionsFinite, as in PerformIteration). */
 DDSOLVE_API int ddsolve_perform_iterations(ddsolve_ctx* ctx, const double* start,
                                            uint32_t n_passes, double* outputs);
 
