@@ -564,6 +564,10 @@ struct ddwarm_ctx {
   uint64_t adam_t = 0;
   // activations for up to `cap` rows
   uint32_t cap = 0;
+  // rows of xb whose padding columns (n_in..di) are known to be zero: every
+  // writer of xb either writes whole padded rows with zero padding (the row
+  // gathers) or the feature columns only (features_kernel)
+  uint32_t xb_zero_rows = 0;
   DevBuf xb, h1, h2, y, t, dy, dz2, dz1, partial, loss, error;
   DevBuf sets, start, x32;  // warm-start features / predictions
   // training data set
@@ -592,6 +596,7 @@ int Reserve(ddwarm_ctx* ctx, uint32_t rows) {
   if (rows <= ctx->cap) return 0;
   const uint32_t r = RoundUp(rows, kMTile);
   WARM_CHECK(ctx, ctx->xb.Reserve(size_t(r) * ctx->di * 2));
+  ctx->xb_zero_rows = 0;  // new memory
   WARM_CHECK(ctx, ctx->h1.Reserve(size_t(r) * ctx->dh * 2));
   WARM_CHECK(ctx, ctx->h2.Reserve(size_t(r) * ctx->dh * 2));
   WARM_CHECK(ctx, ctx->y.Reserve(size_t(r) * ctx->dout * 4));
@@ -1057,7 +1062,10 @@ int ddwarm_predict_start(ddwarm_ctx* ctx, const ddwarm_layout* lay, uint32_t n_s
   if ((rc = Reserve(ctx, rows))) return rc;
   SetPtrs sp{};
   if ((rc = ResolveSets(ctx, lay, n_sets, sets, &sp, &n_sol))) return rc;
-  WARM_CHECK(ctx, cudaMemsetAsync(ctx->xb.ptr, 0, size_t(rows) * ctx->di * 2, ctx->stream));
+  if (rows > ctx->xb_zero_rows) {  // zero padding once per allocation
+    WARM_CHECK(ctx, cudaMemsetAsync(ctx->xb.ptr, 0, size_t(rows) * ctx->di * 2, ctx->stream));
+    ctx->xb_zero_rows = rows;
+  }
   features_kernel<<<256, 256, 0, ctx->stream>>>(sp, n_sets, lay->n_channel_blocks,
                                                 lay->n_antennas, lay->n_sub, lay->n_pol,
                                                 lay->scale, nullptr, ctx->xb.as<uint16_t>(),
