@@ -35,6 +35,8 @@ def built():
     """Builds the native libraries in-tree if they are missing or stale."""
     from dp3_b200 import build
     build.build_all()
-    from oracle import oracle_ffi
+    from oracle import oracle_ffi, ref_ffi
     oracle_ffi.build()
+    if ref_ffi.available():
+        ref_ffi.build()  # compiles only where the reference tree is present
     return True
