@@ -12,8 +12,10 @@ the inputs resident in HBM (CUDA events on the solver's stream, max over
 ranks, all ranks' intervals counted); `e2e` is the same metric through the
 public API with host (pinned) buffers, i.e. including the host-to-device
 upload of the interval and the device-to-host read of the solutions.
-`roofline` covers the streaming kernel, `cpu_baseline` the CPU oracle (the
-restated reference algorithm with its FP32 arithmetic) on the host cores.
+`roofline` covers the streaming kernel, `cpu_baseline` the reference's own
+solver (DP3's solver sources compiled here, oracle/_ref) on the host cores;
+where those are absent or the interval has uneven channel blocks, the
+restated reference algorithm with its FP32 arithmetic (oracle/).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -162,10 +164,70 @@ def workload_name(cfg, config_index, npol):
             f"max {cfg.max_iterations} iterations")
 
 
+class ReferenceCpu:
+    """The reference's own solver (DP3's IterativeDiagonalSolver /
+    IterativeScalarSolver compiled from its sources, oracle/_ref) on the
+    benchmark interval, packed once through its SolveData constructor
+    (timed separately), with all host threads."""
+
+    def __init__(self, cfg, obs, npol):
+        from oracle import ref_ffi as rf
+        self.rf, self.cfg, self.npol = rf, cfg, npol
+        self.threads = os.cpu_count() or 1
+        self.prep = rf.Prepared(cfg, obs.antenna1, obs.antenna2, obs.data, obs.model, 2, npol)
+        self.packing_s = self.prep.seconds_packing
+        self._per_it = None
+
+    def _solve(self, n_it):
+        cfg = self.cfg
+        sol = np.ones((cfg.n_channel_blocks, cfg.n_stations, sum(cfg.nspd), self.npol),
+                      np.complex128)
+        st = self.rf.settings(max_iterations=n_it, accuracy=cfg.tolerance,
+                              step_size=cfg.step_size)
+        return self.prep.solve(sol, st, self.threads).seconds_solve
+
+    def sample(self, iterations_per_interval, budget_s):
+        """Solve time per interval, from a solve of as many iterations as fit
+        in budget_s (at most the interval's own count), scaled to the
+        interval's iteration count."""
+        if self._per_it is None:
+            self._per_it = self._solve(1)
+        n_it = int(max(1, min(iterations_per_interval, budget_s // max(self._per_it, 1e-6))))
+        per_it = self._solve(n_it) / n_it
+        return {"value": per_it * iterations_per_interval, "unit": "s/interval",
+                "cores": self.threads, "kind": "reference",
+                "packing_s": self.packing_s,
+                "sample": f"DP3's own solver (reference sources compiled here, all host "
+                          f"threads): {n_it} iterations of the benchmark interval "
+                          f"({per_it * 1e3:.1f} ms/iteration) scaled to "
+                          f"{iterations_per_interval} iterations; SolveData packing "
+                          f"{self.packing_s:.2f} s, not included"}
+
+    def close(self):
+        self.prep.close()
+
+
+def cpu_baseline(cfg, obs, iterations_per_interval, budget_s=20.0, npol=2):
+    """The reference's own solver when its compiled sources are present
+    (kind "reference"), else the restated oracle (kind "port")."""
+    from oracle import ref_ffi as rf
+    if rf.available() and cfg.n_channel_blocks and all(
+            nc == (cb + 1) * cfg.n_channels // cfg.n_channel_blocks
+            - cb * cfg.n_channels // cfg.n_channel_blocks
+            for cb, nc in enumerate(cfg.cb_channels)):
+        ref = ReferenceCpu(cfg, obs, npol)
+        try:
+            return ref.sample(iterations_per_interval, budget_s)
+        finally:
+            ref.close()
+    return cpu_baseline_port(cfg, obs, iterations_per_interval, budget_s, npol)
+
+
 def cpu_baseline_port(cfg, obs, iterations_per_interval, budget_s=20.0, npol=2):
     """Times the oracle (restated reference solver, FP32 arithmetic, all host
     threads) on a bounded sample: a few iterations of the same interval,
-    scaled to the GPU interval's iteration count."""
+    scaled to the GPU interval's iteration count. Used where the reference's
+    regular SolveData cannot express the interval (uneven channel blocks)."""
     from oracle import oracle_ffi as of
     ap, sm = obs.generic_arrays()
     prob = dict(n_antennas=cfg.n_stations, n_correlations=2, n_pol=npol,
@@ -398,15 +460,24 @@ def run_reference_arm(args):
     cfg = synth.benchmark_configs()[args.config]
     obs = synth.observe(cfg)
     from oracle import oracle_ffi as of
+    from oracle import ref_ffi as rf
     of.build()
     iters = cfg.max_iterations + 1  # the interval does not converge in 50
     times = []
     base = None
+    # the whole run within about three minutes of CPU work
+    budget = min(args.ref_budget, 180.0 / (args.warmup + args.steps))
+    ref = ReferenceCpu(cfg, obs, args.npol) if rf.available() else None
     for i in range(args.warmup + args.steps):
-        b = cpu_baseline_port(cfg, obs, iters, budget_s=args.ref_budget, npol=args.npol)
+        if ref is not None:
+            b = ref.sample(iters, budget)
+        else:
+            b = cpu_baseline_port(cfg, obs, iters, budget_s=budget, npol=args.npol)
         if i >= args.warmup:
             times.append(b["value"])
             base = b
+    if ref is not None:
+        ref.close()
     value = statistics.mean(times)
     line = {
         "impl": "reference", "metric": METRIC, "value": value,
@@ -713,8 +784,8 @@ def run_gpu_arm(args):
         from oracle import oracle_ffi as of
         of.build()
         obs_np = synth.observe(cfg)
-        result["cpu_baseline"] = cpu_baseline_port(cfg, obs_np, int(r.iterations),
-                                                   budget_s=args.ref_budget, npol=args.npol)
+        result["cpu_baseline"] = cpu_baseline(cfg, obs_np, int(r.iterations),
+                                              budget_s=args.ref_budget, npol=args.npol)
     if rank == 0:
         print(json.dumps(result), flush=True)
     ctx.close()

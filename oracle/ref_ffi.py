@@ -94,6 +94,16 @@ def lib():
                                 ctypes.c_uint32, ctypes.POINTER(Constraints), ctypes.c_void_p,
                                 ctypes.POINTER(Result)]
         L.ref_last_error.restype = ctypes.c_char_p
+        L.ref_prepare.restype = ctypes.c_int
+        L.ref_prepare.argtypes = [ctypes.POINTER(Problem), ctypes.c_int,
+                                  ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_double)]
+        L.ref_solve_prepared.restype = ctypes.c_int
+        L.ref_solve_prepared.argtypes = [ctypes.c_void_p, ctypes.POINTER(Problem),
+                                         ctypes.POINTER(Settings), ctypes.c_uint32,
+                                         ctypes.POINTER(Constraints), ctypes.c_void_p,
+                                         ctypes.POINTER(Result)]
+        L.ref_release.restype = None
+        L.ref_release.argtypes = [ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -110,24 +120,13 @@ def kind_of(ncorr, npol):
     return {1: SCALAR_UNI, 2: SCALAR_DUO, 4: SCALAR_FULL}[ncorr]
 
 
-def solve(cfg, antenna1, antenna2, data, model, ncorr, npol, solutions, st, n_threads=1,
-          antenna_sets=None, smoothness=None, cb_frequencies=None):
-    """Runs the reference's Solve on one regular interval.
-
-    cfg: an ObservationConfig-like object (n_stations, n_times, n_baselines,
-    n_channels, cb_channels, nspd). solutions: complex128 [n_cb, n_ant,
-    n_sub, npol], updated in place. antenna_sets: list of antenna-index
-    lists (AntennaConstraint); smoothness: dict(bandwidth_hz=...,
-    bandwidth_ref_frequency_hz=0, spectral_exponent=-1, kernel_truncation=True)
-    (SmoothnessConstraint); cb_frequencies: mean frequency per channel block
-    (needed with any constraint). Returns the Result (iterations,
-    constraint_iterations, seconds_packing, seconds_solve)."""
+def _problem(cfg, antenna1, antenna2, data, model, ncorr):
+    """Problem struct of one regular interval and the arrays it points to."""
     n_cb = len(cfg.cb_channels)
     n_ch = sum(cfg.cb_channels)
     for cb, nc in enumerate(cfg.cb_channels):
         if nc != (cb + 1) * n_ch // n_cb - cb * n_ch // n_cb:
             raise ValueError("channel blocks are not the reference's even split")
-    assert solutions.dtype == np.complex128 and solutions.flags.c_contiguous
     nspd = np.ascontiguousarray(cfg.nspd, np.uint32)
     a1 = np.ascontiguousarray(antenna1, np.int32)
     a2 = np.ascontiguousarray(antenna2, np.int32)
@@ -141,26 +140,47 @@ def solve(cfg, antenna1, antenna2, data, model, ncorr, npol, solutions, st, n_th
                 a2.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
                 ctypes.cast(dp, ctypes.POINTER(ctypes.c_void_p)),
                 ctypes.cast(mp, ctypes.POINTER(ctypes.c_void_p)))
-    cons = None
-    keep = []
-    if antenna_sets or smoothness:
-        freqs = np.ascontiguousarray(cb_frequencies, np.float64)
-        keep.append(freqs)
-        cons = Constraints()
-        cons.channel_block_frequencies = freqs.ctypes.data
-        if antenna_sets:
-            sizes = np.array([len(s) for s in antenna_sets], np.uint32)
-            members = np.concatenate([np.asarray(s, np.uint32) for s in antenna_sets])
-            keep += [sizes, members]
-            cons.n_antenna_sets = len(antenna_sets)
-            cons.antenna_set_sizes = sizes.ctypes.data
-            cons.antenna_set_members = members.ctypes.data
-        if smoothness:
-            cons.smoothness = 1
-            cons.bandwidth_hz = smoothness["bandwidth_hz"]
-            cons.bandwidth_ref_frequency_hz = smoothness.get("bandwidth_ref_frequency_hz", 0.0)
-            cons.spectral_exponent = smoothness.get("spectral_exponent", -1.0)
-            cons.kernel_truncation = int(smoothness.get("kernel_truncation", True))
+    return p, (nspd, a1, a2, data, model, dp, mp)
+
+
+def _constraints(antenna_sets, smoothness, cb_frequencies):
+    if not (antenna_sets or smoothness):
+        return None, ()
+    freqs = np.ascontiguousarray(cb_frequencies, np.float64)
+    keep = [freqs]
+    cons = Constraints()
+    cons.channel_block_frequencies = freqs.ctypes.data
+    if antenna_sets:
+        sizes = np.array([len(s) for s in antenna_sets], np.uint32)
+        members = np.concatenate([np.asarray(s, np.uint32) for s in antenna_sets])
+        keep += [sizes, members]
+        cons.n_antenna_sets = len(antenna_sets)
+        cons.antenna_set_sizes = sizes.ctypes.data
+        cons.antenna_set_members = members.ctypes.data
+    if smoothness:
+        cons.smoothness = 1
+        cons.bandwidth_hz = smoothness["bandwidth_hz"]
+        cons.bandwidth_ref_frequency_hz = smoothness.get("bandwidth_ref_frequency_hz", 0.0)
+        cons.spectral_exponent = smoothness.get("spectral_exponent", -1.0)
+        cons.kernel_truncation = int(smoothness.get("kernel_truncation", True))
+    return cons, keep
+
+
+def solve(cfg, antenna1, antenna2, data, model, ncorr, npol, solutions, st, n_threads=1,
+          antenna_sets=None, smoothness=None, cb_frequencies=None):
+    """Runs the reference's Solve on one regular interval.
+
+    cfg: an ObservationConfig-like object (n_stations, n_times, n_baselines,
+    cb_channels, nspd). solutions: complex128 [n_cb, n_ant, n_sub, npol],
+    updated in place. antenna_sets: list of antenna-index lists
+    (AntennaConstraint); smoothness: dict(bandwidth_hz=...,
+    bandwidth_ref_frequency_hz=0, spectral_exponent=-1, kernel_truncation=True)
+    (SmoothnessConstraint); cb_frequencies: mean frequency per channel block
+    (needed with any constraint). Returns the Result (iterations,
+    constraint_iterations, seconds_packing, seconds_solve)."""
+    assert solutions.dtype == np.complex128 and solutions.flags.c_contiguous
+    p, keep = _problem(cfg, antenna1, antenna2, data, model, ncorr)
+    cons, keep_c = _constraints(antenna_sets, smoothness, cb_frequencies)
     res = Result()
     rc = lib().ref_solve(ctypes.byref(p), ctypes.byref(st), kind_of(ncorr, npol), n_threads,
                          ctypes.byref(cons) if cons is not None else None,
@@ -168,6 +188,41 @@ def solve(cfg, antenna1, antenna2, data, model, ncorr, npol, solutions, st, n_th
     if rc != 0:
         raise RuntimeError("ref_solve: " + lib().ref_last_error().decode())
     return res
+
+
+class Prepared:
+    """One interval packed once through the reference's SolveData
+    constructor (seconds_packing), then solved with any settings."""
+
+    def __init__(self, cfg, antenna1, antenna2, data, model, ncorr, npol):
+        self._p, self._keep = _problem(cfg, antenna1, antenna2, data, model, ncorr)
+        self._h = ctypes.c_void_p()
+        t = ctypes.c_double()
+        rc = lib().ref_prepare(ctypes.byref(self._p), kind_of(ncorr, npol), ctypes.byref(self._h),
+                               ctypes.byref(t))
+        if rc != 0:
+            raise RuntimeError("ref_prepare: " + lib().ref_last_error().decode())
+        self.seconds_packing = t.value
+
+    def solve(self, solutions, st, n_threads=1):
+        assert solutions.dtype == np.complex128 and solutions.flags.c_contiguous
+        res = Result()
+        rc = lib().ref_solve_prepared(self._h, ctypes.byref(self._p), ctypes.byref(st),
+                                      n_threads, None, solutions.ctypes.data, ctypes.byref(res))
+        if rc != 0:
+            raise RuntimeError("ref_solve_prepared: " + lib().ref_last_error().decode())
+        return res
+
+    def close(self):
+        if self._h:
+            lib().ref_release(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def perform_iteration(cfg, antenna1, antenna2, data, model, ncorr, npol, solutions,

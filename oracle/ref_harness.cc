@@ -15,23 +15,15 @@
 // direction-dependent solution indices), sets up the solver the way DDECal's
 // SolverFactory does (SolverFactory.cc:49-146: Initialize, the setters,
 // AddConstraint + Constraint::Initialize) and calls Solve(data, solutions,
-// time) (SolverBase.h:205-227).
-#include <algorithm>
+// time) (SolverBase.h:205-227). The shared steps are in ref_problem.h.
 #include <chrono>
-#include <cstdint>
-#include <cstring>
-#include <memory>
-#include <set>
 #include <stdexcept>
 #include <string>
-#include <vector>
 
-#include "ddecal/constraints/AntennaConstraint.h"
-#include "ddecal/constraints/SmoothnessConstraint.h"
 #include "ddecal/gain_solvers/IterativeDiagonalSolver.h"
 #include "ddecal/gain_solvers/IterativeScalarSolver.h"
-#include "ddecal/gain_solvers/SolveData.h"
 #include "ddecal/linear_solvers/LLSSolver.h"
+#include "ref_problem.h"
 
 namespace dp3::ddecal {
 // SolverBase.cc references LLSSolver::Make (CreateLLSSolver, used only by
@@ -42,185 +34,29 @@ std::unique_ptr<LLSSolver> LLSSolver::Make(LLSSolverType, int, int, int) {
 }
 }  // namespace dp3::ddecal
 
-namespace {
-
-using dp3::base::DPBuffer;
-using dp3::ddecal::SolverBase;
-using DComplex = std::complex<double>;
-
-thread_local std::string g_error;
-
-}  // namespace
-
-extern "C" {
-
-enum {
-  REF_DIAGONAL_DUO = 0,   // IterativeDiagonalSolver<MC2x2FDiag>
-  REF_DIAGONAL_FULL = 1,  // IterativeDiagonalSolver<MC2x2F>
-  REF_SCALAR_UNI = 2,     // IterativeScalarSolver<std::complex<float>>
-  REF_SCALAR_DUO = 3,     // IterativeScalarSolver<MC2x2FDiag>
-  REF_SCALAR_FULL = 4,    // IterativeScalarSolver<MC2x2F>
-};
-
-typedef struct {
-  uint32_t n_antennas, n_times, n_baselines, n_channels, n_channel_blocks, n_directions;
-  uint32_t n_correlations_in;                 // 1, 2 (XX, YY) or 4 per input visibility
-  const uint32_t* n_solutions_per_direction;  // [n_directions]
-  const int32_t* antenna1;                    // [n_baselines]
-  const int32_t* antenna2;
-  // Per channel block cb (channels [cb n_ch / n_cb, (cb + 1) n_ch / n_cb)):
-  //   data[cb]  float [n_times][n_baselines][n_ch_cb][n_correlations_in][2]
-  //   model[cb] float [n_directions][n_times][n_baselines][n_ch_cb][n_corr_in][2]
-  const float* const* data;
-  const float* const* model;
-} ref_problem;
-
-typedef struct {
-  uint32_t max_iterations;
-  uint32_t min_iterations;
-  double accuracy;
-  double constraint_accuracy;
-  double step_size;
-  int32_t detect_stalling;
-  double step_diff_sigma;
-  int32_t phase_only;
-} ref_settings;
-
-typedef struct {
-  // AntennaConstraint: n_antenna_sets sets, set k has antenna_set_sizes[k]
-  // members, listed consecutively in antenna_set_members.
-  uint32_t n_antenna_sets;
-  const uint32_t* antenna_set_sizes;
-  const uint32_t* antenna_set_members;
-  // SmoothnessConstraint (when smoothness != 0).
-  int32_t smoothness;
-  double bandwidth_hz;
-  double bandwidth_ref_frequency_hz;
-  double spectral_exponent;
-  int32_t kernel_truncation;
-  const double* smoothness_weights;  // [n_antennas * n_channel_blocks] or NULL (all 1)
-  // Mean frequency of each channel block (Constraint::Initialize).
-  const double* channel_block_frequencies;  // [n_channel_blocks]
-} ref_constraints;
-
-typedef struct {
-  uint32_t iterations;
-  uint32_t constraint_iterations;
-  double seconds_packing;  // DPBuffers -> SolveData (the reference constructor)
-  double seconds_solve;    // Solve()
-} ref_result;
-
 #define REF_API __attribute__((visibility("default")))
 
-REF_API const char* ref_last_error(void) { return g_error.c_str(); }
-
-}  // extern "C"
-
 namespace {
 
-template <typename V>
-dp3::ddecal::SolveData<V> Pack(const ref_problem& p) {
-  const size_t n_corr = p.n_correlations_in;
-  std::vector<std::string> names;
-  for (uint32_t d = 0; d < p.n_directions; ++d) names.push_back("direction" + std::to_string(d));
-  std::vector<DPBuffer> buffers(p.n_times);
-  for (uint32_t t = 0; t < p.n_times; ++t) {
-    DPBuffer& b = buffers[t];
-    auto fill = [&](DPBuffer::DataType& cube, const float* const* src, size_t dir) {
-      for (uint32_t cb = 0; cb < p.n_channel_blocks; ++cb) {
-        const size_t c0 = size_t(cb) * p.n_channels / p.n_channel_blocks;
-        const size_t c1 = size_t(cb + 1) * p.n_channels / p.n_channel_blocks;
-        const size_t L = c1 - c0;
-        const float* s = src[cb] + (dir * p.n_times + t) * p.n_baselines * L * n_corr * 2;
-        for (uint32_t bl = 0; bl < p.n_baselines; ++bl)
-          for (size_t c = 0; c < L; ++c) {
-            const float* v = s + (size_t(bl) * L + c) * n_corr * 2;
-            std::complex<float>* out = &cube(bl, c0 + c, 0);
-            if (n_corr == 4) {
-              for (int k = 0; k < 4; ++k) out[k] = {v[2 * k], v[2 * k + 1]};
-            } else if (n_corr == 2) {
-              out[0] = {v[0], v[1]};
-              out[1] = out[2] = 0.f;
-              out[3] = {v[2], v[3]};
-            } else {
-              out[0] = out[3] = {v[0], v[1]};
-              out[1] = out[2] = 0.f;
-            }
-          }
-      }
-    };
-    fill(b.AddData("", p.n_baselines, p.n_channels, 4), p.data, 0);
-    for (uint32_t d = 0; d < p.n_directions; ++d)
-      fill(b.AddData(names[d], p.n_baselines, p.n_channels, 4), p.model, d);
-  }
-  const std::vector<size_t> nspd(p.n_solutions_per_direction,
-                                 p.n_solutions_per_direction + p.n_directions);
-  const std::vector<int> a1(p.antenna1, p.antenna1 + p.n_baselines);
-  const std::vector<int> a2(p.antenna2, p.antenna2 + p.n_baselines);
-  return dp3::ddecal::SolveData<V>(std::move(buffers), names, p.n_channel_blocks, p.n_antennas,
-                                   nspd, a1, a2);
-}
+thread_local std::string g_error;
 
 template <typename Solver, typename V>
 int Run(const ref_problem& p, const ref_settings& s, uint32_t n_threads,
         const ref_constraints* c, double* solutions, ref_result* out) {
   schaapcommon::ThreadPool::GetInstance().SetNThreads(std::max<uint32_t>(n_threads, 1));
   const auto t0 = std::chrono::steady_clock::now();
-  const dp3::ddecal::SolveData<V> data = Pack<V>(p);
+  const dp3::ddecal::SolveData<V> data = dp3b200_ref::Pack<V>(p);
   const auto t1 = std::chrono::steady_clock::now();
-
   Solver solver;
-  std::vector<size_t> nspd(p.n_solutions_per_direction,
-                           p.n_solutions_per_direction + p.n_directions);
-  solver.Initialize(p.n_antennas, nspd, p.n_channel_blocks);
-  solver.SetMaxIterations(s.max_iterations);
-  solver.SetMinIterations(s.min_iterations);
-  solver.SetAccuracy(s.accuracy);
-  solver.SetConstraintAccuracy(s.constraint_accuracy);
-  solver.SetStepSize(s.step_size);
-  solver.SetDetectStalling(s.detect_stalling != 0, s.step_diff_sigma);
-  solver.SetPhaseOnly(s.phase_only != 0);
-  if (c) {
-    std::vector<uint32_t> spd(p.n_solutions_per_direction,
-                              p.n_solutions_per_direction + p.n_directions);
-    std::vector<double> freqs(c->channel_block_frequencies,
-                              c->channel_block_frequencies + p.n_channel_blocks);
-    if (c->n_antenna_sets) {
-      auto ac = std::make_unique<dp3::ddecal::AntennaConstraint>();
-      std::vector<std::set<size_t>> sets(c->n_antenna_sets);
-      size_t k = 0;
-      for (uint32_t i = 0; i < c->n_antenna_sets; ++i)
-        for (uint32_t j = 0; j < c->antenna_set_sizes[i]; ++j)
-          sets[i].insert(c->antenna_set_members[k++]);
-      ac->SetAntennaSets(std::move(sets));
-      ac->Initialize(p.n_antennas, spd, freqs);
-      solver.AddConstraint(std::move(ac));
-    }
-    if (c->smoothness) {
-      auto sc = std::make_unique<dp3::ddecal::SmoothnessConstraint>(
-          c->bandwidth_hz, c->bandwidth_ref_frequency_hz, c->spectral_exponent,
-          c->kernel_truncation != 0);
-      sc->Initialize(p.n_antennas, spd, freqs);
-      std::vector<double> w(size_t(p.n_antennas) * p.n_channel_blocks, 1.0);
-      if (c->smoothness_weights) std::copy_n(c->smoothness_weights, w.size(), w.begin());
-      sc->SetWeights(w);
-      sc->SetAntennaFactors(std::vector<double>(p.n_antennas, 1.0));
-      solver.AddConstraint(std::move(sc));
-    }
-  }
-
-  const size_t n_sub = std::accumulate(nspd.begin(), nspd.end(), size_t(0));
+  dp3b200_ref::Configure(solver, p, s, c);
+  const size_t n_sub = std::accumulate(p.n_solutions_per_direction,
+                                       p.n_solutions_per_direction + p.n_directions, size_t(0));
   const size_t per_cb = size_t(p.n_antennas) * n_sub * solver.NSolutionPolarizations();
-  std::vector<std::vector<DComplex>> sol(p.n_channel_blocks);
-  for (uint32_t cb = 0; cb < p.n_channel_blocks; ++cb) {
-    sol[cb].resize(per_cb);
-    std::memcpy(sol[cb].data(), solutions + 2 * cb * per_cb, per_cb * sizeof(DComplex));
-  }
+  auto sol = dp3b200_ref::ToVectors(solutions, p.n_channel_blocks, per_cb);
   const auto t2 = std::chrono::steady_clock::now();
-  const SolverBase::SolveResult r = solver.Solve(data, sol, 0.0);
+  const dp3::ddecal::SolverBase::SolveResult r = solver.Solve(data, sol, 0.0);
   const auto t3 = std::chrono::steady_clock::now();
-  for (uint32_t cb = 0; cb < p.n_channel_blocks; ++cb)
-    std::memcpy(solutions + 2 * cb * per_cb, sol[cb].data(), per_cb * sizeof(DComplex));
+  dp3b200_ref::FromVectors(sol, solutions);
   out->iterations = uint32_t(r.iterations);
   out->constraint_iterations = uint32_t(r.constraint_iterations);
   out->seconds_packing = std::chrono::duration<double>(t1 - t0).count();
@@ -228,11 +64,105 @@ int Run(const ref_problem& p, const ref_settings& s, uint32_t n_threads,
   return 0;
 }
 
+// An interval packed once (SolveData of the solver kind), solved many times.
+struct PreparedBase {
+  virtual ~PreparedBase() = default;
+  virtual int Solve(const ref_problem& p, const ref_settings& s, uint32_t n_threads,
+                    const ref_constraints* c, double* solutions, ref_result* out) = 0;
+};
+
+template <typename Solver, typename V>
+struct Prepared final : PreparedBase {
+  explicit Prepared(const ref_problem& p) : data(dp3b200_ref::Pack<V>(p)) {}
+  int Solve(const ref_problem& p, const ref_settings& s, uint32_t n_threads,
+            const ref_constraints* c, double* solutions, ref_result* out) override {
+    schaapcommon::ThreadPool::GetInstance().SetNThreads(std::max<uint32_t>(n_threads, 1));
+    Solver solver;
+    dp3b200_ref::Configure(solver, p, s, c);
+    const size_t n_sub = std::accumulate(
+        p.n_solutions_per_direction, p.n_solutions_per_direction + p.n_directions, size_t(0));
+    const size_t per_cb = size_t(p.n_antennas) * n_sub * solver.NSolutionPolarizations();
+    auto sol = dp3b200_ref::ToVectors(solutions, p.n_channel_blocks, per_cb);
+    const auto t0 = std::chrono::steady_clock::now();
+    const dp3::ddecal::SolverBase::SolveResult r = solver.Solve(data, sol, 0.0);
+    const auto t1 = std::chrono::steady_clock::now();
+    dp3b200_ref::FromVectors(sol, solutions);
+    out->iterations = uint32_t(r.iterations);
+    out->constraint_iterations = uint32_t(r.constraint_iterations);
+    out->seconds_packing = 0.0;
+    out->seconds_solve = std::chrono::duration<double>(t1 - t0).count();
+    return 0;
+  }
+  const dp3::ddecal::SolveData<V> data;
+};
+
+PreparedBase* Prepare(const ref_problem& p, int kind) {
+  using namespace dp3::ddecal;
+  switch (kind) {
+    case REF_DIAGONAL_DUO:
+      return new Prepared<IterativeDiagonalSolver<aocommon::MC2x2FDiag>, aocommon::MC2x2FDiag>(p);
+    case REF_DIAGONAL_FULL:
+      return new Prepared<IterativeDiagonalSolver<aocommon::MC2x2F>, aocommon::MC2x2F>(p);
+    case REF_SCALAR_UNI:
+      return new Prepared<IterativeScalarSolver<std::complex<float>>, std::complex<float>>(p);
+    case REF_SCALAR_DUO:
+      return new Prepared<IterativeScalarSolver<aocommon::MC2x2FDiag>, aocommon::MC2x2FDiag>(p);
+    case REF_SCALAR_FULL:
+      return new Prepared<IterativeScalarSolver<aocommon::MC2x2F>, aocommon::MC2x2F>(p);
+    default:
+      throw std::runtime_error("unknown solver kind");
+  }
+}
+
 }  // namespace
 
+typedef struct ref_prepared ref_prepared;
+
+// Packs the interval once (the reference's SolveData constructor, timed into
+// *seconds_packing); ref_solve_prepared then solves it with any settings.
+extern "C" REF_API int ref_prepare(const ref_problem* p, int kind, ref_prepared** out,
+                                   double* seconds_packing) {
+  if (!p || !out) {
+    g_error = "NULL argument";
+    return 1;
+  }
+  try {
+    const auto t0 = std::chrono::steady_clock::now();
+    *out = reinterpret_cast<ref_prepared*>(Prepare(*p, kind));
+    if (seconds_packing)
+      *seconds_packing =
+          std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return 0;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return 2;
+  }
+}
+
+// `p` supplies the dimensions again (the same problem as ref_prepare's).
+extern "C" REF_API int ref_solve_prepared(ref_prepared* h, const ref_problem* p,
+                                          const ref_settings* s, uint32_t n_threads,
+                                          const ref_constraints* c, double* solutions,
+                                          ref_result* out) {
+  if (!h || !p || !s || !solutions || !out) {
+    g_error = "NULL argument";
+    return 1;
+  }
+  try {
+    return reinterpret_cast<PreparedBase*>(h)->Solve(*p, *s, n_threads, c, solutions, out);
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return 2;
+  }
+}
+
+extern "C" REF_API void ref_release(ref_prepared* h) { delete reinterpret_cast<PreparedBase*>(h); }
+
+extern "C" REF_API const char* ref_last_error(void) { return g_error.c_str(); }
+
 extern "C" REF_API int ref_solve(const ref_problem* p, const ref_settings* s, int kind,
-                         uint32_t n_threads, const ref_constraints* c, double* solutions,
-                         ref_result* out) {
+                                 uint32_t n_threads, const ref_constraints* c,
+                                 double* solutions, ref_result* out) {
   if (!p || !s || !solutions || !out) {
     g_error = "NULL argument";
     return 1;
