@@ -4176,12 +4176,12 @@ int ddsolve_autotune(ddsolve_ctx* ctx, uint32_t launches, ddsolve_tuning* chosen
 // Allocation-free entry point: one direction-iterative pass over regular
 // data that the caller already holds in device memory, with the per-antenna
 // accumulators in a fixed-size array that lives in the library's own device
-// image. Some callers cannot let a library allocate device memory: code that
-// runs while a CUDA graph is being captured (cudaMalloc is not allowed
-// during capture), frameworks that hand all device memory out of their own
-// pool or arena, and hosts whose device memory is already fully budgeted.
-// This variant only uses that static array; it never calls cudaMalloc,
-// cudaFree or an allocating library routine.
+// image. Some callers cannot let a library allocate device memory:
+// frameworks that hand all device memory out of their own pool or arena (a
+// library cudaMalloc would bypass the pool's accounting and could fail once
+// the pool holds the device), and hosts whose device memory is already fully
+// budgeted. This variant only uses that static array; it never calls
+// cudaMalloc, cudaFree or an allocating library routine.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -4189,6 +4189,7 @@ constexpr size_t kNoAllocScratchFloats = size_t(1) << 20;  // 4 MiB
 constexpr uint32_t kNoAllocMaxChannelBlocks = 256;
 constexpr uint32_t kNoAllocMaxDirections = 64;
 constexpr uint32_t kNoAllocMaxChannels = 16;  // channels per block
+constexpr uint32_t kNoAllocMaxTimes = 65535;   // grid y dimension
 constexpr int kNoAllocThreads = 128;
 
 // Per-antenna accumulators [cb][ant][sub][pol][num.re, num.im, den]. Every
@@ -4222,7 +4223,9 @@ __global__ void __launch_bounds__(kNoAllocThreads)
   if (bl >= p.n_bl) return;
   const uint32_t a1 = p.antenna1[bl];
   const uint32_t a2 = p.antenna2[bl];
-  if (a1 >= p.n_ant || a2 >= p.n_ant) return;  // invalid pairs are ignored
+  // Invalid pairs are ignored; autocorrelations are dropped, as the regular
+  // SolveData constructor drops them (SolveData.cc:100,137).
+  if (a1 >= p.n_ant || a2 >= p.n_ant || a1 == a2) return;
   const uint32_t L = p.cb_channels[cb];
   const uint64_t n_vis_cb = uint64_t(p.n_times) * p.n_bl * L;
   const uint64_t v0 = (uint64_t(t) * p.n_bl + bl) * L;
@@ -4349,7 +4352,9 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // Device address of g_noalloc_scratch, looked up once per device (with that
-// device current) and cached.
+// device current) and cached for the life of the process. The cache assumes
+// the device's primary context is never reset: after cudaDeviceReset the
+// cached address is stale.
 int NoAllocScratchAddress(int device, float** out) {
   static std::mutex mu;
   static std::map<int, float*> cache;
@@ -4405,6 +4410,11 @@ extern "C" int ddsolve_perform_iteration_noalloc(
   for (uint32_t d = 0; d < n_dir; ++d) n_sub += dims->n_solutions_per_direction[d];
   if (n_cb > kNoAllocMaxChannelBlocks || n_dir > kNoAllocMaxDirections) {
     g_last_error = std::string(who) + "more than 256 channel blocks or 64 directions";
+    return DDSOLVE_E_UNSUPPORTED;
+  }
+  if (n_times > kNoAllocMaxTimes) {
+    // the launch grid's y dimension runs over the time steps
+    g_last_error = std::string(who) + "more than 65535 time steps";
     return DDSOLVE_E_UNSUPPORTED;
   }
   const uint64_t acc_floats = uint64_t(n_cb) * n_ant * n_sub * n_pol * 3;

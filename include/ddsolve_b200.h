@@ -2,9 +2,9 @@
  * ddsolve_b200 -- C ABI of the B200 direction-iterative gain solver.
  *
  * This is the drop-in boundary for DP3's DDECal direction-iterative solvers.
- * A DP3-side adapter class derived from dp3::ddecal::SolverBase (see
- * INTEGRATION.md) binds these entry points; every entry point below names the
- * reference interface it replaces.
+ * A DP3-side adapter class derived from dp3::ddecal::SolverBase
+ * (dp3_b200/dp3/IterativeSolverB200.h) binds these entry points; every entry
+ * point below names the reference interface it replaces.
  *
  * Conventions
  *  - Plain pointers and sizes only. No exception crosses the ABI: every
@@ -248,15 +248,18 @@ DDSOLVE_API int ddsolve_time_stream_kernel(ddsolve_ctx* ctx, uint32_t n_launches
 /* Allocation-free direction-iterative pass (no counterpart in the reference:
  * DP3's solvers always own their buffers).
  *
- * Some callers cannot let a library allocate device memory: code running
- * while a CUDA graph is being captured (cudaMalloc is not permitted during
- * capture), frameworks that serve all device memory from their own pool or
- * arena, and processes whose device memory is budgeted in advance. This
- * entry point computes the same next_solutions as ddsolve_perform_iteration
- * without a context and without calling cudaMalloc, cudaFree or any
- * allocating library routine. Its per-antenna accumulators live in one fixed
- * 4 MiB array compiled into this library; every GPU that loads the library
- * holds that array until the process exits.
+ * Some callers cannot let a library allocate device memory: frameworks that
+ * serve all device memory from their own pool or arena (an allocation behind
+ * the pool's back escapes its accounting and can fail once the pool holds
+ * the device), and processes whose device memory is budgeted in advance.
+ * This entry point computes the same next_solutions as
+ * ddsolve_perform_iteration without a context and without calling
+ * cudaMalloc, cudaFree or any allocating library routine. Its per-antenna
+ * accumulators live in one fixed 4 MiB array compiled into this library;
+ * every GPU that loads the library holds that array until the process exits.
+ * They are summed with FP32 global atomics, without compensation, so the
+ * summation order (and the last bits of the result) can differ between
+ * calls; the context entry points use fixed-order compensated merges.
  *
  * Inputs and outputs are DEVICE pointers the caller owns, for regular data
  * in the layout of ddsolve_set_channel_block_regular, with the channel blocks
@@ -265,16 +268,19 @@ DDSOLVE_API int ddsolve_time_stream_kernel(ddsolve_ctx* ctx, uint32_t n_launches
  * then cb 1's, ...; antenna1 / antenna2 [n_baselines]; solutions and
  * next_solutions [n_cb][n_ant][n_sub][n_pol] complex double. dims and
  * cb_channels are host pointers. Baselines with an antenna index
- * >= n_antennas are skipped.
+ * >= n_antennas are skipped, and so are autocorrelations (antenna1 ==
+ * antenna2), which the reference's SolveData drops (SolveData.cc:100,137).
  *
  * Limits (DDSOLVE_E_UNSUPPORTED with a message beyond them): at most 256
- * channel blocks, 64 directions and 16 channels per block, and
- * n_cb * n_ant * n_sub * n_pol * 3 <= 1048576 accumulators.
+ * channel blocks, 64 directions, 16 channels per block and 65535 time steps,
+ * and n_cb * n_ant * n_sub * n_pol * 3 <= 1048576 accumulators.
  *
  * Work is queued on `stream` (a cudaStream_t; NULL = the legacy default
  * stream) and the call returns without waiting. The first call on a device
- * looks up the array's device address with that device current; make that
- * first call before any stream capture. Every call reuses the same array and
+ * looks up the array's device address with that device current and caches
+ * it for the rest of the process; cudaDeviceReset invalidates that cached
+ * address, so do not call this entry point after resetting the device.
+ * Every call reuses the same array and
  * clears the part it needs at its start, so calls that overlap on the GPU
  * (different streams or devices sharing a context) race: order them on one
  * stream or synchronise between them. */

@@ -60,6 +60,28 @@ def make_solver(problem, max_iterations=50, accuracy=1e-5, step_size=0.2,
     return s
 
 
+def perturbed_start(obs, problem, scale=0.3, seed=3):
+    """Initial solutions: true gain at the block's first channel times a
+    random perturbation, so one pass does real work."""
+    cfg = obs.cfg
+    rng = np.random.default_rng(seed)
+    ncb = cfg.n_channel_blocks
+    n_sub = sum(problem["n_solutions_per_direction"])
+    npol = problem["n_pol"]
+    starts = np.cumsum([0] + list(cfg.cb_channels))[:-1]
+    sol = np.ones((ncb, cfg.n_stations, n_sub, npol), np.complex128)
+    d_of_sub = np.repeat(np.arange(cfg.n_directions),
+                         problem["n_solutions_per_direction"])
+    for cb in range(ncb):
+        g = obs.true_gains[starts[cb]]  # [st, dir, 2]
+        for s in range(n_sub):
+            gg = g[:, d_of_sub[s], :npol]
+            pert = 1 + scale * (rng.standard_normal(gg.shape)
+                                + 1j * rng.standard_normal(gg.shape))
+            sol[cb, :, s, :] = gg * pert
+    return sol
+
+
 def unit_solutions(problem):
     n_sub = sum(problem["n_solutions_per_direction"])
     return np.ones((len(problem["data"]), problem["n_antennas"], n_sub,
