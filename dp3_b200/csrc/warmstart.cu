@@ -172,6 +172,9 @@ __device__ __forceinline__ float FromBf16(uint16_t u) {
   return __uint_as_float(uint32_t(u) << 16);
 }
 
+__device__ __forceinline__ void StoreEpilogueRow(const GemmParams& p, int row, int nb,
+                                                 bool vec_out, bool vec_mask, float (&v)[32]);
+
 template <int NT>
 __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmParams p) {
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -262,7 +265,11 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmParams p) 
   const bool vec_mask = p.epilogue == kEpiBf16Mask &&
                         (reinterpret_cast<uintptr_t>(p.mask) & 15u) == 0 &&
                         (size_t(p.ldc) * 2) % 16 == 0;
+  // Every lane of the warp runs every column group's tcgen05.ld (a
+  // .sync.aligned warp-collective): rows beyond M only skip their stores,
+  // inside the group, and the warp reconverges before the next load.
   for (int col = 0; col < NT; col += 32) {
+    __syncwarp();
     uint32_t r[32];
     const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + uint32_t(col);
     asm volatile(
@@ -285,7 +292,21 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmParams p) 
 #pragma unroll
     for (int j = 0; j < 32; ++j)
       v[j] = __uint_as_float(r[j]) + (p.bias && nb + j < p.N ? __ldg(p.bias + nb + j) : 0.f);
-    if (row >= p.M) continue;
+    if (row < p.M) StoreEpilogueRow(p, row, nb, vec_out, vec_mask, v);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(uint32_t(NT))
+                 : "memory");
+}
+
+// One row's 32-column group of the epilogue: bias already added in v; applies
+// the ReLU or the ReLU-derivative mask and stores FP32 or BF16.
+__device__ __forceinline__ void StoreEpilogueRow(const GemmParams& p, int row, int nb,
+                                                 bool vec_out, bool vec_mask, float (&v)[32]) {
+  {  // one output row, columns nb .. nb + 31
     const size_t o0 = size_t(row) * p.ldc + nb;
     const bool full = vec_out && nb + 32 <= p.N;
     if (p.epilogue == kEpiF32) {
@@ -299,7 +320,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmParams p) 
         for (int j = 0; j < 32; ++j)
           if (nb + j < p.N) out[j] = v[j];
       }
-      continue;
+      return;
     }
     if (p.epilogue == kEpiBf16Mask) {  // v = 0 where the mask (ReLU output) is not > 0
       const uint16_t* mk = p.mask + o0;
@@ -340,12 +361,6 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(const GemmParams p) 
         if (nb + j < p.N) out[j] = ToBf16(v[j]);
     }
   }
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
-  if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(uint32_t(NT))
-                 : "memory");
 }
 
 template <int NT>
@@ -931,6 +946,60 @@ int ddwarm_gradients(ddwarm_ctx* ctx, uint32_t n, const float* x, const float* t
   if ((rc = CopyParams(ctx, grads, true, true))) return rc;
   if (loss) {
     WARM_CHECK(ctx, cudaMemcpyAsync(loss, ctx->loss.ptr, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    WARM_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return 0;
+}
+
+int ddwarm_trace(ddwarm_ctx* ctx, uint32_t n, const float* x, const float* target,
+                 const ddwarm_trace_out* out) {
+  if (!ctx || n == 0 || !x || !out) return 1;
+  cudaSetDevice(ctx->device);
+  int rc;
+  if ((rc = Reserve(ctx, n))) return rc;
+  if ((rc = Upload(ctx, ctx->ds_x, x, size_t(n) * ctx->n_in * 4))) return rc;
+  if (target && (rc = Upload(ctx, ctx->ds_t, target, size_t(n) * ctx->n_out * 4))) return rc;
+  gather_rows_kernel<<<n, 128, 0, ctx->stream>>>(
+      ctx->ds_x.as<float>(), ctx->n_in, nullptr, n, ctx->xb.as<uint16_t>(), ctx->di,
+      target ? ctx->ds_t.as<float>() : nullptr, ctx->n_out, ctx->t.as<float>(), ctx->dout);
+  WARM_CHECK(ctx, cudaGetLastError());
+  if ((rc = Forward(ctx, n))) return rc;
+  if (target && (rc = Backward(ctx, n))) return rc;
+  if ((rc = CheckError(ctx))) return rc;
+  // Padded device rows [n][ld] -> host [n][cols] FP32.
+  auto fetch = [&](const DevBuf& src, bool bf16, uint32_t ld, uint32_t cols, float* dst) {
+    if (!dst) return 0;
+    const size_t esz = bf16 ? 2 : 4;
+    std::vector<unsigned char> tmp(size_t(n) * ld * esz);
+    WARM_CHECK(ctx, cudaMemcpyAsync(tmp.data(), src.ptr, tmp.size(), cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+    WARM_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
+    for (uint32_t r = 0; r < n; ++r)
+      for (uint32_t c = 0; c < cols; ++c) {
+        const size_t i = size_t(r) * ld + c;
+        if (bf16) {
+          uint16_t u;
+          memcpy(&u, tmp.data() + i * 2, 2);
+          const uint32_t w = uint32_t(u) << 16;
+          memcpy(dst + size_t(r) * cols + c, &w, 4);
+        } else {
+          memcpy(dst + size_t(r) * cols + c, tmp.data() + i * 4, 4);
+        }
+      }
+    return 0;
+  };
+  if ((rc = fetch(ctx->xb, true, ctx->di, ctx->n_in, out->xb))) return rc;
+  if ((rc = fetch(ctx->h1, true, ctx->dh, ctx->n_hidden, out->h1))) return rc;
+  if ((rc = fetch(ctx->h2, true, ctx->dh, ctx->n_hidden, out->h2))) return rc;
+  if ((rc = fetch(ctx->y, false, ctx->dout, ctx->n_out, out->y))) return rc;
+  if (!target) return 0;
+  if ((rc = fetch(ctx->dy, true, ctx->dout, ctx->n_out, out->dy))) return rc;
+  if ((rc = fetch(ctx->dz2, true, ctx->dh, ctx->n_hidden, out->dz2))) return rc;
+  if ((rc = fetch(ctx->dz1, true, ctx->dh, ctx->n_hidden, out->dz1))) return rc;
+  if (out->grads && (rc = CopyParams(ctx, out->grads, true, true))) return rc;
+  if (out->loss) {
+    WARM_CHECK(ctx, cudaMemcpyAsync(out->loss, ctx->loss.ptr, 4, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
     WARM_CHECK(ctx, cudaStreamSynchronize(ctx->stream));
   }
   return 0;

@@ -38,7 +38,7 @@ EXPORTED_SYMBOLS = (
     "ddwarm_create", "ddwarm_destroy", "ddwarm_last_error", "ddwarm_param_count",
     "ddwarm_get_params", "ddwarm_set_params", "ddwarm_predict",
     "ddwarm_gradients", "ddwarm_train", "ddwarm_features", "ddwarm_predict_start",
-    "ddwarm_set_stream",
+    "ddwarm_set_stream", "ddwarm_trace",
 )
 
 _lib = None
@@ -70,6 +70,7 @@ def lib():
         L.ddwarm_features.argtypes = [vp, vp, u32, vp, vp]
         L.ddwarm_predict_start.argtypes = [vp, vp, u32, vp, vp]
         L.ddwarm_set_stream.argtypes = [vp, vp]
+        L.ddwarm_trace.argtypes = [vp, u32, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -142,6 +143,28 @@ class MLP:
                                            ctypes.byref(loss)))
         return g, float(loss.value)
 
+    def trace(self, x, t=None):
+        """Intermediate values of one pass (ddwarm_trace): dict with xb, h1,
+        h2, y and, with a target t, dy, dz2, dz1, grads and loss."""
+        x = np.ascontiguousarray(x, np.float32)
+        n = x.shape[0]
+        h, o = self.hidden, self.n_out
+        out = {"xb": np.zeros((n, self.n_in), np.float32), "h1": np.zeros((n, h), np.float32),
+               "h2": np.zeros((n, h), np.float32), "y": np.zeros((n, o), np.float32)}
+        if t is not None:
+            t = np.ascontiguousarray(t, np.float32)
+            out.update(dy=np.zeros((n, o), np.float32), dz2=np.zeros((n, h), np.float32),
+                       dz1=np.zeros((n, h), np.float32),
+                       grads=np.zeros(lib().ddwarm_param_count(self._h), np.float32),
+                       loss=np.zeros(1, np.float32))
+        st = TraceOut(*[ctypes.c_void_p(out[k].ctypes.data) if k in out else None
+                        for k in TraceOut.KEYS])
+        self._check(lib().ddwarm_trace(self._h, n, _ptr(x), _ptr(t) if t is not None else None,
+                                       ctypes.byref(st)))
+        if t is not None:
+            out["loss"] = float(out["loss"][0])
+        return out
+
     def train(self, x, t, epochs=100, batch=1024, lr=1e-3, seed=1):
         x = np.ascontiguousarray(x, np.float32)
         t = np.ascontiguousarray(t, np.float32)
@@ -149,6 +172,12 @@ class MLP:
         self._check(lib().ddwarm_train(self._h, x.shape[0], _ptr(x), _ptr(t), epochs, batch,
                                        ctypes.c_float(lr), seed, _ptr(losses)))
         return losses[:epochs]
+
+
+class TraceOut(ctypes.Structure):
+    """ddwarm_trace_out (include/ddwarm_b200.h)."""
+    KEYS = ("xb", "h1", "h2", "y", "dy", "dz2", "dz1", "grads", "loss")
+    _fields_ = [(k, ctypes.c_void_p) for k in KEYS]
 
 
 class Layout(ctypes.Structure):

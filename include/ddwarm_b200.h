@@ -60,6 +60,33 @@ DDSOLVE_API int ddwarm_predict(ddwarm_ctx* ctx, uint32_t n, const float* x, floa
 DDSOLVE_API int ddwarm_gradients(ddwarm_ctx* ctx, uint32_t n, const float* x,
                                  const float* target, float* grads, float* loss);
 
+/* Intermediate values of one pass, so that each tensor-core product can be
+ * checked on its own against an oracle fed the GPU's own inputs of that
+ * layer. Every pointer may be NULL (not returned). Host FP32 arrays, BF16
+ * quantities as their exact FP32 values:
+ *   xb [n][n_in]       the input rounded to BF16 (the first product's A)
+ *   h1, h2 [n][n_hidden]  BF16 hidden activations relu(z + b)
+ *   y [n][n_out]       FP32 output
+ * With a target [n][n_out] (else these stay untouched):
+ *   dy [n][n_out]      BF16 dL/dY = 2 (y - t) / (n n_out)
+ *   dz2, dz1 [n][n_hidden]  BF16 dL/dZ after the ReLU masks
+ *   grads              packed as the parameters (as ddwarm_gradients)
+ *   loss               mean (y - t)^2 (one float)
+ * No counterpart in the reference (DP3 has no learned component). */
+typedef struct {
+  float* xb;
+  float* h1;
+  float* h2;
+  float* y;
+  float* dy;
+  float* dz2;
+  float* dz1;
+  float* grads;
+  float* loss;
+} ddwarm_trace_out;
+DDSOLVE_API int ddwarm_trace(ddwarm_ctx* ctx, uint32_t n, const float* x, const float* target,
+                             const ddwarm_trace_out* out);
+
 /* Trains on the data set x [n][n_in], target [n][n_out] (host FP32, uploaded
  * once): `epochs` passes of shuffled mini-batches of `batch` rows (the order
  * from std::mt19937_64(seed)), Adam (beta 0.9 / 0.999, eps 1e-8) at learning
