@@ -1,0 +1,159 @@
+"""Full-size GPU solves against the reference itself and the oracles.
+
+The reference here is DP3's own IterativeDiagonalSolver / IterativeScalarSolver
+compiled from the reference sources (oracle/_ref, oracle/ref_ffi.py), run with
+one thread per channel block (a fixed FP32 summation order). The bar is the
+north star's: identical iteration counts at tolerance 1e-5 and solutions
+within 1e-4 relative after phase referencing to antenna 0. Cases:
+
+* benchmark configurations from unit solutions (51 iterations, capped): c1
+  (62 stations, 10 directions, 240 channels) and c3 (512 stations, diagonal
+  and scalar solvers);
+* converging full-size solves (c4 and c1 from a start near the true gains),
+  which stop at an iteration count below the cap;
+* a solve that DP3's stall detection stops (SolverBase.cc:63-86), on the
+  device's own stall detection;
+* the 40-direction configuration with uneven channel blocks (which the
+  reference's regular SolveData cannot express) batched as three full-size
+  intervals in one launch, each against the FP64 oracle over the full 51
+  iterations and the FP32 restatement over 10, and the same configuration
+  with even blocks against the reference.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+from dp3_b200 import ddsolve, synth
+from oracle import oracle_ffi as of
+from oracle import ref_ffi as rf
+from tests import helpers as H
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not rf.available(), reason="reference-code oracle not built")]
+
+RTOL = 1e-4
+
+
+def _ref_solve(obs, prob, sol, n_threads, **st):
+    cfg = obs.cfg
+    return rf.solve(cfg, obs.antenna1, obs.antenna2, prob["data"], prob["model"],
+                    prob["n_correlations"], prob["n_pol"], sol, rf.settings(**st),
+                    n_threads=n_threads)
+
+
+def _gpu_solve(obs, prob, sol, **st):
+    solver = H.make_solver(prob, max_iterations=st["max_iterations"],
+                           accuracy=st.get("accuracy", 1e-5),
+                           step_size=st.get("step_size", 0.2),
+                           detect_stalling=st.get("detect_stalling", True))
+    return solver.Solve(obs.solve_data(), sol, 0.0)
+
+
+@pytest.mark.parametrize("cfg_index,npol", [(1, 2), (3, 2), (3, 1)])
+def test_benchmark_config_matches_reference(built, cfg_index, npol):
+    cfg = synth.benchmark_configs()[cfg_index]
+    obs = synth.observe(cfg)
+    prob = H.problem_from_observation(obs, 2, npol)
+    st = dict(max_iterations=cfg.max_iterations, accuracy=cfg.tolerance,
+              step_size=cfg.step_size)
+    ref = H.unit_solutions(prob)
+    r = _ref_solve(obs, prob, ref, cfg.n_channel_blocks, **st)
+    got = H.unit_solutions(prob)
+    res = _gpu_solve(obs, prob, got, **st)
+    assert res.iterations == r.iterations
+    assert H.max_rel_diff(got, ref) < RTOL
+
+
+@pytest.mark.parametrize("cfg_index", [4, 1])
+def test_converging_full_size_solve(built, cfg_index):
+    """Start within a few per cent of the true gains, maximum 500
+    iterations: the solve converges at tolerance 1e-5 well before the cap,
+    at the same iteration on the GPU, the reference and the FP32 oracle."""
+    cfg = synth.benchmark_configs()[cfg_index]
+    obs = synth.observe(cfg)
+    prob = H.problem_from_observation(obs)
+    start = H.perturbed_start(obs, prob, scale=0.02, seed=7)
+    st = dict(max_iterations=500, accuracy=cfg.tolerance, step_size=cfg.step_size)
+    ref = start.copy()
+    r = _ref_solve(obs, prob, ref, cfg.n_channel_blocks, **st)
+    assert r.iterations < 500
+    ora = start.copy()
+    ro, _ = of.solve(prob, ora, of.settings(**st), precision=32,
+                     n_threads=cfg.n_channel_blocks)
+    got = start.copy()
+    res = _gpu_solve(obs, prob, got, **st)
+    assert res.has_converged
+    assert res.iterations == r.iterations == ro.iterations
+    assert H.max_rel_diff(got, ref) < RTOL
+
+
+def test_stall_detection_matches_reference(built):
+    """Accuracy 1e-14, beyond FP32: the step magnitudes plateau and the
+    device's stall detection stops the solve at the reference's iteration."""
+    obs = H.small_observation(n_stations=10, n_directions=3, n_channels=8, n_cb=2,
+                              n_times=3, seed=21)
+    prob = H.problem_from_observation(obs)
+    st = dict(max_iterations=3000, accuracy=1e-14, step_size=0.5)
+    ref = H.unit_solutions(prob)
+    r = _ref_solve(obs, prob, ref, 1, **st)
+    assert r.iterations < 3000
+    got = H.unit_solutions(prob)
+    res = _gpu_solve(obs, prob, got, **st)
+    assert res.has_stalled and not res.has_converged
+    assert res.iterations == r.iterations
+    assert H.max_rel_diff(got, ref) < RTOL
+
+
+def test_dd_configuration_even_blocks_matches_reference(built):
+    """The 40-direction DD-interval configuration (8/4/2/1 solutions per
+    8-timestep interval) with the reference's even channel blocks, so that
+    the reference's own SolveData packs it: 20 iterations."""
+    cfg = dataclasses.replace(synth.benchmark_configs()[2],
+                              cb_channels=synth._even_blocks(120, 12))
+    obs = synth.observe(cfg)
+    prob = H.problem_from_observation(obs)
+    st = dict(max_iterations=20, accuracy=cfg.tolerance, step_size=cfg.step_size)
+    start = H.perturbed_start(obs, prob, scale=0.1)
+    ref = start.copy()
+    r = _ref_solve(obs, prob, ref, cfg.n_channel_blocks, **st)
+    got = start.copy()
+    res = _gpu_solve(obs, prob, got, **st)
+    assert res.iterations == r.iterations
+    assert H.max_rel_diff(got, ref) < RTOL
+
+
+def test_batched_dd_intervals_against_oracle(built):
+    """Three full-size intervals of the 40-direction configuration (uneven
+    channel blocks of 3-12 channels) batched in one context and one launch
+    per iteration (ddsolve_set_intervals / ddsolve_solve_batch), each
+    interval against the FP64 oracle's own solve (51 iterations from unit
+    solutions) and against the FP32 restatement over 10 iterations."""
+    cfg = synth.benchmark_configs()[2]
+    n_cb = cfg.n_channel_blocks
+    obs_list = [synth.observe(cfg, true_gains=synth.gains(cfg, seed=s), start_time_s=600.0 * k,
+                              noise_seed=77 + k)
+                for k, s in enumerate((5, 6, 7))]
+    n_sub = sum(cfg.nspd)
+    for max_it, precision in ((10, 32), (cfg.max_iterations, 64)):
+        st = ddsolve.default_settings()
+        st.max_iterations, st.accuracy, st.step_size = max_it, cfg.tolerance, cfg.step_size
+        ctx = ddsolve.Context(cfg.n_stations, cfg.nspd, 3 * n_cb, 2, 2)
+        ctx.set_settings(st)
+        ctx.set_intervals([0, n_cb, 2 * n_cb, 3 * n_cb])
+        for g, obs in enumerate(obs_list):
+            for cb, nc in enumerate(cfg.cb_channels):
+                ctx.set_channel_block_regular(g * n_cb + cb, cfg.n_times, cfg.n_baselines, nc,
+                                              obs.data[cb], obs.model[cb], obs.antenna1,
+                                              obs.antenna2)
+        sol = np.ones((3 * n_cb, cfg.n_stations, n_sub, 2), np.complex128)
+        res = ctx.solve_batch(sol)
+        ctx.close()
+        for g, obs in enumerate(obs_list):
+            prob = H.problem_from_observation(obs)
+            ref = H.unit_solutions(prob)
+            r, _ = of.solve(prob, ref, of.settings(max_iterations=max_it, accuracy=cfg.tolerance,
+                                                   step_size=cfg.step_size),
+                            precision=precision)
+            assert res[g].iterations == r.iterations, (g, max_it)
+            assert H.max_rel_diff(sol[g * n_cb:(g + 1) * n_cb], ref) < RTOL, (g, max_it)
