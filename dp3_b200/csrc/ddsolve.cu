@@ -46,6 +46,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <type_traits>
@@ -281,6 +282,203 @@ __global__ void pack_kernel(const PackSlab* __restrict__ slabs, uint32_t slab,
     for (uint32_t d = 0; d < n_dir; ++d)
       CopyVis<NCORR>(src_model + (d * n_vis + v) * NCORR,
                      dst + SlabElem(s.R, s.W, 1 + n_dir, tl, 1 + d, r) * NCORR, valid, flip);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// predict_kernel: model visibilities of point sources for one regular
+// channel block, written in the reference layout model[dir][vis][corr] that
+// pack_kernel reads -- DP3's predict of a point source (base/Simulator.cc:
+// 112-245 visit(PointSource), station phases :477-520, flat Stokes spectrum
+// :522-547): per source, phi_p = 2 pi / c (u_p l + v_p m + w_p (n - 1)) and
+// V_pq(nu) += S exp(i (phi_q - phi_p) nu), with S = I + Q, U + iV, U - iV,
+// I - Q for XX, XY, YX, YY (NCORR = 4), XX and YY (NCORR = 2) or I
+// (NCORR = 1: DP3's single-correlation data is (XX + YY) / 2). FP64
+// throughout, stored complex64. One thread per (time, baseline, direction);
+// channels in chunks of kPredictChunk / NCORR held in registers. Where the
+// block's channels are evenly spaced the phasor advances by one complex
+// multiplication per channel (exp(i dphi (nu0 + k df)) = exp(i dphi nu0)
+// exp(i dphi df)^k, restarted per chunk; relative drift ~ chunk * 1e-16,
+// far below the complex64 rounding of the result), else one sincos per
+// channel.
+// ---------------------------------------------------------------------------
+constexpr int kPredictChunk = 16;
+constexpr int kPredictThreads = 128;
+constexpr double kTwoPiOverC = 2.0 * 3.14159265358979323846 / 299792458.0;
+
+struct PredictParams {
+  const double* uvw;        // [n_times][n_ant][3] station UVW (m)
+  const double* src;        // [n_src_total][8]: l, m, n - 1, I, Q, U, V, 0
+  const uint32_t* src_off;  // [n_dir + 1]: sources of direction d
+  const double* freq;       // [L] channel frequencies of the block (Hz)
+  const uint32_t* a1;       // [n_bl]
+  const uint32_t* a2;
+  float2* model;            // [n_dir][n_times * n_bl * L][NCORR]
+  uint32_t n_times, n_bl, L, n_ant, n_dir, max_src;
+  int uniform;              // channels evenly spaced: df between them
+  double df;
+};
+
+template <int NCORR>
+__global__ void __launch_bounds__(kPredictThreads) predict_kernel(const PredictParams p) {
+  constexpr int CH = kPredictChunk / NCORR;
+  extern __shared__ double predict_smem[];
+  const uint32_t t = blockIdx.y, d = blockIdx.z;
+  double* uvw = predict_smem;                          // [n_ant][3]
+  double* src = predict_smem + size_t(p.n_ant) * 3;    // [n_src][8]
+  const uint32_t s0 = p.src_off[d], ns = p.src_off[d + 1] - s0;
+  for (uint32_t i = threadIdx.x; i < p.n_ant * 3; i += blockDim.x)
+    uvw[i] = p.uvw[size_t(t) * p.n_ant * 3 + i];
+  for (uint32_t i = threadIdx.x; i < ns * 8; i += blockDim.x) src[i] = p.src[size_t(s0) * 8 + i];
+  __syncthreads();
+  const uint32_t bl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (bl >= p.n_bl) return;
+  const uint32_t ap = p.a1[bl], aq = p.a2[bl];
+  const double du = uvw[aq * 3] - uvw[ap * 3];
+  const double dv = uvw[aq * 3 + 1] - uvw[ap * 3 + 1];
+  const double dw = uvw[aq * 3 + 2] - uvw[ap * 3 + 2];
+  const uint64_t n_vis = uint64_t(p.n_times) * p.n_bl * p.L;
+  const uint64_t v0 = (uint64_t(t) * p.n_bl + bl) * p.L;
+  float2* out = p.model + (uint64_t(d) * n_vis + v0) * NCORR;
+  for (uint32_t c0 = 0; c0 < p.L; c0 += CH) {
+    const uint32_t nc = min(uint32_t(CH), p.L - c0);
+    double2 acc[CH][NCORR];
+#pragma unroll
+    for (int c = 0; c < CH; ++c)
+#pragma unroll
+      for (int k = 0; k < NCORR; ++k) acc[c][k] = make_double2(0.0, 0.0);
+    for (uint32_t s = 0; s < ns; ++s) {
+      const double* q = src + s * 8;
+      // phi_q - phi_p per Hz
+      const double dphi = kTwoPiOverC * (du * q[0] + dv * q[1] + dw * q[2]);
+      double zs, zc, ss = 0.0, sc = 1.0;
+      sincos(dphi * p.freq[c0], &zs, &zc);
+      if (p.uniform) sincos(dphi * p.df, &ss, &sc);
+      double2 stokes[NCORR];
+      if (NCORR == 1) {
+        stokes[0] = make_double2(q[3], 0.0);
+      } else if (NCORR == 2) {
+        stokes[0] = make_double2(q[3] + q[4], 0.0);
+        stokes[NCORR - 1] = make_double2(q[3] - q[4], 0.0);
+      } else {
+        stokes[0] = make_double2(q[3] + q[4], 0.0);
+        stokes[1] = make_double2(q[5], q[6]);
+        stokes[2] = make_double2(q[5], -q[6]);
+        stokes[NCORR - 1] = make_double2(q[3] - q[4], 0.0);
+      }
+#pragma unroll
+      for (int c = 0; c < CH; ++c) {
+        if (c < int(nc)) {
+          if (c > 0) {
+            if (p.uniform) {
+              const double r = zc * sc - zs * ss;
+              zs = zc * ss + zs * sc;
+              zc = r;
+            } else {
+              sincos(dphi * p.freq[c0 + c], &zs, &zc);
+            }
+          }
+#pragma unroll
+          for (int k = 0; k < NCORR; ++k) {
+            acc[c][k].x += stokes[k].x * zc - stokes[k].y * zs;
+            acc[c][k].y += stokes[k].x * zs + stokes[k].y * zc;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CH; ++c)
+      if (c < int(nc))
+#pragma unroll
+        for (int k = 0; k < NCORR; ++k)
+          out[uint64_t(c0 + c) * NCORR + k] =
+              make_float2(float(acc[c][k].x), float(acc[c][k].y));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// weigh_kernel: DDECal's AssignAndWeight (ddecal/gain_solvers/SolverTools.cc:
+// 81-167) and the regular SolveData conversion (SolveData.cc:18-31, 77-188)
+// of one channel block, from DP3's raw buffer layout ([time][baseline]
+// [channel][XX XY YX YY]) into the reference layout that pack_kernel reads.
+// Per visibility: flagged if any correlation is flagged or non-finite in the
+// data or in any direction's model (:112-124); data and every model weighted
+// by sqrt(w) (or w in linear mode) per correlation (:131-139, Weigh :48-79);
+// flagged visibilities zeroed (:145-162); then ToSpecificMatrix (XX, YY for
+// 2 correlations, (XX + YY) / 2 for 1). One thread per (time, cross
+// baseline, channel of the block); autocorrelations are not visited (the
+// SolveData constructor drops them, :100,137).
+// ---------------------------------------------------------------------------
+struct WeighParams {
+  const float2* data;            // [n_times][n_bl][n_ch][4]
+  const float* weights;          // [n_times][n_bl][n_ch][4]
+  const uint8_t* flags;          // [n_times][n_bl][n_ch][4] or null
+  const float2* model;           // raw [dir][t][bl][ch][4], or predicted [dir][t][bx][L][4]
+  const uint32_t* bl_of_cross;   // [n_bx] buffer baseline of each cross baseline
+  float2* out;                   // data [n_vis][NCORR], then model [dir][n_vis][NCORR]
+  uint32_t n_times, n_bl, n_ch, n_bx, c0, L, n_dir;
+  int model_predicted, linear;
+};
+
+template <int NCORR>
+__global__ void weigh_kernel(const WeighParams p) {
+  const uint64_t n_vis = uint64_t(p.n_times) * p.n_bx * p.L;
+  for (uint64_t v = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; v < n_vis;
+       v += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t ch = uint32_t(v % p.L);
+    const uint32_t bx = uint32_t((v / p.L) % p.n_bx);
+    const uint32_t t = uint32_t(v / (uint64_t(p.L) * p.n_bx));
+    const uint32_t bl = p.bl_of_cross[bx];
+    const uint64_t ri = (uint64_t(t) * p.n_bl + bl) * p.n_ch + p.c0 + ch;
+    auto model_at = [&](uint32_t d) -> const float2* {
+      const uint64_t mi = p.model_predicted
+                              ? (uint64_t(d) * p.n_times + t) * p.n_bx * p.L +
+                                    uint64_t(bx) * p.L + ch
+                              : (uint64_t(d) * p.n_times + t) * p.n_bl * p.n_ch +
+                                    uint64_t(bl) * p.n_ch + p.c0 + ch;
+      return p.model + mi * 4;
+    };
+    auto finite = [](float2 z) { return isfinite(z.x) && isfinite(z.y); };
+    float2 dv[4];
+    float pw[4];
+    bool flag = false;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      dv[k] = p.data[ri * 4 + k];
+      const float w = p.weights[ri * 4 + k];
+      pw[k] = p.linear ? w : sqrtf(w);
+      flag = flag || (p.flags && p.flags[ri * 4 + k]) || !finite(dv[k]);
+    }
+    for (uint32_t d = 0; d < p.n_dir && !flag; ++d) {
+      const float2* m = model_at(d);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) flag = flag || !finite(m[k]);
+    }
+    auto put = [&](float2* dst, const float2 (&z)[4]) {
+      if (NCORR == 4) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dst[k] = z[k];
+      } else if (NCORR == 2) {
+        dst[0] = z[0];
+        dst[1] = z[3];
+      } else {
+        dst[0] = make_float2(0.5f * (z[0].x + z[3].x), 0.5f * (z[0].y + z[3].y));
+      }
+    };
+    float2 z[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      z[k] = flag ? make_float2(0.f, 0.f) : make_float2(dv[k].x * pw[k], dv[k].y * pw[k]);
+    put(p.out + v * NCORR, z);
+    for (uint32_t d = 0; d < p.n_dir; ++d) {
+      const float2* m = model_at(d);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float2 mk = m[k];
+        z[k] = flag ? make_float2(0.f, 0.f) : make_float2(mk.x * pw[k], mk.y * pw[k]);
+      }
+      put(p.out + (n_vis * (1 + d) + v) * NCORR, z);
+    }
   }
 }
 
@@ -2177,6 +2375,9 @@ struct ddsolve_ctx {
 
   std::vector<ChannelBlockStore> cbs;
   DevBuf staging, pack_desc, run_src_dev, run_len_dev;
+  DevBuf predict_in;  // station UVW, sky, frequencies and antennas of a predict
+  DevBuf raw_in;      // DP3-layout interval buffers (ddsolve_set_interval_buffers)
+  DevBuf raw_model;   // the 4-correlation predicted model of one block
 
   // plan
   bool plan_dirty = true;
@@ -2219,6 +2420,7 @@ struct ddsolve_ctx {
   cudaGraphConditionalHandle handle = 0;
   bool graph_ok = false;
   uint64_t last_launches = 0;
+  uint64_t last_predict_launches = 0;  // predict_kernel launches since creation
   // Pinned host staging of the per-call read-backs (error counters, loop
   // state, step magnitudes), copied before the call's single synchronization.
   struct HostStage {
@@ -2428,9 +2630,121 @@ uint32_t LayoutTileRuns(const ddsolve_ctx* ctx, uint32_t R) {
   return ((R + n_tiles - 1) / n_tiles + 3u) & ~3u;
 }
 
-// Uploads the staged reference-layout block and packs it into slabs.
-int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const float* data,
-                  const float* model) {
+// A point-source predict of one regular channel block (predict_kernel).
+struct PredictJob {
+  uint32_t n_times, n_bl, L;
+  const double* freq;  // [L]
+  const double* uvw;   // [n_times][n_ant][3]
+  const uint32_t* a1;  // [n_bl]
+  const uint32_t* a2;
+  const ddsolve_sky_direction* sky;  // [n_dir]
+};
+
+constexpr size_t kPredictMaxSmem = 200 * 1024;
+
+// Host-side checks of a predict job; DDSOLVE_OK or a status with the message.
+int CheckPredictJob(ddsolve_ctx* ctx, const PredictJob& j) {
+  if (!j.freq || !j.uvw || !j.a1 || !j.a2 || !j.sky)
+    return ctx->Fail(DDSOLVE_E_INVALID, "predict: NULL pointer");
+  uint32_t max_src = 0;
+  for (uint32_t d = 0; d < ctx->n_dir; ++d) {
+    if (j.sky[d].n_sources && (!j.sky[d].lmn || !j.sky[d].stokes))
+      return ctx->Fail(DDSOLVE_E_INVALID, "predict: NULL source arrays");
+    max_src = std::max(max_src, j.sky[d].n_sources);
+  }
+  const size_t smem = (size_t(ctx->n_ant) * 3 + size_t(max_src) * 8) * sizeof(double);
+  if (smem > kPredictMaxSmem)
+    return ctx->Fail(DDSOLVE_E_UNSUPPORTED,
+                     "predict: stations x 3 + sources x 8 doubles exceed 200 KiB of shared "
+                     "memory (too many sources in one direction)");
+  for (uint32_t b = 0; b < j.n_bl; ++b)
+    if (j.a1[b] >= ctx->n_ant || j.a2[b] >= ctx->n_ant)
+      return ctx->Fail(DDSOLVE_E_INVALID, "predict: antenna index out of range");
+  return DDSOLVE_OK;
+}
+
+// Uploads the job's inputs and launches predict_kernel into `model` (device
+// memory, [n_dir][n_times * n_bl * L][n_corr]) on the context stream; n_corr
+// is the context's unless n_corr_out (1, 2 or 4) is given.
+int LaunchPredict(ddsolve_ctx* ctx, const PredictJob& j, float2* model, uint32_t n_corr_out = 0) {
+  const uint32_t nc = n_corr_out ? n_corr_out : ctx->n_corr;
+  uint32_t n_src = 0, max_src = 0;
+  std::vector<uint32_t> off(ctx->n_dir + 1, 0);
+  for (uint32_t d = 0; d < ctx->n_dir; ++d) {
+    off[d] = n_src;
+    n_src += j.sky[d].n_sources;
+    max_src = std::max(max_src, j.sky[d].n_sources);
+  }
+  off[ctx->n_dir] = n_src;
+  std::vector<double> src(size_t(n_src) * 8, 0.0);
+  for (uint32_t d = 0; d < ctx->n_dir; ++d)
+    for (uint32_t s = 0; s < j.sky[d].n_sources; ++s) {
+      double* o = &src[(size_t(off[d]) + s) * 8];
+      o[0] = j.sky[d].lmn[3 * s];
+      o[1] = j.sky[d].lmn[3 * s + 1];
+      o[2] = j.sky[d].lmn[3 * s + 2] - 1.0;  // n - 1, as Simulator.cc:486 uses it
+      for (int k = 0; k < 4; ++k) o[3 + k] = j.sky[d].stokes[4 * s + k];
+    }
+  // Evenly spaced channels (to 1e-6 Hz) use the phasor recurrence.
+  double df = j.L > 1 ? (j.freq[j.L - 1] - j.freq[0]) / (j.L - 1) : 0.0;
+  int uniform = j.L > 1;
+  for (uint32_t c = 0; c < j.L && uniform; ++c)
+    uniform = std::abs(j.freq[c] - (j.freq[0] + c * df)) <= 1e-6;
+  auto align = [](size_t x) { return (x + 255) / 256 * 256; };
+  const size_t b_uvw = size_t(j.n_times) * ctx->n_ant * 3 * 8, b_src = src.size() * 8 + 8;
+  const size_t b_off = off.size() * 4, b_f = size_t(j.L) * 8, b_a = size_t(j.n_bl) * 4;
+  const size_t o_src = align(b_uvw), o_off = o_src + align(b_src), o_f = o_off + align(b_off);
+  const size_t o_a1 = o_f + align(b_f), o_a2 = o_a1 + align(b_a), total = o_a2 + align(b_a);
+  DDS_CHECK_CUDA(ctx, ctx->predict_in.Reserve(total));
+  char* base = ctx->predict_in.as<char>();
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base, j.uvw, b_uvw, cudaMemcpyDefault, ctx->stream));
+  if (!src.empty())
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_src, src.data(), src.size() * 8,
+                                        cudaMemcpyHostToDevice, ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_off, off.data(), b_off, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_f, j.freq, b_f, cudaMemcpyDefault, ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_a1, j.a1, b_a, cudaMemcpyDefault, ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_a2, j.a2, b_a, cudaMemcpyDefault, ctx->stream));
+  PredictParams p;
+  p.uvw = reinterpret_cast<const double*>(base);
+  p.src = reinterpret_cast<const double*>(base + o_src);
+  p.src_off = reinterpret_cast<const uint32_t*>(base + o_off);
+  p.freq = reinterpret_cast<const double*>(base + o_f);
+  p.a1 = reinterpret_cast<const uint32_t*>(base + o_a1);
+  p.a2 = reinterpret_cast<const uint32_t*>(base + o_a2);
+  p.model = model;
+  p.n_times = j.n_times;
+  p.n_bl = j.n_bl;
+  p.L = j.L;
+  p.n_ant = ctx->n_ant;
+  p.n_dir = ctx->n_dir;
+  p.max_src = max_src;
+  p.uniform = uniform;
+  p.df = df;
+  const size_t smem = (size_t(ctx->n_ant) * 3 + size_t(max_src) * 8) * sizeof(double);
+  const dim3 grid((j.n_bl + kPredictThreads - 1) / kPredictThreads, j.n_times, ctx->n_dir);
+  const void* fn = nc == 1   ? reinterpret_cast<const void*>(predict_kernel<1>)
+                   : nc == 2 ? reinterpret_cast<const void*>(predict_kernel<2>)
+                             : reinterpret_cast<const void*>(predict_kernel<4>);
+  DDS_CHECK_CUDA(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           int(kPredictMaxSmem)));
+  void* args[] = {&p};
+  DDS_CHECK_CUDA(ctx, cudaLaunchKernel(fn, grid, dim3(kPredictThreads), args, smem,
+                                       ctx->stream));
+  ctx->last_predict_launches += 1;
+  return DDSOLVE_OK;
+}
+
+// Fills the staging buffer of one channel block (reference layout: data
+// [n_vis][n_corr], then model [n_dir][n_vis][n_corr]) on the context stream.
+using StageFn = std::function<int(char* staging)>;
+
+// Stages a block and packs it into slabs. `stage` writes the reference-layout
+// block into the staging buffer: copies of host or device arrays
+// (StageCopy), a copy of the data plus the GPU predict of the model, or the
+// GPU weighting of raw buffers.
+int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const StageFn& stage) {
   const size_t E = ctx->elem_bytes;
   const size_t src_bytes = size_t(cb.n_vis) * E * (1 + ctx->n_dir);
   DDS_CHECK_CUDA(ctx, ctx->staging.Reserve(src_bytes));
@@ -2448,11 +2762,8 @@ int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const float* data,
   DDS_CHECK_CUDA(ctx, ctx->pack_desc.Reserve(ps.size() * sizeof(PackSlab)));
   char* st = ctx->staging.as<char>();
   if (cb.n_vis) {
-    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(st, data, size_t(cb.n_vis) * E,
-                                        cudaMemcpyHostToDevice, ctx->stream));
-    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(st + size_t(cb.n_vis) * E, model,
-                                        size_t(cb.n_vis) * E * ctx->n_dir,
-                                        cudaMemcpyHostToDevice, ctx->stream));
+    const int rc = stage(st);
+    if (rc != DDSOLVE_OK) return rc;
   }
   DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(cb.run_ant_dev.ptr, cb.run_ant.data(),
                                       cb.run_ant.size() * 4,
@@ -2501,6 +2812,28 @@ int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const float* data,
   cb.set = true;
   ctx->powers_dirty = true;
   return DDSOLVE_OK;
+}
+
+// Stager of data and model arrays in the reference layout (host or device).
+StageFn StageCopy(ddsolve_ctx* ctx, const ChannelBlockStore& cb, const float* data,
+                  const float* model) {
+  const size_t n = size_t(cb.n_vis) * ctx->elem_bytes;
+  return [ctx, n, data, model](char* st) {
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(st, data, n, cudaMemcpyDefault, ctx->stream));
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(st + n, model, n * ctx->n_dir, cudaMemcpyDefault,
+                                        ctx->stream));
+    return DDSOLVE_OK;
+  };
+}
+
+// Stager of the data array plus the GPU predict of the model.
+StageFn StagePredict(ddsolve_ctx* ctx, const ChannelBlockStore& cb, const float* data,
+                     const PredictJob& job) {
+  const size_t n = size_t(cb.n_vis) * ctx->elem_bytes;
+  return [ctx, n, data, job](char* st) {
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(st, data, n, cudaMemcpyDefault, ctx->stream));
+    return LaunchPredict(ctx, job, reinterpret_cast<float2*>(st + n));
+  };
 }
 
 constexpr int kPlanNoPipe = -1;  // BuildPipePlan: use the stream_kernel path
@@ -3504,16 +3837,16 @@ uint64_t ddsolve_last_launch_count(const ddsolve_ctx* ctx) {
   return ctx ? ctx->last_launches : 0;
 }
 
-int ddsolve_set_channel_block_regular(ddsolve_ctx* ctx, uint32_t cbi,
-                                      uint32_t n_times, uint32_t n_baselines,
-                                      uint32_t n_channels, const float* data,
-                                      const float* model,
-                                      const uint32_t* antenna1,
-                                      const uint32_t* antenna2) {
+// The regular layout of ddsolve_set_channel_block_regular; `make_stage`
+// returns the stager that fills the block's staging buffer (copies, GPU
+// predict, GPU weighting) once the block's visibility count is set.
+static int SetRegularBlock(ddsolve_ctx* ctx, uint32_t cbi, uint32_t n_times,
+                           uint32_t n_baselines, uint32_t n_channels,
+                           const uint32_t* antenna1, const uint32_t* antenna2,
+                           const std::function<StageFn(const ChannelBlockStore&)>& make_stage) {
   if (!ctx) return DDSOLVE_E_INVALID;
   if (cbi >= ctx->n_cb) return ctx->Fail(DDSOLVE_E_INVALID, "channel block out of range");
-  if (n_times == 0 || n_baselines == 0 || n_channels == 0 || !data || !model ||
-      !antenna1 || !antenna2)
+  if (n_times == 0 || n_baselines == 0 || n_channels == 0 || !antenna1 || !antenna2)
     return ctx->Fail(DDSOLVE_E_INVALID, "empty channel block or NULL pointer");
   for (uint32_t b = 0; b < n_baselines; ++b)
     if (antenna1[b] >= ctx->n_ant || antenna2[b] >= ctx->n_ant ||
@@ -3600,7 +3933,181 @@ int ddsolve_set_channel_block_regular(ddsolve_ctx* ctx, uint32_t cbi,
     t0 = t1;
   }
   cb.n_elems = off;
-  return UploadAndPack(ctx, cb, data, model);
+  return UploadAndPack(ctx, cb, make_stage(cb));
+}
+
+int ddsolve_set_channel_block_regular(ddsolve_ctx* ctx, uint32_t cbi, uint32_t n_times,
+                                      uint32_t n_baselines, uint32_t n_channels,
+                                      const float* data, const float* model,
+                                      const uint32_t* antenna1, const uint32_t* antenna2) {
+  if (ctx && (!data || !model))
+    return ctx->Fail(DDSOLVE_E_INVALID, "empty channel block or NULL pointer");
+  return SetRegularBlock(ctx, cbi, n_times, n_baselines, n_channels, antenna1, antenna2,
+                         [&](const ChannelBlockStore& cb) {
+                           return StageCopy(ctx, cb, data, model);
+                         });
+}
+
+int ddsolve_set_channel_block_regular_sky(ddsolve_ctx* ctx, uint32_t cbi, uint32_t n_times,
+                                          uint32_t n_baselines, uint32_t n_channels,
+                                          const float* data, const double* frequencies,
+                                          const double* station_uvw,
+                                          const uint32_t* antenna1, const uint32_t* antenna2,
+                                          const ddsolve_sky_direction* sky) {
+  if (!ctx) return DDSOLVE_E_INVALID;
+  if (!data) return ctx->Fail(DDSOLVE_E_INVALID, "empty channel block or NULL pointer");
+  const PredictJob job{n_times, n_baselines, n_channels, frequencies, station_uvw,
+                       antenna1, antenna2, sky};
+  const int rc = CheckPredictJob(ctx, job);
+  if (rc != DDSOLVE_OK) return rc;
+  return SetRegularBlock(ctx, cbi, n_times, n_baselines, n_channels, antenna1, antenna2,
+                         [&](const ChannelBlockStore& cb) {
+                           return StagePredict(ctx, cb, data, job);
+                         });
+}
+
+// A device address for a host-or-device input: device memory of the
+// context's device is used in place, host memory is copied into `dst` at
+// byte offset `off` (stream-ordered).
+static int DeviceView(ddsolve_ctx* ctx, const void* src, size_t bytes, DevBuf& dst, size_t off,
+                      const void** out) {
+  cudaPointerAttributes attr{};
+  const bool dev = cudaPointerGetAttributes(&attr, src) == cudaSuccess &&
+                   attr.type == cudaMemoryTypeDevice && attr.device == ctx->device;
+  cudaGetLastError();
+  if (dev) {
+    *out = src;
+    return DDSOLVE_OK;
+  }
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(dst.as<char>() + off, src, bytes, cudaMemcpyDefault,
+                                      ctx->stream));
+  *out = dst.as<char>() + off;
+  return DDSOLVE_OK;
+}
+
+int ddsolve_set_interval_buffers(ddsolve_ctx* ctx, const ddsolve_interval_buffers* in) {
+  if (!ctx) return DDSOLVE_E_INVALID;
+  if (!in || !in->antenna1 || !in->antenna2 || !in->data || !in->weights ||
+      in->n_times == 0 || in->n_baselines == 0 || in->n_channels < ctx->n_cb)
+    return ctx->Fail(DDSOLVE_E_INVALID, "interval buffers: NULL pointer or empty interval");
+  if (!in->model && (!in->sky || !in->frequencies || !in->station_uvw))
+    return ctx->Fail(DDSOLVE_E_INVALID, "interval buffers: no model and no sky to predict it");
+  cudaSetDevice(ctx->device);
+  const uint32_t n_t = in->n_times, n_bl = in->n_baselines, n_ch = in->n_channels;
+  // Cross baselines in buffer order (the regular SolveData constructor's).
+  std::vector<uint32_t> bl_of_cross, a1x, a2x;
+  for (uint32_t b = 0; b < n_bl; ++b) {
+    if (in->antenna1[b] >= ctx->n_ant || in->antenna2[b] >= ctx->n_ant)
+      return ctx->Fail(DDSOLVE_E_INVALID, "interval buffers: antenna index out of range");
+    if (in->antenna1[b] == in->antenna2[b]) continue;
+    bl_of_cross.push_back(b);
+    a1x.push_back(in->antenna1[b]);
+    a2x.push_back(in->antenna2[b]);
+  }
+  const uint32_t n_bx = uint32_t(bl_of_cross.size());
+  if (n_bx == 0) return ctx->Fail(DDSOLVE_E_INVALID, "interval buffers: no cross baselines");
+  const size_t n_raw = size_t(n_t) * n_bl * n_ch;
+  const size_t b_data = n_raw * 32, b_w = n_raw * 16, b_f = in->flags ? n_raw * 4 : 0;
+  const size_t b_m = in->model ? n_raw * 32 * ctx->n_dir : 0;
+  auto align = [](size_t x) { return (x + 255) / 256 * 256; };
+  const size_t o_w = align(b_data), o_f = o_w + align(b_w), o_m = o_f + align(b_f);
+  const size_t o_x = o_m + align(b_m);
+  DDS_CHECK_CUDA(ctx, ctx->raw_in.Reserve(o_x + align(size_t(n_bx) * 4)));
+  const void *d_data = nullptr, *d_w = nullptr, *d_f = nullptr, *d_m = nullptr;
+  int rc;
+  if ((rc = DeviceView(ctx, in->data, b_data, ctx->raw_in, 0, &d_data)) != DDSOLVE_OK) return rc;
+  if ((rc = DeviceView(ctx, in->weights, b_w, ctx->raw_in, o_w, &d_w)) != DDSOLVE_OK) return rc;
+  if (in->flags &&
+      (rc = DeviceView(ctx, in->flags, b_f, ctx->raw_in, o_f, &d_f)) != DDSOLVE_OK)
+    return rc;
+  if (in->model &&
+      (rc = DeviceView(ctx, in->model, b_m, ctx->raw_in, o_m, &d_m)) != DDSOLVE_OK)
+    return rc;
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->raw_in.as<char>() + o_x, bl_of_cross.data(),
+                                      size_t(n_bx) * 4, cudaMemcpyHostToDevice, ctx->stream));
+  const uint32_t* d_x = reinterpret_cast<const uint32_t*>(ctx->raw_in.as<char>() + o_x);
+  for (uint32_t cbi = 0; cbi < ctx->n_cb; ++cbi) {
+    const uint32_t c0 = uint32_t(uint64_t(cbi) * n_ch / ctx->n_cb);
+    const uint32_t L = uint32_t(uint64_t(cbi + 1) * n_ch / ctx->n_cb) - c0;
+    PredictJob job{n_t, n_bx, L, in->frequencies ? in->frequencies + c0 : nullptr,
+                   in->station_uvw, a1x.data(), a2x.data(), in->sky};
+    if (!in->model && (rc = CheckPredictJob(ctx, job)) != DDSOLVE_OK) return rc;
+    rc = SetRegularBlock(ctx, cbi, n_t, n_bx, L, a1x.data(), a2x.data(),
+                         [&](const ChannelBlockStore& cb) -> StageFn {
+                           return [&, c0, L, job](char* st) {
+                             WeighParams p;
+                             p.data = static_cast<const float2*>(d_data);
+                             p.weights = static_cast<const float*>(d_w);
+                             p.flags = static_cast<const uint8_t*>(d_f);
+                             p.model = static_cast<const float2*>(d_m);
+                             p.model_predicted = in->model ? 0 : 1;
+                             if (!in->model) {  // the unweighted 4-correlation model
+                               DDS_CHECK_CUDA(ctx, ctx->raw_model.Reserve(
+                                                       size_t(ctx->n_dir) * cb.n_vis * 32));
+                               const int r2 =
+                                   LaunchPredict(ctx, job, ctx->raw_model.as<float2>(), 4);
+                               if (r2 != DDSOLVE_OK) return r2;
+                               p.model = ctx->raw_model.as<float2>();
+                             }
+                             p.bl_of_cross = d_x;
+                             p.out = reinterpret_cast<float2*>(st);
+                             p.n_times = n_t;
+                             p.n_bl = n_bl;
+                             p.n_ch = n_ch;
+                             p.n_bx = n_bx;
+                             p.c0 = c0;
+                             p.L = L;
+                             p.n_dir = ctx->n_dir;
+                             p.linear = in->linear_weighting ? 1 : 0;
+                             const uint32_t blocks = uint32_t(std::min<uint64_t>(
+                                 (cb.n_vis + 255) / 256, uint64_t(ctx->n_sm) * 16));
+                             if (ctx->n_corr == 1)
+                               weigh_kernel<1><<<blocks, 256, 0, ctx->stream>>>(p);
+                             else if (ctx->n_corr == 2)
+                               weigh_kernel<2><<<blocks, 256, 0, ctx->stream>>>(p);
+                             else
+                               weigh_kernel<4><<<blocks, 256, 0, ctx->stream>>>(p);
+                             DDS_CHECK_CUDA(ctx, cudaGetLastError());
+                             return DDSOLVE_OK;
+                           };
+                         });
+    if (rc != DDSOLVE_OK) return rc;
+  }
+  // The kernels just enqueued read raw_in; returning after them lets the
+  // caller reuse its buffers and keeps raw_in free for the next call.
+  DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return DDSOLVE_OK;
+}
+
+int ddsolve_predict_regular(ddsolve_ctx* ctx, uint32_t n_times, uint32_t n_baselines,
+                            uint32_t n_channels, const double* frequencies,
+                            const double* station_uvw, const uint32_t* antenna1,
+                            const uint32_t* antenna2, const ddsolve_sky_direction* sky,
+                            float* model) {
+  if (!ctx) return DDSOLVE_E_INVALID;
+  if (n_times == 0 || n_baselines == 0 || n_channels == 0 || !model)
+    return ctx->Fail(DDSOLVE_E_INVALID, "predict: empty block or NULL model");
+  const PredictJob job{n_times, n_baselines, n_channels, frequencies, station_uvw,
+                       antenna1, antenna2, sky};
+  int rc = CheckPredictJob(ctx, job);
+  if (rc != DDSOLVE_OK) return rc;
+  cudaSetDevice(ctx->device);
+  const size_t bytes =
+      size_t(ctx->n_dir) * n_times * n_baselines * n_channels * ctx->elem_bytes;
+  cudaPointerAttributes attr{};
+  const bool on_device = cudaPointerGetAttributes(&attr, model) == cudaSuccess &&
+                         attr.type == cudaMemoryTypeDevice && attr.device == ctx->device;
+  cudaGetLastError();  // a host pointer may leave an error state behind
+  float2* out = reinterpret_cast<float2*>(model);
+  if (!on_device) {
+    DDS_CHECK_CUDA(ctx, ctx->staging.Reserve(bytes));
+    out = ctx->staging.as<float2>();
+  }
+  if ((rc = LaunchPredict(ctx, job, out)) != DDSOLVE_OK) return rc;
+  if (!on_device)
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(model, out, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return DDSOLVE_OK;
 }
 
 int ddsolve_set_channel_block(ddsolve_ctx* ctx, uint32_t cbi, uint64_t n_vis,
@@ -3690,7 +4197,7 @@ int ddsolve_set_channel_block(ddsolve_ctx* ctx, uint32_t cbi, uint64_t n_vis,
     cb.run_src.assign(4, 0u);
     cb.run_len.assign(4, 0u);
   }
-  return UploadAndPack(ctx, cb, data, model);
+  return UploadAndPack(ctx, cb, StageCopy(ctx, cb, data, model));
 }
 
 }  // extern "C"

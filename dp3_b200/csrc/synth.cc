@@ -129,6 +129,33 @@ int synth_layout(const synth_config* cfg, double* enu) {
   return 0;
 }
 
+int synth_station_uvw(const synth_config* cfg, double* uvw) {
+  if (!cfg || !uvw) return 1;
+  const synth_config& c = *cfg;
+  const Sky s = MakeSky(c);
+  const double dec = c.dec_deg * kPi / 180.0, lat = c.lat_deg * kPi / 180.0;
+  const double omega = 7.2921150e-5;  // as synth_observe
+  std::vector<double> one;
+  for (uint32_t t = 0; t < c.n_times; ++t) {
+    StationUvw(s.enu, c.n_stations, omega * (c.start_time_s + t * c.time_step_s), dec, lat,
+               one);
+    std::memcpy(uvw + size_t(t) * c.n_stations * 3, one.data(), one.size() * sizeof(double));
+  }
+  return 0;
+}
+
+int synth_sky(const synth_config* cfg, double* lmn, double* flux) {
+  if (!cfg || !lmn || !flux) return 1;
+  const Sky s = MakeSky(*cfg);
+  for (size_t k = 0; k < s.l.size(); ++k) {
+    lmn[3 * k] = s.l[k];
+    lmn[3 * k + 1] = s.m[k];
+    lmn[3 * k + 2] = s.nm1[k] + 1.0;
+    flux[k] = s.flux[k];
+  }
+  return 0;
+}
+
 int synth_frequencies(const synth_config* cfg, double* freqs) {
   if (!cfg || !freqs) return 1;
   const std::vector<double> f = Frequencies(*cfg);

@@ -56,6 +56,14 @@ int synth_layout(const synth_config* cfg, double* enu);
 int synth_gains(const synth_config* cfg, uint64_t seed, double amp_sigma,
                 double delay_sigma_ns, double* gains);
 
+/* Station UVW (m) of each time step, [n_times][n_stations][3] (the UVW
+ * synth_observe uses). */
+int synth_station_uvw(const synth_config* cfg, double* uvw);
+
+/* The point-source sky: lmn [n_directions * n_sources][3] (l, m, n) and the
+ * Stokes I flux [n_directions * n_sources] (Jy), direction-major. */
+int synth_sky(const synth_config* cfg, double* lmn, double* flux);
+
 /* Channel centre frequencies [n_channels]. */
 int synth_frequencies(const synth_config* cfg, double* freqs);
 

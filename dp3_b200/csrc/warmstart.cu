@@ -368,6 +368,255 @@ constexpr size_t GemmSmem() {
   return 2 * size_t(kMTile) * kKChunk * 2 + 2 * size_t(NT) * kKChunk * 2 + 64;
 }
 
+// ---------------------------------------------------------------------------
+// Fused forward pass: all three products of the network in one kernel, one
+// CTA per 128-row tile. Operands live in global memory pre-tiled in the
+// canonical K-major layout of the tensor cores, chunk by chunk:
+//   tiled(r, k) = (((k / 64) * (R / 8) + r / 8) * 8 + (k % 64) / 8) * 64
+//                 + (r % 8) * 8 + k % 8        (BF16 elements, R rows)
+// so that one K-chunk of a 128-row tile (16 KB) or of a whole weight matrix
+// (N x 64, N * 128 bytes) is one contiguous block that a single bulk copy
+// (cp.async.bulk, no multicast) moves into shared memory in the layout the
+// MMA descriptors read. One thread of warp 4 streams the chunks of all three
+// layers through a 3-stage ring (layer 1: the input tile and W1; layers 2
+// and 3: W2 and W3) and issues tcgen05.mma (M = 128, K = 16) into tensor
+// memory: layer 1 at columns 0.., layer 2 at 256.., layer 3 at 0.. again.
+// Warps 0-3 run the epilogues: each reads its 32 accumulator lanes
+// (tcgen05.ld), adds the bias, applies the ReLU and writes the BF16 hidden
+// activations into shared memory in the canonical layout, where the next
+// layer's MMAs read them as their A operand; the last epilogue writes the
+// FP32 output. Every wait is bounded (kWaitNs) and sets the error flag.
+// ---------------------------------------------------------------------------
+constexpr int kFusedThreads = 160;  // warps 0-3 epilogue, warp 4 producer / MMA
+constexpr int kFusedStages = 3;
+constexpr uint32_t kFusedABytes = kMTile * kKChunk * 2;                 // 16 KB input chunk
+constexpr uint32_t kFusedStageBytes = kFusedABytes + 256 * kKChunk * 2;  // + 32 KB weights
+constexpr uint32_t kFusedHBytes = kMTile * 256 * 2;                     // 64 KB hidden tile
+constexpr size_t kFusedSmem = size_t(kFusedStages) * kFusedStageBytes + kFusedHBytes + 128;
+
+__host__ __device__ inline size_t TiledIndex(uint32_t r, uint32_t k, uint32_t rows) {
+  return ((size_t(k / 64) * (rows / 8) + r / 8) * 8 + (k % 64) / 8) * 64 + (r % 8) * 8 + k % 8;
+}
+
+// The first `rows` rows of a row-major BF16 [..][ld] matrix -> a tiled one of
+// layout_rows rows (layout_rows >= rows, a multiple of 8; ld of 64).
+__global__ void tile_kernel(const uint16_t* __restrict__ src, uint32_t rows, uint32_t ld,
+                            uint16_t* __restrict__ dst, uint32_t layout_rows) {
+  const size_t total = size_t(rows) * ld;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += size_t(gridDim.x) * blockDim.x) {
+    const uint32_t r = uint32_t(i / ld), k = uint32_t(i % ld);
+    dst[TiledIndex(r, k, layout_rows)] = src[i];
+  }
+}
+
+struct FusedParams {
+  const uint16_t* xt;   // input, tiled with rows_pad rows, k1_chunks * 64 columns
+  const uint16_t* w1t;  // [dh][k1 * 64] tiled
+  const uint16_t* w2t;  // [dh][dh] tiled
+  const uint16_t* w3t;  // [dout][dh] tiled
+  const float* b1;
+  const float* b2;
+  const float* b3;
+  float* y;  // [M][dout]
+  unsigned int* error;
+  uint32_t rows_pad, M, k1_chunks, dh, dout;
+};
+
+__device__ __forceinline__ void FusedBulkCopy(void* dst, const void* src, uint32_t bytes,
+                                              uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(SmemAddr(dst)),
+      "l"(src), "r"(bytes), "r"(SmemAddr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void MbarArrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(SmemAddr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void FusedExpectTx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(SmemAddr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__global__ void __launch_bounds__(kFusedThreads, 1) mlp_forward_kernel(const FusedParams p) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* stages = smem;
+  unsigned char* hbuf = smem + size_t(kFusedStages) * kFusedStageBytes;
+  uint64_t* full = reinterpret_cast<uint64_t*>(hbuf + kFusedHBytes);
+  uint64_t* empty = full + kFusedStages;
+  uint64_t* done = empty + kFusedStages;  // one phase per layer's MMAs
+  uint64_t* hready = done + 1;            // one phase per hidden tile written
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(hready + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t tile = blockIdx.x;
+  const uint32_t h_chunks = p.dh / kKChunk;
+  const uint32_t n_steps = p.k1_chunks + 2 * h_chunks;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     SmemAddr(tmem_slot)),
+                 "r"(512u)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 128) {
+    for (int s = 0; s < kFusedStages; ++s) {
+      MbarInit(&full[s], 1);
+      MbarInit(&empty[s], 1);
+    }
+    MbarInit(done, 1);
+    MbarInit(hready, 128);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 4) {
+    if (lane == 0) {
+      // Step j: layer 1 chunks 0..k1-1, then layer 2 and layer 3 chunks.
+      auto issue = [&](uint32_t j) {
+        unsigned char* st = stages + size_t(j % kFusedStages) * kFusedStageBytes;
+        uint64_t* bar = &full[j % kFusedStages];
+        if (j < p.k1_chunks) {
+          const uint32_t wb = p.dh * kKChunk * 2;
+          FusedExpectTx(bar, kFusedABytes + wb);
+          // 8-row group g of chunk j starts at element (j * rows_pad / 8 + g) * 512
+          FusedBulkCopy(st, p.xt + (size_t(j) * (p.rows_pad / 8) + 16 * tile) * 512,
+                        kFusedABytes, bar);
+          FusedBulkCopy(st + kFusedABytes, p.w1t + size_t(j) * p.dh * kKChunk, wb, bar);
+        } else if (j < p.k1_chunks + h_chunks) {
+          const uint32_t c = j - p.k1_chunks, wb = p.dh * kKChunk * 2;
+          FusedExpectTx(bar, wb);
+          FusedBulkCopy(st + kFusedABytes, p.w2t + size_t(c) * p.dh * kKChunk, wb, bar);
+        } else {
+          const uint32_t c = j - p.k1_chunks - h_chunks, wb = p.dout * kKChunk * 2;
+          FusedExpectTx(bar, wb);
+          FusedBulkCopy(st + kFusedABytes, p.w3t + size_t(c) * p.dout * kKChunk, wb, bar);
+        }
+      };
+      for (uint32_t j = 0; j < n_steps && j < uint32_t(kFusedStages); ++j) issue(j);
+      bool ok = true;
+      for (uint32_t i = 0; i < n_steps && ok; ++i) {
+        const uint32_t layer = i < p.k1_chunks ? 1u : (i < p.k1_chunks + h_chunks ? 2u : 3u);
+        const uint32_t c = layer == 1 ? i : (layer == 2 ? i - p.k1_chunks
+                                                        : i - p.k1_chunks - h_chunks);
+        const uint32_t n_chunks = layer == 1 ? p.k1_chunks : h_chunks;
+        if (layer > 1 && c == 0) ok = MbarWait(hready, layer - 2, p.error);
+        ok = ok && MbarWait(&full[i % kFusedStages], (i / kFusedStages) & 1u, p.error);
+        if (!ok) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const unsigned char* st = stages + size_t(i % kFusedStages) * kFusedStageBytes;
+        const uint32_t a_addr = layer == 1 ? SmemAddr(st) : SmemAddr(hbuf) + c * kFusedABytes;
+        const uint32_t b_addr = SmemAddr(st + kFusedABytes);
+        const uint32_t d = tmem + (layer == 2 ? 256u : 0u);
+        const uint32_t idesc = InstrDesc(kMTile, int(layer == 3 ? p.dout : p.dh));
+#pragma unroll
+        for (int s = 0; s < kKChunk / 16; ++s) {
+          const uint64_t ad = SmemDesc(a_addr + s * 256, 128, 1024);
+          const uint64_t bd = SmemDesc(b_addr + s * 256, 128, 1024);
+          const uint32_t acc = (c > 0 || s > 0) ? 1u : 0u;
+          asm volatile(
+              "{\n .reg .pred p;\n"
+              " setp.ne.b32 p, %4, 0;\n"
+              " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+              "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+              : "memory");
+        }
+        asm volatile(
+            "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                SmemAddr(&empty[i % kFusedStages]))
+            : "memory");
+        if (c + 1 == n_chunks)
+          asm volatile(
+              "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                  SmemAddr(done))
+              : "memory");
+        if (i + kFusedStages < n_steps) {
+          ok = MbarWait(&empty[i % kFusedStages], (i / kFusedStages) & 1u, p.error);
+          if (ok) issue(i + kFusedStages);
+        }
+      }
+      // Before returning (also after a timeout): the MMAs already issued
+      // have finished, so that tensor memory can be freed.
+      for (uint32_t i = n_steps > kFusedStages ? n_steps - kFusedStages : 0; i < n_steps; ++i)
+        MbarWait(&empty[i % kFusedStages], (i / kFusedStages) & 1u, p.error);
+    }
+    __syncwarp();
+  } else {
+    // Epilogues: warp w owns accumulator lanes / tile rows 32w .. 32w + 31.
+    const uint32_t row_in = uint32_t(warp * 32 + lane);
+    const uint32_t row = tile * kMTile + row_in;
+    for (uint32_t layer = 1; layer <= 3; ++layer) {
+      if (!MbarWait(done, (layer - 1) & 1u, p.error)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t ncols = layer == 3 ? p.dout : p.dh;
+      const float* bias = layer == 1 ? p.b1 : (layer == 2 ? p.b2 : p.b3);
+      const uint32_t base = layer == 2 ? 256u : 0u;
+      for (uint32_t col = 0; col < ncols; col += 32) {
+        __syncwarp();
+        uint32_t r[32];
+        const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + base + col;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
+            "%10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, "
+            "%26, %27, %28, %29, %30, %31}, [%32];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+              "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+              "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]),
+              "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+              "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
+              "=r"(r[30]), "=r"(r[31])
+            : "r"(taddr)
+            : "memory");
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        float v[32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]) + __ldg(bias + col + j);
+        if (layer < 3) {
+          // BF16 ReLU activations into the canonical layout of the next A.
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            uint4 w;
+            const int j = q * 8;
+            w.x = uint32_t(ToBf16(fmaxf(v[j], 0.f))) |
+                  (uint32_t(ToBf16(fmaxf(v[j + 1], 0.f))) << 16);
+            w.y = uint32_t(ToBf16(fmaxf(v[j + 2], 0.f))) |
+                  (uint32_t(ToBf16(fmaxf(v[j + 3], 0.f))) << 16);
+            w.z = uint32_t(ToBf16(fmaxf(v[j + 4], 0.f))) |
+                  (uint32_t(ToBf16(fmaxf(v[j + 5], 0.f))) << 16);
+            w.w = uint32_t(ToBf16(fmaxf(v[j + 6], 0.f))) |
+                  (uint32_t(ToBf16(fmaxf(v[j + 7], 0.f))) << 16);
+            const uint32_t k = col + uint32_t(j);
+            *reinterpret_cast<uint4*>(hbuf + TiledIndex(row_in, k, kMTile) * 2) = w;
+          }
+        } else if (row < p.M) {
+          float* out = p.y + size_t(row) * p.dout + col;
+#pragma unroll
+          for (int j = 0; j < 32; j += 4)
+            *reinterpret_cast<float4*>(out + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+        }
+      }
+      if (layer < 3) {
+        // generic-proxy writes -> visible to the tensor core; TMEM reads done
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        MbarArrive(hready);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u)
+                 : "memory");
+}
+
 // x fp32 [n][n_in] (rows idx[i] if idx) -> bf16 [n][ld] zero-padded; target
 // fp32 [n][n_out] -> fp32 [n][ld_t] zero-padded.
 __global__ void gather_rows_kernel(const float* __restrict__ x, uint32_t n_in, const uint32_t* idx,
@@ -471,11 +720,12 @@ struct SetPtrs {
 
 // Network samples from solution sets (see ddwarm_features); one thread per
 // (row, value, set >= 1). Writes FP32 features (x32, ld = n_feat) and / or
-// BF16 features (xb, ld = ldb).
+// BF16 features (xb: row-major with ld = ldb, or, with tiled_rows > 0, in the
+// tiled layout of the fused forward pass with tiled_rows rows).
 __global__ void features_kernel(const SetPtrs sets, uint32_t n_sets, uint32_t n_cb,
                                 uint32_t n_ant, uint32_t n_sub, uint32_t n_pol, double scale,
                                 float* __restrict__ x32, uint16_t* __restrict__ xb,
-                                uint32_t ldb) {
+                                uint32_t ldb, uint32_t tiled_rows) {
   const uint32_t w_n = n_cb * n_pol;
   const uint32_t rows = n_ant * n_sub;
   const size_t total = size_t(rows) * w_n * (n_sets - 1);
@@ -503,8 +753,11 @@ __global__ void features_kernel(const SetPtrs sets, uint32_t n_sets, uint32_t n_
       x32[size_t(row) * n_feat + c + w_n] = float(scale * lim);
     }
     if (xb) {
-      xb[size_t(row) * ldb + c] = ToBf16(float(scale * lre));
-      xb[size_t(row) * ldb + c + w_n] = ToBf16(float(scale * lim));
+      const size_t i0 = tiled_rows ? TiledIndex(row, c, tiled_rows) : size_t(row) * ldb + c;
+      const size_t i1 =
+          tiled_rows ? TiledIndex(row, c + w_n, tiled_rows) : size_t(row) * ldb + c + w_n;
+      xb[i0] = ToBf16(float(scale * lre));
+      xb[i1] = ToBf16(float(scale * lim));
     }
   }
 }
@@ -567,6 +820,7 @@ uint32_t RoundUp(uint32_t x, uint32_t m) { return (x + m - 1) / m * m; }
 struct Layer {
   uint32_t out, in, rows, ld;  // logical out/in, padded rows (out) and ld (in)
   DevBuf w, b, gw, gb, mw, vw, mb, vb, wb;
+  DevBuf wt;  // wb in the tiled layout of the fused forward pass
 };
 
 struct ddwarm_ctx {
@@ -585,6 +839,10 @@ struct ddwarm_ctx {
   uint32_t xb_zero_rows = 0;
   DevBuf xb, h1, h2, y, t, dy, dz2, dz1, partial, loss, error;
   DevBuf sets, start, x32;  // warm-start features / predictions
+  // fused forward pass: the input in the tiled layout, rows padded to 128;
+  // xt_zero_rows as xb_zero_rows (features_kernel writes feature columns only)
+  DevBuf xt;
+  uint32_t xt_rows = 0, xt_zero_rows = 0;
   // training data set
   DevBuf ds_x, ds_t, ds_idx;
 
@@ -674,6 +932,52 @@ int Forward(ddwarm_ctx* ctx, uint32_t n) {
     return rc;
   return Gemm(ctx, ctx->h2.as<uint16_t>(), ctx->dh, 0, l3.wb.as<uint16_t>(), l3.ld, 0, n,
               ctx->dout, ctx->dh, ctx->y.ptr, ctx->dout, l3.b.as<float>(), nullptr, kEpiF32);
+}
+
+// Tiled input buffer of the fused forward pass for `rows` rows (padded to
+// whole 128-row tiles).
+int ReserveTiled(ddwarm_ctx* ctx, uint32_t rows) {
+  const uint32_t r = RoundUp(std::max<uint32_t>(rows, 1), kMTile);
+  if (r <= ctx->xt_rows) return 0;
+  WARM_CHECK(ctx, ctx->xt.Reserve(size_t(r) * ctx->di * 2));
+  ctx->xt_rows = r;
+  ctx->xt_zero_rows = 0;  // new memory
+  return 0;
+}
+
+// The BF16 weights in the tiled layout of the fused forward pass (after
+// every change of the weights that inference will use).
+int RefreshTiled(ddwarm_ctx* ctx) {
+  for (Layer& l : ctx->L) {
+    WARM_CHECK(ctx, l.wt.Reserve(size_t(l.rows) * l.ld * 2));
+    tile_kernel<<<64, 256, 0, ctx->stream>>>(l.wb.as<uint16_t>(), l.rows, l.ld,
+                                             l.wt.as<uint16_t>(), l.rows);
+  }
+  WARM_CHECK(ctx, cudaGetLastError());
+  return 0;
+}
+
+// Forward pass on the first n rows of ctx->xt (tiled input): y (FP32), one
+// launch of mlp_forward_kernel.
+int ForwardFused(ddwarm_ctx* ctx, uint32_t n) {
+  FusedParams p;
+  p.xt = ctx->xt.as<uint16_t>();
+  p.w1t = ctx->L[0].wt.as<uint16_t>();
+  p.w2t = ctx->L[1].wt.as<uint16_t>();
+  p.w3t = ctx->L[2].wt.as<uint16_t>();
+  p.b1 = ctx->L[0].b.as<float>();
+  p.b2 = ctx->L[1].b.as<float>();
+  p.b3 = ctx->L[2].b.as<float>();
+  p.y = ctx->y.as<float>();
+  p.error = ctx->error.as<unsigned int>();
+  p.rows_pad = ctx->xt_rows;
+  p.M = n;
+  p.k1_chunks = ctx->di / kKChunk;
+  p.dh = ctx->dh;
+  p.dout = ctx->dout;
+  mlp_forward_kernel<<<(n + kMTile - 1) / kMTile, kFusedThreads, kFusedSmem, ctx->stream>>>(p);
+  WARM_CHECK(ctx, cudaGetLastError());
+  return 0;
 }
 
 // Loss and gradients for the first n rows of xb / t (after Forward).
@@ -787,6 +1091,7 @@ int CopyParams(ddwarm_ctx* ctx, float* host, bool to_host, bool grads) {
       WARM_CHECK(ctx, cudaGetLastError());
     }
   }
+  if (!to_host && !grads) return RefreshTiled(ctx);
   return 0;
 }
 
@@ -836,7 +1141,9 @@ int ddwarm_create(uint32_t n_in, uint32_t n_hidden, uint32_t n_out, uint64_t see
   if (cudaFuncSetAttribute(gemm_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            int(GemmSmem<256>())) != cudaSuccess ||
       cudaFuncSetAttribute(gemm_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           int(GemmSmem<64>())) != cudaSuccess)
+                           int(GemmSmem<64>())) != cudaSuccess ||
+      cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           int(kFusedSmem)) != cudaSuccess)
     return fail(2);
   std::mt19937_64 rng(seed);
   for (int i = 0; i < 3; ++i) {
@@ -917,7 +1224,12 @@ int ddwarm_predict(ddwarm_ctx* ctx, uint32_t n, const float* x, float* y) {
                                                  ctx->xb.as<uint16_t>(), ctx->di, nullptr, 0,
                                                  nullptr, 0);
   WARM_CHECK(ctx, cudaGetLastError());
-  if ((rc = Forward(ctx, n))) return rc;
+  // The fused forward pass (one launch): the input rows tiled first.
+  if ((rc = ReserveTiled(ctx, n))) return rc;
+  tile_kernel<<<64, 256, 0, ctx->stream>>>(ctx->xb.as<uint16_t>(), n, ctx->di,
+                                           ctx->xt.as<uint16_t>(), ctx->xt_rows);
+  WARM_CHECK(ctx, cudaGetLastError());
+  if ((rc = ForwardFused(ctx, n))) return rc;
   std::vector<float> tmp(size_t(n) * ctx->dout);
   WARM_CHECK(ctx, cudaMemcpyAsync(tmp.data(), ctx->y.ptr, tmp.size() * 4, cudaMemcpyDeviceToHost,
                                   ctx->stream));
@@ -1048,6 +1360,7 @@ int ddwarm_train(ddwarm_ctx* ctx, uint32_t n, const float* x, const float* targe
       if ((rc = AdamStep(ctx, lr))) return rc;
     }
   }
+  if ((rc = RefreshTiled(ctx))) return rc;  // the trained weights for inference
   if ((rc = CheckError(ctx))) return rc;
   if (epoch_loss && epochs) {
     std::vector<float> l(size_t(epochs) * steps_per_epoch);
@@ -1110,7 +1423,8 @@ int ddwarm_features(ddwarm_ctx* ctx, const ddwarm_layout* lay, uint32_t n_sets,
   WARM_CHECK(ctx, ctx->x32.Reserve(rows * n_feat * 4));
   features_kernel<<<256, 256, 0, ctx->stream>>>(sp, n_sets, lay->n_channel_blocks,
                                                 lay->n_antennas, lay->n_sub, lay->n_pol,
-                                                lay->scale, ctx->x32.as<float>(), nullptr, 0);
+                                                lay->scale, ctx->x32.as<float>(), nullptr, 0,
+                                                0);
   WARM_CHECK(ctx, cudaGetLastError());
   WARM_CHECK(ctx, cudaMemcpyAsync(x, ctx->x32.ptr, rows * n_feat * 4, cudaMemcpyDefault,
                                   ctx->stream));
@@ -1131,16 +1445,17 @@ int ddwarm_predict_start(ddwarm_ctx* ctx, const ddwarm_layout* lay, uint32_t n_s
   if ((rc = Reserve(ctx, rows))) return rc;
   SetPtrs sp{};
   if ((rc = ResolveSets(ctx, lay, n_sets, sets, &sp, &n_sol))) return rc;
-  if (rows > ctx->xb_zero_rows) {  // zero padding once per allocation
-    WARM_CHECK(ctx, cudaMemsetAsync(ctx->xb.ptr, 0, size_t(rows) * ctx->di * 2, ctx->stream));
-    ctx->xb_zero_rows = rows;
+  if ((rc = ReserveTiled(ctx, rows))) return rc;
+  if (rows > ctx->xt_zero_rows) {  // zero padding once per allocation
+    WARM_CHECK(ctx, cudaMemsetAsync(ctx->xt.ptr, 0, ctx->xt.bytes, ctx->stream));
+    ctx->xt_zero_rows = ctx->xt_rows;
   }
   features_kernel<<<256, 256, 0, ctx->stream>>>(sp, n_sets, lay->n_channel_blocks,
                                                 lay->n_antennas, lay->n_sub, lay->n_pol,
-                                                lay->scale, nullptr, ctx->xb.as<uint16_t>(),
-                                                ctx->di);
+                                                lay->scale, nullptr, ctx->xt.as<uint16_t>(),
+                                                0, ctx->xt_rows);
   WARM_CHECK(ctx, cudaGetLastError());
-  if ((rc = Forward(ctx, rows))) return rc;
+  if ((rc = ForwardFused(ctx, rows))) return rc;
   cudaPointerAttributes attr{};
   const bool dev_out = cudaPointerGetAttributes(&attr, start) == cudaSuccess &&
                        (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged) &&

@@ -25,6 +25,8 @@ EXPORTED_SYMBOLS = (
     "ddsolve_last_launch_count", "ddsolve_perform_iteration_noalloc",
     "ddsolve_perform_iterations", "ddsolve_get_tuning", "ddsolve_set_plan_tuning",
     "ddsolve_autotune", "ddsolve_set_intervals", "ddsolve_solve_batch",
+    "ddsolve_set_channel_block_regular_sky", "ddsolve_predict_regular",
+    "ddsolve_set_interval_buffers",
 )
 
 
@@ -91,6 +93,10 @@ def lib():
         L.ddsolve_set_channel_block.argtypes = [vp, u32, u64, vp, vp, vp, vp]
         L.ddsolve_set_channel_block_regular.argtypes = [vp, u32, u32, u32, u32,
                                                         vp, vp, vp, vp]
+        L.ddsolve_set_channel_block_regular_sky.argtypes = [vp, u32, u32, u32, u32, vp, vp,
+                                                            vp, vp, vp, vp]
+        L.ddsolve_predict_regular.argtypes = [vp, u32, u32, u32, vp, vp, vp, vp, vp, vp]
+        L.ddsolve_set_interval_buffers.argtypes = [vp, vp]
         L.ddsolve_solve.argtypes = [vp, vp, ctypes.POINTER(Result), vp]
         L.ddsolve_perform_iteration.argtypes = [vp, vp, vp]
         L.ddsolve_perform_iterations.argtypes = [vp, vp, u32, vp]
@@ -128,6 +134,36 @@ def _addr(a):
 
 def _is_torch(a):
     return hasattr(a, "data_ptr") and hasattr(a, "is_cuda")
+
+
+class SkyDirection(ctypes.Structure):
+    """ddsolve_sky_direction (include/ddsolve_b200.h)."""
+    _fields_ = [("n_sources", ctypes.c_uint32), ("lmn", ctypes.c_void_p),
+                ("stokes", ctypes.c_void_p)]
+
+
+class IntervalBuffers(ctypes.Structure):
+    """ddsolve_interval_buffers (include/ddsolve_b200.h)."""
+    _fields_ = [("n_times", ctypes.c_uint32), ("n_baselines", ctypes.c_uint32),
+                ("n_channels", ctypes.c_uint32), ("antenna1", ctypes.c_void_p),
+                ("antenna2", ctypes.c_void_p), ("data", ctypes.c_void_p),
+                ("weights", ctypes.c_void_p), ("flags", ctypes.c_void_p),
+                ("model", ctypes.c_void_p), ("frequencies", ctypes.c_void_p),
+                ("station_uvw", ctypes.c_void_p), ("sky", ctypes.c_void_p),
+                ("linear_weighting", ctypes.c_int32)]
+
+
+def _sky_struct(sky):
+    """ddsolve_sky_direction array of [(lmn [n][3], stokes [n][4]), ...]."""
+    keep = []
+    arr = (SkyDirection * len(sky))()
+    for d, (lmn, stokes) in enumerate(sky):
+        lmn = np.ascontiguousarray(lmn, np.float64).reshape(-1, 3)
+        stokes = np.ascontiguousarray(stokes, np.float64).reshape(-1, 4)
+        assert lmn.shape[0] == stokes.shape[0]
+        keep += [lmn, stokes]
+        arr[d] = SkyDirection(lmn.shape[0], lmn.ctypes.data, stokes.ctypes.data)
+    return arr, keep
 
 
 class Context:
@@ -222,6 +258,78 @@ class Context:
             self._h, cb, n_times, n_baselines, n_channels, _ptr_any(data),
             _ptr_any(model), _addr(a1), _addr(a2)),
             "ddsolve_set_channel_block_regular")
+
+    def set_channel_block_regular_sky(self, cb, n_times, n_baselines, data, frequencies,
+                                      station_uvw, antenna1, antenna2, sky):
+        """ddsolve_set_channel_block_regular_sky: the model predicted on the
+        GPU from `sky` (per direction (lmn [n][3], stokes [n][4])) at this
+        block's `frequencies`; only `data` is uploaded."""
+        freqs = np.ascontiguousarray(frequencies, np.float64)
+        uvw = np.ascontiguousarray(station_uvw, np.float64)
+        a1 = np.ascontiguousarray(antenna1, dtype=np.uint32)
+        a2 = np.ascontiguousarray(antenna2, dtype=np.uint32)
+        sky_arr, keep = _sky_struct(sky)
+        data = _host_buffer(data)
+        self._keep[cb] = (data,)
+        self._check(lib().ddsolve_set_channel_block_regular_sky(
+            self._h, cb, n_times, n_baselines, len(freqs), _ptr_any(data), _addr(freqs),
+            _addr(uvw), _addr(a1), _addr(a2), ctypes.cast(sky_arr, ctypes.c_void_p)),
+            "ddsolve_set_channel_block_regular_sky")
+
+    def predict_regular(self, n_times, n_baselines, frequencies, station_uvw, antenna1,
+                        antenna2, sky, out=None):
+        """ddsolve_predict_regular: model [n_dir][n_times * n_baselines *
+        n_channels][n_corr][2] float32 (numpy, or `out`: a contiguous
+        float32 torch tensor on the context's GPU)."""
+        freqs = np.ascontiguousarray(frequencies, np.float64)
+        uvw = np.ascontiguousarray(station_uvw, np.float64)
+        a1 = np.ascontiguousarray(antenna1, dtype=np.uint32)
+        a2 = np.ascontiguousarray(antenna2, dtype=np.uint32)
+        sky_arr, keep = _sky_struct(sky)
+        n_vis = n_times * n_baselines * len(freqs)
+        if out is None:
+            out = np.zeros((len(sky), n_vis, self.n_correlations, 2), np.float32)
+        self._check(lib().ddsolve_predict_regular(
+            self._h, n_times, n_baselines, len(freqs), _addr(freqs), _addr(uvw), _addr(a1),
+            _addr(a2), ctypes.cast(sky_arr, ctypes.c_void_p), _ptr_any(out)),
+            "ddsolve_predict_regular")
+        return out
+
+    def set_interval_buffers(self, antenna1, antenna2, data, weights, flags=None, model=None,
+                             frequencies=None, station_uvw=None, sky=None,
+                             linear_weighting=False):
+        """ddsolve_set_interval_buffers: one interval in DP3's buffer layout
+        (data complex64 [n_t][n_bl][n_ch][4], weights float32 [..][4], flags
+        uint8 [..][4] or None, model complex64 [n_dir][n_t][n_bl][n_ch][4] or
+        None with frequencies / station_uvw / sky to predict it)."""
+        data = np.ascontiguousarray(data, np.complex64)
+        weights = np.ascontiguousarray(weights, np.float32)
+        n_t, n_bl, n_ch, _ = data.shape
+        a1 = np.ascontiguousarray(antenna1, dtype=np.uint32)
+        a2 = np.ascontiguousarray(antenna2, dtype=np.uint32)
+        keep = [data, weights, a1, a2]
+        ib = IntervalBuffers()
+        ib.n_times, ib.n_baselines, ib.n_channels = n_t, n_bl, n_ch
+        ib.antenna1, ib.antenna2 = a1.ctypes.data, a2.ctypes.data
+        ib.data, ib.weights = data.ctypes.data, weights.ctypes.data
+        if flags is not None:
+            flags = np.ascontiguousarray(flags, np.uint8)
+            keep.append(flags)
+            ib.flags = flags.ctypes.data
+        if model is not None:
+            model = np.ascontiguousarray(model, np.complex64)
+            keep.append(model)
+            ib.model = model.ctypes.data
+        else:
+            freqs = np.ascontiguousarray(frequencies, np.float64)
+            uvw = np.ascontiguousarray(station_uvw, np.float64)
+            sky_arr, sk = _sky_struct(sky)
+            keep += [freqs, uvw, sky_arr, sk]
+            ib.frequencies, ib.station_uvw = freqs.ctypes.data, uvw.ctypes.data
+            ib.sky = ctypes.cast(sky_arr, ctypes.c_void_p).value
+        ib.linear_weighting = int(linear_weighting)
+        self._check(lib().ddsolve_set_interval_buffers(self._h, ctypes.byref(ib)),
+                    "ddsolve_set_interval_buffers")
 
     def solve(self, solutions, step_magnitudes=None):
         """solutions: complex128 [n_cb, n_ant, n_sub, n_pol], updated in place

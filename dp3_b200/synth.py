@@ -186,6 +186,35 @@ def frequencies(cfg: ObservationConfig):
     return f
 
 
+def station_uvw(cfg: ObservationConfig, start_time_s=0.0):
+    """Station UVW (m) per time step [n_times][n_stations][3], as observe()
+    uses them for an interval starting at start_time_s."""
+    c = cfg.c_config(start_time_s)
+    uvw = np.zeros((cfg.n_times, cfg.n_stations, 3), np.float64)
+    if lib().synth_station_uvw(ctypes.byref(c), ctypes.c_void_p(uvw.ctypes.data)) != 0:
+        raise RuntimeError("synth_station_uvw failed")
+    return uvw
+
+
+def sky(cfg: ObservationConfig):
+    """The point-source sky of cfg: per direction (lmn [n_sources][3], Stokes
+    [n_sources][4] with I = the flux, Q = U = V = 0)."""
+    c = cfg.c_config()
+    n = cfg.n_directions * cfg.n_sources
+    lmn = np.zeros((n, 3), np.float64)
+    flux = np.zeros(n, np.float64)
+    if lib().synth_sky(ctypes.byref(c), ctypes.c_void_p(lmn.ctypes.data),
+                       ctypes.c_void_p(flux.ctypes.data)) != 0:
+        raise RuntimeError("synth_sky failed")
+    out = []
+    for d in range(cfg.n_directions):
+        sl = slice(d * cfg.n_sources, (d + 1) * cfg.n_sources)
+        st = np.zeros((cfg.n_sources, 4), np.float64)
+        st[:, 0] = flux[sl]
+        out.append((np.ascontiguousarray(lmn[sl]), st))
+    return out
+
+
 def gain_sequence(cfg: ObservationConfig, n_intervals, seed=None, phase_sigma=0.05,
                   amp_sigma=0.01, dispersive_sigma=0.05):
     """True gains of `n_intervals` consecutive solution intervals,

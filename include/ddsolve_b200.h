@@ -116,9 +116,10 @@ DDSOLVE_API int ddsolve_set_settings(ddsolve_ctx* ctx, const ddsolve_settings* s
  * (replaces reading SolveData<V>::ChannelBlockData, SolveData.h:31-133, inside
  * IterativeDiagonalSolver::Solve). Any visibility order and antenna/solution
  * assignment is accepted (regular and BDA data); consecutive visibilities
- * that share antennas and solution indices are solved together. Host pointers;
- * pinned memory makes the copy asynchronous. Replaces any previous data of
- * that channel block. */
+ * that share antennas and solution indices are solved together. data and
+ * model may be host memory (pinned memory makes the copy asynchronous) or
+ * device memory of the context's device; antenna_pairs and solution_map are
+ * host memory. Replaces any previous data of that channel block. */
 DDSOLVE_API int ddsolve_set_channel_block(ddsolve_ctx* ctx, uint32_t channel_block,
                               uint64_t n_vis, const float* data,
                               const float* model,
@@ -130,13 +131,90 @@ DDSOLVE_API int ddsolve_set_channel_block(ddsolve_ctx* ctx, uint32_t channel_blo
  * ((t * n_baselines) + b) * n_channels + c, baseline b between antenna1[b] and
  * antenna2[b] (autocorrelations already removed), solution index of direction
  * d at time t = t * min(n_sol[d], n_times) / n_times + first solution of d.
- * No per-visibility antenna / solution arrays are read. */
+ * No per-visibility antenna / solution arrays are read. data and model as in
+ * ddsolve_set_channel_block (host or device memory); antenna1 / antenna2 are
+ * host memory. */
 DDSOLVE_API int ddsolve_set_channel_block_regular(ddsolve_ctx* ctx, uint32_t channel_block,
                                       uint32_t n_times, uint32_t n_baselines,
                                       uint32_t n_channels, const float* data,
                                       const float* model,
                                       const uint32_t* antenna1,
                                       const uint32_t* antenna2);
+
+/* Point sources of one direction: DP3's PointSource (base/PointSource.h)
+ * with a flat spectrum (Stokes I, Q, U, V independent of frequency). */
+typedef struct {
+  uint32_t n_sources;
+  const double* lmn;    /* [n_sources][3]: l, m, n of each source relative to
+                           the phase centre (as DP3's radec2lmn gives them) */
+  const double* stokes; /* [n_sources][4]: I, Q, U, V in Jy */
+} ddsolve_sky_direction;
+
+/* ddsolve_set_channel_block_regular with the model visibilities predicted
+ * on the GPU instead of uploaded: replaces DDECal's per-direction predict of
+ * point sources (steps/OnePredict.cc -> base/Simulator.cc:112-245
+ * visit(PointSource), station phases :477-520, spectrum :522-547) together
+ * with the model's SolveData packing. Per source, phi_p = 2 pi / c (u_p l +
+ * v_p m + w_p (n - 1)) and V_pq(nu) = sum S exp(i (phi_q - phi_p) nu) with
+ * S = I + Q, U + iV, U - iV, I - Q for XX, XY, YX, YY (XX and YY for 2
+ * correlations, I for 1), in FP64, stored complex64; no time or frequency
+ * smearing and no beam. Only `data` crosses PCIe (host or device memory);
+ * frequencies [n_channels] (Hz) are this block's channels, station_uvw
+ * [n_times][n_antennas][3] (m) the station UVW per time step, sky one entry
+ * per direction. Limit: 3 n_antennas + 8 (sources of one direction) doubles
+ * must fit in 200 KiB (DDSOLVE_E_UNSUPPORTED beyond). */
+DDSOLVE_API int ddsolve_set_channel_block_regular_sky(
+    ddsolve_ctx* ctx, uint32_t channel_block, uint32_t n_times, uint32_t n_baselines,
+    uint32_t n_channels, const float* data, const double* frequencies,
+    const double* station_uvw, const uint32_t* antenna1, const uint32_t* antenna2,
+    const ddsolve_sky_direction* sky);
+
+/* The same prediction alone: model [n_directions][n_times * n_baselines *
+ * n_channels][n_correlations][2] float32, in host memory or device memory of
+ * the context's device; returns after the model is written. */
+DDSOLVE_API int ddsolve_predict_regular(ddsolve_ctx* ctx, uint32_t n_times,
+                                        uint32_t n_baselines, uint32_t n_channels,
+                                        const double* frequencies, const double* station_uvw,
+                                        const uint32_t* antenna1, const uint32_t* antenna2,
+                                        const ddsolve_sky_direction* sky, float* model);
+
+/* One solution interval in DP3's buffer layout (the DPBuffers DDECal holds
+ * per interval: [time][baseline][channel][XX XY YX YY], autocorrelations
+ * included). */
+typedef struct {
+  uint32_t n_times;
+  uint32_t n_baselines; /* all baselines of the buffers */
+  uint32_t n_channels;  /* all channels; channel block cb of the context gets
+                           channels [cb n_ch / n_cb, (cb + 1) n_ch / n_cb) */
+  const uint32_t* antenna1; /* [n_baselines] */
+  const uint32_t* antenna2;
+  const float* data;    /* [n_times][n_baselines][n_channels][4][2] unweighted */
+  const float* weights; /* [n_times][n_baselines][n_channels][4] */
+  const uint8_t* flags; /* [n_times][n_baselines][n_channels][4], nonzero =
+                           flagged; NULL = nothing flagged */
+  const float* model;   /* [n_directions][n_times][n_baselines][n_channels][4][2]
+                           unweighted model, or NULL: predicted from `sky` */
+  const double* frequencies;        /* [n_channels] Hz (with sky) */
+  const double* station_uvw;        /* [n_times][n_antennas][3] m (with sky) */
+  const ddsolve_sky_direction* sky; /* [n_directions] (with sky) */
+  int32_t linear_weighting; /* 1: weight by w, 0: by sqrt(w) */
+} ddsolve_interval_buffers;
+
+/* Uploads one solution interval from DP3's raw buffers and does on the GPU
+ * what DDECal does on the host before a solve: AssignAndWeight
+ * (ddecal/gain_solvers/SolverTools.cc:81-167: a visibility is flagged when
+ * any correlation of the data or of any direction's model is flagged or
+ * non-finite; data and models are weighted by sqrt(w) per correlation, or
+ * by w in linear_weighting mode; flagged visibilities become zero) and the
+ * regular SolveData constructor (SolveData.cc:77-188: even channel-block
+ * split, autocorrelations dropped, XX / YY or (XX + YY) / 2 per the
+ * context's correlations, direction-dependent solution indices), for every
+ * channel block of the context. With model == NULL the unweighted model is
+ * predicted on the GPU first (as ddsolve_set_channel_block_regular_sky).
+ * data, weights, flags and model may be host memory or device memory of the
+ * context's device; the call returns when the interval is in place. */
+DDSOLVE_API int ddsolve_set_interval_buffers(ddsolve_ctx* ctx,
+                                             const ddsolve_interval_buffers* buffers);
 
 /* Full iterate-until-converged solve on the device with no host constraints:
  * replaces IterativeDiagonalSolver<V>::Solve
