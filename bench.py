@@ -408,6 +408,34 @@ def run_mlp_only(args):
     return 0
 
 
+def run_mlp_infer(args):
+    """The warm start's inference product alone: forward passes of the
+    first-stage network (336 inputs, two hidden layers of 256, 48 outputs) on
+    the 620 samples of one 62-station, 10-direction interval, through
+    ddwarm_predict (one fused mlp_forward_kernel launch per call after the
+    input rows are gathered and tiled); the command the inference profile
+    uses. Prints the wall time per call."""
+    import torch
+    from dp3_b200 import warmstart
+    rng = np.random.default_rng(7)
+    n, n_in, n_out = 620, 336, 48
+    x = rng.normal(size=(n, n_in)).astype(np.float32)
+    mlp = warmstart.MLP(n_in, n_out, hidden=256, seed=1)
+    for _ in range(args.warmup):
+        mlp.predict(x)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        mlp.predict(x)
+    dt = (time.perf_counter() - t0) / max(args.steps, 1)
+    flops = 2 * n * (n_in * 256 + 256 * 256 + 256 * n_out)
+    print(json.dumps({"mlp_predict_us_per_call": dt * 1e6, "rows": n,
+                      "note": "host x in, host y out: includes the H2D / D2H copies",
+                      "forward_mflop": flops / 1e6}), flush=True)
+    mlp.close()
+    return 0
+
+
 def run_fp64_check(args):
     """Solution error of the GPU solver against the FP64 oracle on
     configuration `args.config` (a numerical statement, not a timing): one
@@ -867,6 +895,8 @@ def main():
                     help="solution error against the FP64 oracle (no timing)")
     ap.add_argument("--batch", type=int, default=1,
                     help="independent intervals of --config solved in one context")
+    ap.add_argument("--mlp-infer", action="store_true",
+                    help="time only the warm-start network's forward pass (for profiling)")
     ap.add_argument("--mlp-only", action="store_true",
                     help="time only the warm-start network's training (for profiling)")
     ap.add_argument("--mlp-rows", type=int, default=60000)
@@ -880,6 +910,8 @@ def main():
         return run_reference_arm(args)
     if args.mlp_only:
         return run_mlp_only(args)
+    if args.mlp_infer:
+        return run_mlp_infer(args)
     if args.fp64_check:
         return run_fp64_check(args)
     if args.batch > 1:
