@@ -142,15 +142,27 @@ struct StreamParams {
   uint32_t n_ant, n_dir, n_sub, ng;
 };
 
+// Finalisation modes of a solve iteration. Fused: merge, FP64 division,
+// SolverBase::Step, AssignSolutions and the iteration control in one pass.
+// With device constraints the iteration is split around them
+// (IterativeDiagonalSolver.cc:77-83: Step, ApplyConstraints, AssignSolutions):
+// StepOnly writes the stepped next solutions to next_out and stops there;
+// AssignOnly reads the constrained next solutions from next_out and does the
+// rest (norm, solutions, gain tables, non-finite flags, control).
+constexpr int32_t kFinFused = 0;
+constexpr int32_t kFinStepOnly = 1;
+constexpr int32_t kFinAssignOnly = 2;
+
 struct FinParams {
   const float* partials;
   const uint32_t* fin_off;     // [n_cb * n_sub + 1]
   const uint32_t* fin_visits;  // visit indices
   const uint32_t* dir_of_sub;  // [n_sub]
   double2* solutions;          // [n_cb][n_ant][n_sub][NPOL]
-  double2* next_out;           // host mode output
+  double2* next_out;           // host mode output; the constrained passes' buffer
   uint32_t n_cb, n_ant, n_dir, n_sub;
   int32_t host_mode;
+  int32_t fin_mode;            // FinFused / FinStepOnly / FinAssignOnly
   const DevSettings* settings;
   double* block_sum;
   uint32_t* block_cnt;
@@ -454,6 +466,8 @@ __global__ void weigh_kernel(const WeighParams p) {
 #pragma unroll
       for (int k = 0; k < 4; ++k) flag = flag || !finite(m[k]);
     }
+    // Products and the 1-correlation sum rounded separately (no fused
+    // multiply-add), as the reference's complex<float> arithmetic rounds them.
     auto put = [&](float2* dst, const float2 (&z)[4]) {
       if (NCORR == 4) {
 #pragma unroll
@@ -462,20 +476,22 @@ __global__ void weigh_kernel(const WeighParams p) {
         dst[0] = z[0];
         dst[1] = z[3];
       } else {
-        dst[0] = make_float2(0.5f * (z[0].x + z[3].x), 0.5f * (z[0].y + z[3].y));
+        dst[0] = make_float2(0.5f * __fadd_rn(z[0].x, z[3].x), 0.5f * __fadd_rn(z[0].y, z[3].y));
       }
     };
     float2 z[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-      z[k] = flag ? make_float2(0.f, 0.f) : make_float2(dv[k].x * pw[k], dv[k].y * pw[k]);
+      z[k] = flag ? make_float2(0.f, 0.f)
+                  : make_float2(__fmul_rn(dv[k].x, pw[k]), __fmul_rn(dv[k].y, pw[k]));
     put(p.out + v * NCORR, z);
     for (uint32_t d = 0; d < p.n_dir; ++d) {
       const float2* m = model_at(d);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const float2 mk = m[k];
-        z[k] = flag ? make_float2(0.f, 0.f) : make_float2(mk.x * pw[k], mk.y * pw[k]);
+        z[k] = flag ? make_float2(0.f, 0.f)
+                    : make_float2(__fmul_rn(mk.x, pw[k]), __fmul_rn(mk.y, pw[k]));
       }
       put(p.out + (n_vis * (1 + d) + v) * NCORR, z);
     }
@@ -847,7 +863,7 @@ __global__ void __launch_bounds__(kThreads) finalize_kernel(const FinParams p) {
     const uint32_t acc_n = p.n_ant * p.n_dir * NPOL * 3;
     NeumaierSum nr[NPOL], ni[NPOL], dn[NPOL];
     const uint32_t j0 = p.fin_off[cb * p.n_sub + s];
-    const uint32_t j1 = p.fin_off[cb * p.n_sub + s + 1];
+    const uint32_t j1 = p.fin_mode == kFinAssignOnly ? j0 : p.fin_off[cb * p.n_sub + s + 1];
     for (uint32_t j = j0; j < j1; ++j) {
       const float* a = p.partials + size_t(p.fin_visits[j]) * acc_n +
                        ((ant * p.n_dir + d) * NPOL) * 3;
@@ -877,11 +893,15 @@ __global__ void __launch_bounds__(kThreads) finalize_kernel(const FinParams p) {
                               ga_i + double(ni[q].Value()) / double(den));
       }
     }
+    double2* out = p.next_out + (size_t(cb) * p.n_ant * p.n_sub +
+                                 size_t(ant) * p.n_sub + s) * NPOL;
     if (p.host_mode) {
-      double2* out = p.next_out + (size_t(cb) * p.n_ant * p.n_sub +
-                                   size_t(ant) * p.n_sub + s) * NPOL;
 #pragma unroll
       for (int q = 0; q < NPOL; ++q) out[q] = nxt[q];
+    } else if (p.fin_mode == kFinAssignOnly) {
+      // the stepped and constrained next solutions of this iteration
+#pragma unroll
+      for (int q = 0; q < NPOL; ++q) nxt[q] = out[q];
     } else {
       // SolverBase::Step (SolverBase.cc:88-158)
 #pragma unroll
@@ -901,6 +921,12 @@ __global__ void __launch_bounds__(kThreads) finalize_kernel(const FinParams p) {
           nxt[q] = make_double2(cs, sn);
         }
       }
+      if (p.fin_mode == kFinStepOnly) {
+#pragma unroll
+        for (int q = 0; q < NPOL; ++q) out[q] = nxt[q];
+      }
+    }
+    if (!p.host_mode && p.fin_mode != kFinStepOnly) {
       // SolverBase::AssignSolutions norm (SolverBase.cc:234-285)
       if (NPOL == 1) {
         if (old[0].x != 0.0 || old[0].y != 0.0) {
@@ -939,7 +965,7 @@ __global__ void __launch_bounds__(kThreads) finalize_kernel(const FinParams p) {
       if (!all_finite) p.nonfinite[cb] = 1u;
     }
   }
-  if (p.host_mode) return;
+  if (p.host_mode || p.fin_mode == kFinStepOnly) return;
 
   // Block reduction of the norm, then the last block finishes the iteration.
   __shared__ double s_sum[kThreads];
@@ -1051,6 +1077,7 @@ struct PipeParams {
   uint32_t* counters;    // [0] CTAs finalised, [1] error flag, [2] grid barrier
   double2* next_out;
   int32_t host_mode;
+  int32_t fin_mode;      // FinFused / FinStepOnly / FinAssignOnly
   const DevSettings* settings;
   LoopState* state;
   double* step_magnitudes;
@@ -1243,7 +1270,10 @@ __device__ __forceinline__ void WriteTables(const PipeParams& p, uint32_t cb,
 // norms in CTA order, runs ReachedStoppingCriterion / DetectStall (SolverBase.h:274-285,
 // SolverBase.cc:63-86), and prepares the next iteration's
 // MakeSolutionsFinite{1,2}Pol (SolverBase.cc:316-371) for channel blocks that
-// got non-finite solutions.
+// got non-finite solutions. With device constraints the work is split by
+// p.fin_mode: kFinStepOnly (pipe_kernel) stops after the step, writing the
+// stepped solutions to next_out; kFinAssignOnly (assign_kernel) starts from
+// the constrained ones in next_out.
 template <int NPOL>
 __device__ __forceinline__ void FinalizeDistributed(const PipeParams& p, int ctid,
                                                  double* s_sum, uint32_t* s_cnt,
@@ -1284,8 +1314,8 @@ __device__ __forceinline__ void FinalizeDistributed(const PipeParams& p, int cti
             double(float(old[q].y)) + double(ni[q].Value()) / double(den));
       }
     }
+    double2* out = p.next_out + size_t(item) * NPOL;
     if (p.host_mode) {
-      double2* out = p.next_out + size_t(item) * NPOL;
 #pragma unroll
       for (int q = 0; q < NPOL; ++q) out[q] = nxt[q];
       // the gain tables of a chained next pass, which starts from `nxt`
@@ -1293,21 +1323,32 @@ __device__ __forceinline__ void FinalizeDistributed(const PipeParams& p, int cti
       WriteTables<NPOL>(p, cb, ant, s, nxt);
       return;
     }
+    if (p.fin_mode == kFinAssignOnly) {
+      // the stepped and constrained next solutions of this iteration
 #pragma unroll
-    for (int q = 0; q < NPOL; ++q) {
-      if (!st.phase_only) {
-        nxt[q] = make_double2(old[q].x * (1.0 - st.step_size) + nxt[q].x * st.step_size,
-                              old[q].y * (1.0 - st.step_size) + nxt[q].y * st.step_size);
-      } else {
-        const double from = atan2(old[q].y, old[q].x);
-        double dist = atan2(nxt[q].y, nxt[q].x) - from;
-        if (dist > M_PI)
-          dist -= 2.0 * M_PI;
-        else if (dist < -M_PI)
-          dist += 2.0 * M_PI;
-        double sn, cs;
-        sincos(from + st.step_size * dist, &sn, &cs);
-        nxt[q] = make_double2(cs, sn);
+      for (int q = 0; q < NPOL; ++q) nxt[q] = out[q];
+    } else {
+#pragma unroll
+      for (int q = 0; q < NPOL; ++q) {
+        if (!st.phase_only) {
+          nxt[q] = make_double2(old[q].x * (1.0 - st.step_size) + nxt[q].x * st.step_size,
+                                old[q].y * (1.0 - st.step_size) + nxt[q].y * st.step_size);
+        } else {
+          const double from = atan2(old[q].y, old[q].x);
+          double dist = atan2(nxt[q].y, nxt[q].x) - from;
+          if (dist > M_PI)
+            dist -= 2.0 * M_PI;
+          else if (dist < -M_PI)
+            dist += 2.0 * M_PI;
+          double sn, cs;
+          sincos(from + st.step_size * dist, &sn, &cs);
+          nxt[q] = make_double2(cs, sn);
+        }
+      }
+      if (p.fin_mode == kFinStepOnly) {
+#pragma unroll
+        for (int q = 0; q < NPOL; ++q) out[q] = nxt[q];
+        return;
       }
     }
     if (NPOL == 1) {
@@ -1393,6 +1434,7 @@ __device__ __forceinline__ void FinalizeDistributed(const PipeParams& p, int cti
       uint32_t n_rounds = 0;
   #pragma unroll
       for (int b = 0; b < kFinBatch; ++b) n_rounds = max(n_rounds, j1v[b] - j0v[b]);
+      if (p.fin_mode == kFinAssignOnly) n_rounds = 0;  // no partial slots to merge
       NeumaierSum nr[kFinBatch][NPOL], ni[kFinBatch][NPOL], dn[kFinBatch][NPOL];
       constexpr int kR = 4;  // slots per item and round
       for (uint32_t k = 0; k < n_rounds; k += kR) {
@@ -1465,6 +1507,14 @@ __device__ __forceinline__ void FinalizeDistributed(const PipeParams& p, int cti
   ConsumerBarrier();
   if (!*s_last) return;
   __threadfence();
+  if (p.fin_mode == kFinStepOnly) {
+    // the assignment pass after the constraints finishes the iteration
+    if (ctid == 0) {
+      p.counters[0] = 0;
+      p.counters[2] = 0;
+    }
+    return;
+  }
   // Channel blocks with new non-finite solutions, checked by all consumer
   // threads at once (the serial pass below runs only when there are some).
   uint32_t any_bad = 0;
@@ -2268,6 +2318,174 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
   FinalizeDistributed<NPOL>(p, ctid, s_sum, s_cnt, s_last);
 }
 
+// The assignment pass of a constrained iteration on the pipelined path
+// (fin_mode = kFinAssignOnly): FinalizeDistributed over the constrained next
+// solutions, with kPipeRuns threads per CTA (its barriers span them) and the
+// CTA count of pipe_kernel (its norm partials).
+template <int NPOL>
+__global__ void __launch_bounds__(kPipeRuns) assign_kernel(const PipeParams p) {
+  if (p.use_handle && static_cast<volatile const LoopState*>(p.state)->done) return;
+  __shared__ double s_sum[kPipeRuns];
+  __shared__ uint32_t s_cnt[kPipeRuns];
+  __shared__ uint32_t s_last;
+  if (threadIdx.x == 0) s_last = 0;
+  __syncthreads();
+  FinalizeDistributed<NPOL>(p, int(threadIdx.x), s_sum, s_cnt, &s_last);
+}
+
+// ---------------------------------------------------------------------------
+// Device constraints: DP3's SmoothnessConstraint, AntennaConstraint and
+// Constraint::ApplyReferenceAntenna applied to the stepped next solutions
+// [n_cb][n_ant][n_sub][NPOL] (complex128) of an iteration, between the
+// step-only and the assignment passes, so that a constrained solve stays in
+// the device loop. All FP64, in the reference's order of operations. Every
+// kernel returns at once when the solve has stopped (unrolled graph bodies).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool SolveStopped(const LoopState* state, int use_handle) {
+  return use_handle && static_cast<volatile const LoopState*>(state)->done;
+}
+
+struct SmoothParams {
+  const double2* in;        // [n_cb][n_series]
+  double2* out;             // [n_cb][n_series]
+  uint32_t n_cb, n_series;  // series = (ant * n_sub + sub) * n_pol + pol
+  uint32_t n_ant, n_sub, n_pol;
+  const double* freq;       // [n_cb] channel-block frequencies (Hz)
+  const double* fcorr;      // [n_cb] (local bandwidth / bandwidth)^exponent
+  const uint32_t* band;     // [n_cb][2] first and end channel block of the kernel
+  const double* weights;    // [n_weight_sets][n_ant * n_cb]
+  uint32_t per_sub_weights; // weights per sub-solution (SetSubSolutionWeights)
+  const double* factor;     // [n_ant * n_sub] kernel size factor (dd / antenna)
+  double bandwidth;
+  int32_t truncate;
+  const LoopState* state;
+  int32_t use_handle;
+};
+
+// SmoothnessConstraint::Apply (SmoothnessConstraint.cc:48-97) with
+// KernelSmoother::Smooth / Kernel (KernelSmoother.h:69-98, 108-160), Gaussian
+// kernel: one thread per (channel block i, series); output i of a series is
+// the kernel-weighted mean of its finite values over the band of i.
+__global__ void __launch_bounds__(256) smooth_kernel(const SmoothParams p) {
+  if (SolveStopped(p.state, p.use_handle)) return;
+  const uint64_t idx = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= uint64_t(p.n_cb) * p.n_series) return;
+  const uint32_t i = uint32_t(idx / p.n_series);
+  const uint32_t series = uint32_t(idx - uint64_t(i) * p.n_series);
+  const uint32_t sub = (series / p.n_pol) % p.n_sub;
+  const uint32_t ant = series / (p.n_sub * p.n_pol);
+  const double* w = p.weights + (p.per_sub_weights ? size_t(sub) * p.n_ant * p.n_cb : 0) +
+                    size_t(ant) * p.n_cb;
+  const double kernel_correction = p.fcorr[i] * p.factor[size_t(ant) * p.n_sub + sub];
+  double2 sum = make_double2(0.0, 0.0);
+  double weight_sum = 0.0;
+  for (uint32_t j = p.band[2 * i]; j < p.band[2 * i + 1]; ++j) {
+    const double2 v = p.in[size_t(j) * p.n_series + series];
+    if (!dfinite(v)) continue;  // data 0, weight 0: adds nothing
+    const double x = ((p.freq[i] - p.freq[j]) * kernel_correction) / p.bandwidth;
+    const double k = (p.truncate && (x < -1.0 || x > 1.0)) ? 0.0 : exp(-x * x * 9.0);
+    const double wt = k * w[j];
+    sum.x += v.x * wt;
+    sum.y += v.y * wt;
+    weight_sum += wt;
+  }
+  p.out[size_t(i) * p.n_series + series] =
+      weight_sum == 0.0 ? make_double2(nan(""), nan(""))
+                        : make_double2(sum.x / weight_sum, sum.y / weight_sum);
+}
+
+// AntennaConstraint::Apply (AntennaConstraint.h:39-76): per channel block,
+// antenna set, sub-solution and polarization, the mean of the set's finite
+// solutions (0 / 0 = NaN when there are none) replaces each member's. One
+// thread per (channel block, sub-solution, polarization), the sets in order.
+__global__ void __launch_bounds__(256)
+    antenna_constraint_kernel(double2* sol, uint32_t n_cb, uint32_t n_ant, uint32_t n_sub,
+                              uint32_t n_pol, const uint32_t* set_off, const uint32_t* members,
+                              uint32_t n_sets, const LoopState* state, int use_handle) {
+  if (SolveStopped(state, use_handle)) return;
+  const uint32_t per_cb = n_sub * n_pol;
+  const uint64_t idx = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= uint64_t(n_cb) * per_cb) return;
+  const uint32_t cb = uint32_t(idx / per_cb);
+  const uint32_t sp = uint32_t(idx - uint64_t(cb) * per_cb);  // sub * n_pol + pol
+  double2* base = sol + size_t(cb) * n_ant * per_cb + sp;
+  for (uint32_t k = 0; k < n_sets; ++k) {
+    double2 sum = make_double2(0.0, 0.0);
+    double count = 0.0;
+    for (uint32_t m = set_off[k]; m < set_off[k + 1]; ++m) {
+      const double2 v = base[size_t(members[m]) * per_cb];
+      if (dfinite(v)) {
+        sum.x += v.x;
+        sum.y += v.y;
+        count += 1.0;
+      }
+    }
+    const double2 mean = make_double2(sum.x / count, sum.y / count);
+    for (uint32_t m = set_off[k]; m < set_off[k + 1]; ++m) base[size_t(members[m]) * per_cb] = mean;
+  }
+}
+
+// Constraint::ApplyReferenceAntenna (Constraint.cc:7-37), first half: per
+// polarization the first antenna whose direction-0 solutions are finite in
+// more than 20% of the channel blocks (antenna 0 when there is none).
+__global__ void reference_antenna_select_kernel(const double2* sol, uint32_t n_cb,
+                                                uint32_t n_ant, uint32_t n_sub, uint32_t n_pol,
+                                                uint32_t* ref_ant, const LoopState* state,
+                                                int use_handle) {
+  if (SolveStopped(state, use_handle)) return;
+  const uint32_t pol = threadIdx.x;
+  if (pol >= n_pol) return;
+  uint32_t ref = 0;
+  for (; ref < n_ant; ++ref) {
+    uint32_t n_finite = 0;
+    for (uint32_t cb = 0; cb < n_cb; ++cb)
+      n_finite += dfinite(sol[((size_t(cb) * n_ant + ref) * n_sub) * n_pol + pol]) ? 1u : 0u;
+    if (double(n_finite) > 0.2 * double(n_cb)) break;
+  }
+  ref_ant[pol] = ref == n_ant ? 0u : ref;
+}
+
+// std::complex<double> division a / b as C99 Annex G (G.5.1) specifies it:
+// the divisor scaled by a power of two before the products.
+__device__ __forceinline__ double2 ddiv(double2 a, double2 b) {
+  const double m = fmax(fabs(b.x), fabs(b.y));
+  int ilogbw = 0;
+  double c = b.x, d = b.y;
+  const double lw = logb(m);
+  if (isfinite(lw)) {
+    ilogbw = int(lw);
+    c = scalbn(c, -ilogbw);
+    d = scalbn(d, -ilogbw);
+  }
+  const double denom = c * c + d * d;
+  return make_double2(scalbn((a.x * c + a.y * d) / denom, -ilogbw),
+                      scalbn((a.y * c - a.x * d) / denom, -ilogbw));
+}
+
+// Second half: one thread per (channel block, polarization); every other
+// antenna's solutions (all sub-solutions) are divided by the reference
+// antenna's, which become 1.
+__global__ void __launch_bounds__(256)
+    reference_antenna_apply_kernel(double2* sol, uint32_t n_cb, uint32_t n_ant, uint32_t n_sub,
+                                   uint32_t n_pol, const uint32_t* ref_ant,
+                                   const LoopState* state, int use_handle) {
+  if (SolveStopped(state, use_handle)) return;
+  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n_cb * n_pol) return;
+  const uint32_t cb = idx / n_pol, pol = idx - cb * n_pol;
+  const uint32_t ref = ref_ant[pol];
+  double2* base = sol + size_t(cb) * n_ant * n_sub * n_pol + pol;
+  for (uint32_t s = 0; s < n_sub; ++s) {
+    const double2 r = base[(size_t(ref) * n_sub + s) * n_pol];
+    for (uint32_t a = 0; a < n_ant; ++a)
+      if (a != ref) {
+        double2& v = base[(size_t(a) * n_sub + s) * n_pol];
+        v = ddiv(v, r);
+      }
+  }
+  for (uint32_t s = 0; s < n_sub; ++s) base[(size_t(ref) * n_sub + s) * n_pol] = make_double2(1.0, 0.0);
+}
+
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
@@ -2406,6 +2624,20 @@ struct ddsolve_ctx {
   // solver state
   DevBuf d_sol, d_next, d_state, d_nonfinite, d_mags, d_settings;
   DevBuf d_chain;  // outputs of ddsolve_perform_iterations
+  // Device constraints (ddsolve_add_*_constraint), applied in the order they
+  // were added between the step-only and the assignment passes of every
+  // solve iteration.
+  struct DeviceConstraint {
+    int kind = 0;         // DDSOLVE_CONSTRAINT_*
+    DevBuf buf;           // the constraint's device arrays, one allocation
+    size_t off[6] = {};   // byte offsets of those arrays in buf
+    uint32_t n_sets = 0;  // antenna constraint
+    uint32_t per_sub_weights = 0;
+    double bandwidth = 0.0;
+    int32_t truncate = 0;
+  };
+  std::vector<DeviceConstraint> constraints;
+  DevBuf d_cons, d_ref_ant;  // second next-solutions buffer; reference antennas
   // independent solution intervals (ddsolve_set_intervals): interval g owns
   // channel blocks [group_first_cb[g], group_first_cb[g + 1])
   uint32_t n_groups = 1;
@@ -3439,6 +3671,7 @@ FinParams MakeFinParams(ddsolve_ctx* ctx, bool host_mode) {
   f.n_dir = ctx->n_dir;
   f.n_sub = ctx->n_sub;
   f.host_mode = host_mode ? 1 : 0;
+  f.fin_mode = kFinFused;
   f.settings = ctx->d_settings.as<DevSettings>();
   f.block_sum = ctx->d_block_sum.as<double>();
   f.block_cnt = ctx->d_block_cnt.as<uint32_t>();
@@ -3505,6 +3738,7 @@ PipeParams MakePipeParams(ddsolve_ctx* ctx, bool host_mode, bool use_handle) {
   p.counters = ctx->d_counters.as<uint32_t>();
   p.next_out = ctx->d_next.as<double2>();
   p.host_mode = host_mode ? 1 : 0;
+  p.fin_mode = kFinFused;
   p.settings = ctx->d_settings.as<DevSettings>();
   p.state = ctx->d_state.as<LoopState>();
   p.step_magnitudes = ctx->d_mags.as<double>();
@@ -3571,16 +3805,84 @@ int LaunchMakeFinite(ddsolve_ctx* ctx, bool use_handle) {
   return DDSOLVE_OK;
 }
 
+// Launches the device constraints, in order, on the stepped next solutions
+// (d_next); *result = the buffer that then holds the constrained ones (the
+// smoothing writes to the other buffer of the pair).
+int LaunchConstraints(ddsolve_ctx* ctx, bool use_handle, double2** result) {
+  double2* cur = ctx->d_next.as<double2>();
+  const uint32_t n_series = ctx->n_ant * ctx->n_sub * ctx->n_pol;
+  const int uh = use_handle ? 1 : 0;
+  const LoopState* state = ctx->d_state.as<LoopState>();
+  for (const ddsolve_ctx::DeviceConstraint& c : ctx->constraints) {
+    const char* b = c.buf.as<const char>();
+    if (c.kind == DDSOLVE_CONSTRAINT_SMOOTHNESS) {
+      double2* dst = cur == ctx->d_next.as<double2>() ? ctx->d_cons.as<double2>()
+                                                      : ctx->d_next.as<double2>();
+      SmoothParams sp;
+      sp.in = cur;
+      sp.out = dst;
+      sp.n_cb = ctx->n_cb;
+      sp.n_series = n_series;
+      sp.n_ant = ctx->n_ant;
+      sp.n_sub = ctx->n_sub;
+      sp.n_pol = ctx->n_pol;
+      sp.freq = reinterpret_cast<const double*>(b + c.off[0]);
+      sp.fcorr = reinterpret_cast<const double*>(b + c.off[1]);
+      sp.band = reinterpret_cast<const uint32_t*>(b + c.off[2]);
+      sp.weights = reinterpret_cast<const double*>(b + c.off[3]);
+      sp.per_sub_weights = c.per_sub_weights;
+      sp.factor = reinterpret_cast<const double*>(b + c.off[4]);
+      sp.bandwidth = c.bandwidth;
+      sp.truncate = c.truncate;
+      sp.state = state;
+      sp.use_handle = uh;
+      const uint64_t n = uint64_t(ctx->n_cb) * n_series;
+      smooth_kernel<<<uint32_t((n + 255) / 256), 256, 0, ctx->stream>>>(sp);
+      cur = dst;
+    } else if (c.kind == DDSOLVE_CONSTRAINT_ANTENNA) {
+      const uint64_t n = uint64_t(ctx->n_cb) * ctx->n_sub * ctx->n_pol;
+      antenna_constraint_kernel<<<uint32_t((n + 255) / 256), 256, 0, ctx->stream>>>(
+          cur, ctx->n_cb, ctx->n_ant, ctx->n_sub, ctx->n_pol,
+          reinterpret_cast<const uint32_t*>(b + c.off[0]),
+          reinterpret_cast<const uint32_t*>(b + c.off[1]), c.n_sets, state, uh);
+    } else {
+      reference_antenna_select_kernel<<<1, 32, 0, ctx->stream>>>(
+          cur, ctx->n_cb, ctx->n_ant, ctx->n_sub, ctx->n_pol, ctx->d_ref_ant.as<uint32_t>(),
+          state, uh);
+      const uint32_t n = ctx->n_cb * ctx->n_pol;
+      reference_antenna_apply_kernel<<<(n + 255) / 256, 256, 0, ctx->stream>>>(
+          cur, ctx->n_cb, ctx->n_ant, ctx->n_sub, ctx->n_pol, ctx->d_ref_ant.as<uint32_t>(),
+          state, uh);
+    }
+    DDS_CHECK_CUDA(ctx, cudaGetLastError());
+  }
+  *result = cur;
+  return DDSOLVE_OK;
+}
+
+// Kernel launches of the device constraints per iteration.
+uint32_t ConstraintLaunches(const ddsolve_ctx* ctx) {
+  uint32_t n = 0;
+  for (const ddsolve_ctx::DeviceConstraint& c : ctx->constraints)
+    n += c.kind == DDSOLVE_CONSTRAINT_REFERENCE_ANTENNA ? 2u : 1u;
+  return n;
+}
+
 // Launches one iteration's kernels on the context stream: pipe_kernel alone
 // on the pipelined path (its fused finalisation repairs non-finite solutions
 // lazily, so make_finite_kernel only runs once before the loop), else
-// make_finite_kernel + stream_kernel + finalize_kernel.
+// make_finite_kernel + stream_kernel + finalize_kernel. With device
+// constraints (solve mode) the finalisation is split around them: the pass
+// finalises in step-only mode, the constraints run, and an assignment pass
+// (assign_kernel, or finalize_kernel again) finishes the iteration.
 int LaunchIteration(ddsolve_ctx* ctx, bool host_mode, bool use_handle,
                     bool with_make_finite) {
+  const bool constrained = !host_mode && !ctx->constraints.empty();
   if (ctx->use_pipe) {
     // Cooperative launch: pipe_kernel has a grid barrier, so all CTAs must be
     // resident (the grid is #SM x occupancy).
     PipeParams pp = MakePipeParams(ctx, host_mode, use_handle);
+    if (constrained) pp.fin_mode = kFinStepOnly;
     void* args[] = {&pp};
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ctx->n_ctas);
@@ -3593,6 +3895,18 @@ int LaunchIteration(ddsolve_ctx* ctx, bool host_mode, bool use_handle,
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     DDS_CHECK_CUDA(ctx, cudaLaunchKernelExC(&cfg, ctx->pipe_fn, args));
+    if (!constrained) return DDSOLVE_OK;
+    double2* cons = nullptr;
+    const int rc = LaunchConstraints(ctx, use_handle, &cons);
+    if (rc != DDSOLVE_OK) return rc;
+    PipeParams ap = pp;
+    ap.fin_mode = kFinAssignOnly;
+    ap.next_out = cons;
+    if (ctx->n_pol == 2)
+      assign_kernel<2><<<ctx->n_ctas, kPipeRuns, 0, ctx->stream>>>(ap);
+    else
+      assign_kernel<1><<<ctx->n_ctas, kPipeRuns, 0, ctx->stream>>>(ap);
+    DDS_CHECK_CUDA(ctx, cudaGetLastError());
     return DDSOLVE_OK;
   }
   if (with_make_finite) {
@@ -3604,11 +3918,21 @@ int LaunchIteration(ddsolve_ctx* ctx, bool host_mode, bool use_handle,
   DDS_CHECK_CUDA(ctx, cudaGetLastError());
   FinParams fp = MakeFinParams(ctx, host_mode);
   fp.use_handle = use_handle ? 1 : 0;
-  if (ctx->n_pol == 2)
-    finalize_kernel<2><<<ctx->fin_blocks, kThreads, 0, ctx->stream>>>(fp);
-  else
-    finalize_kernel<1><<<ctx->fin_blocks, kThreads, 0, ctx->stream>>>(fp);
-  DDS_CHECK_CUDA(ctx, cudaGetLastError());
+  if (constrained) fp.fin_mode = kFinStepOnly;
+  for (int pass = 0; pass < (constrained ? 2 : 1); ++pass) {
+    if (pass == 1) {
+      double2* cons = nullptr;
+      const int rc = LaunchConstraints(ctx, use_handle, &cons);
+      if (rc != DDSOLVE_OK) return rc;
+      fp.fin_mode = kFinAssignOnly;
+      fp.next_out = cons;
+    }
+    if (ctx->n_pol == 2)
+      finalize_kernel<2><<<ctx->fin_blocks, kThreads, 0, ctx->stream>>>(fp);
+    else
+      finalize_kernel<1><<<ctx->fin_blocks, kThreads, 0, ctx->stream>>>(fp);
+    DDS_CHECK_CUDA(ctx, cudaGetLastError());
+  }
   return DDSOLVE_OK;
 }
 
@@ -4212,6 +4536,9 @@ int SolveImpl(ddsolve_ctx* ctx, double* solutions, ddsolve_result* results,
   cudaSetDevice(ctx->device);
   int rc;
   bool solve_powers = false;
+  if (ctx->n_groups > 1 && !ctx->constraints.empty())
+    return ctx->Fail(DDSOLVE_E_UNSUPPORTED,
+                     "device constraints apply to single-interval contexts");
   if (ctx->plan_dirty && (rc = BuildPlan(ctx)) != DDSOLVE_OK) return rc;
   const uint32_t n_groups = ctx->n_groups;
   const size_t n_sol = size_t(ctx->n_cb) * ctx->n_ant * ctx->n_sub * ctx->n_pol;
@@ -4301,9 +4628,13 @@ int SolveImpl(ddsolve_ctx* ctx, double* solutions, ddsolve_result* results,
     }
   }
   // pipe path: make_finite + build_tables (+ power_kernel) + one pipe_kernel
-  // per iteration; else three kernels per iteration
-  ctx->last_launches = ctx->use_pipe ? uint64_t(max_it) + 2 + (solve_powers ? 1 : 0)
-                                     : uint64_t(max_it) * 3;
+  // per iteration; else three kernels per iteration; with device constraints
+  // also their kernels and the assignment pass, every iteration
+  const uint64_t per_it_cons =
+      ctx->constraints.empty() ? 0u : uint64_t(ConstraintLaunches(ctx)) + 1u;
+  ctx->last_launches = ctx->use_pipe
+                           ? uint64_t(max_it) * (1 + per_it_cons) + 2 + (solve_powers ? 1 : 0)
+                           : uint64_t(max_it) * (3 + per_it_cons);
   // the model powers are fresh for one solve only (see LaunchPowers)
   ctx->powers_dirty = true;
   if ((rc = CheckDeviceError(ctx, staged)) != DDSOLVE_OK) return rc;
@@ -4359,6 +4690,130 @@ int ddsolve_set_intervals(ddsolve_ctx* ctx, uint32_t n_intervals,
   ctx->plan_dirty = true;
   ctx->DestroyGraph();
   return UploadSettings(ctx);
+}
+
+int ddsolve_add_smoothness_constraint(ddsolve_ctx* ctx, const ddsolve_smoothness* s) {
+  if (!ctx || !s || !s->frequencies) return DDSOLVE_E_INVALID;
+  if (!s->weights && !s->sub_solution_weights)
+    return ctx->Fail(DDSOLVE_E_INVALID, "smoothness constraint: no weights");
+  if (!(s->bandwidth_hz > 0.0) || !std::isfinite(s->bandwidth_hz))
+    return ctx->Fail(DDSOLVE_E_INVALID, "smoothness constraint: bandwidth must be positive");
+  const uint32_t n = ctx->n_cb, n_ant = ctx->n_ant, n_sub = ctx->n_sub;
+  const std::vector<double> f(s->frequencies, s->frequencies + n);
+  for (uint32_t i = 1; i < n; ++i)
+    if (!(f[i] >= f[i - 1]))
+      return ctx->Fail(DDSOLVE_E_INVALID, "smoothness constraint: frequencies must ascend");
+  // The band and frequency correction of each output channel block, as
+  // KernelSmoother::Smooth (KernelSmoother.h:108-160) walks them.
+  const double bw = s->bandwidth_hz;
+  std::vector<double> fcorr(n);
+  std::vector<uint32_t> band(2 * size_t(n));
+  size_t band_left = 0;
+  const size_t lbound =
+      size_t(std::lower_bound(f.begin(), f.end(), f[0] + bw * 0.5) - f.begin());
+  size_t band_right = std::min(lbound + 1, size_t(n));
+  for (size_t i = 0; i < n; ++i) {
+    size_t start = 0, end = n;
+    const double local = s->bandwidth_ref_frequency_hz == 0.0
+                             ? bw
+                             : bw * f[i] / s->bandwidth_ref_frequency_hz;
+    if (s->kernel_truncation) {
+      while (band_left < n && f[band_left] < f[i] - local * 0.5) ++band_left;
+      while (band_right != n && f[band_right] < f[i] + local * 0.5) ++band_right;
+      start = band_left > 0 ? band_left - 1 : 0;
+      end = band_right < n ? band_right + 1 : n;
+    }
+    band[2 * i] = uint32_t(start);
+    band[2 * i + 1] = uint32_t(end);
+    fcorr[i] = std::pow(local / bw, s->spectral_exponent);
+  }
+  // Kernel size factor of each (antenna, sub-solution): dd factor / antenna
+  // factor (SmoothnessConstraint.cc:82-92).
+  std::vector<double> factor(size_t(n_ant) * n_sub);
+  for (uint32_t a = 0; a < n_ant; ++a)
+    for (uint32_t k = 0; k < n_sub; ++k) {
+      const double dd = s->dd_factors ? 1.0 / s->dd_factors[k] : 1.0;
+      factor[size_t(a) * n_sub + k] = dd / (s->antenna_factors ? s->antenna_factors[a] : 1.0);
+    }
+  const bool per_sub = s->sub_solution_weights != nullptr;
+  const size_t n_w = size_t(per_sub ? n_sub : 1) * n_ant * n;
+  const double* w = per_sub ? s->sub_solution_weights : s->weights;
+  ddsolve_ctx::DeviceConstraint c;
+  c.kind = DDSOLVE_CONSTRAINT_SMOOTHNESS;
+  c.per_sub_weights = per_sub ? 1u : 0u;
+  c.bandwidth = bw;
+  c.truncate = s->kernel_truncation ? 1 : 0;
+  const size_t sizes[5] = {n * 8ull, n * 8ull, 2ull * n * 4, n_w * 8, factor.size() * 8};
+  const void* src[5] = {f.data(), fcorr.data(), band.data(), w, factor.data()};
+  size_t total = 0;
+  for (int k = 0; k < 5; ++k) {
+    c.off[k] = total;
+    total += (sizes[k] + 15) / 16 * 16;
+  }
+  cudaSetDevice(ctx->device);
+  DDS_CHECK_CUDA(ctx, c.buf.Reserve(total));
+  for (int k = 0; k < 5; ++k)
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(c.buf.as<char>() + c.off[k], src[k], sizes[k],
+                                        cudaMemcpyHostToDevice, ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // pageable sources
+  const size_t n_sol = size_t(n) * n_ant * n_sub * ctx->n_pol;
+  DDS_CHECK_CUDA(ctx, ctx->d_cons.Reserve(n_sol * sizeof(double2)));
+  ctx->constraints.push_back(std::move(c));
+  ctx->DestroyGraph();
+  return DDSOLVE_OK;
+}
+
+int ddsolve_add_antenna_constraint(ddsolve_ctx* ctx, uint32_t n_sets, const uint32_t* set_offsets,
+                                   const uint32_t* antennas) {
+  if (!ctx || (n_sets > 0 && !set_offsets)) return DDSOLVE_E_INVALID;
+  // each set as a std::set: ascending, without repeats
+  std::vector<uint32_t> off{0}, members;
+  for (uint32_t k = 0; k < n_sets; ++k) {
+    if (set_offsets[k + 1] < set_offsets[k] || (set_offsets[k + 1] > set_offsets[k] && !antennas))
+      return ctx->Fail(DDSOLVE_E_INVALID, "antenna constraint: bad set offsets");
+    std::vector<uint32_t> set(antennas + set_offsets[k], antennas + set_offsets[k + 1]);
+    for (uint32_t a : set)
+      if (a >= ctx->n_ant) return ctx->Fail(DDSOLVE_E_INVALID, "antenna constraint: bad antenna");
+    std::sort(set.begin(), set.end());
+    set.erase(std::unique(set.begin(), set.end()), set.end());
+    members.insert(members.end(), set.begin(), set.end());
+    off.push_back(uint32_t(members.size()));
+  }
+  ddsolve_ctx::DeviceConstraint c;
+  c.kind = DDSOLVE_CONSTRAINT_ANTENNA;
+  c.n_sets = n_sets;
+  c.off[0] = 0;
+  c.off[1] = (off.size() * 4 + 15) / 16 * 16;
+  cudaSetDevice(ctx->device);
+  DDS_CHECK_CUDA(ctx, c.buf.Reserve(c.off[1] + members.size() * 4 + 16));
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(c.buf.ptr, off.data(), off.size() * 4,
+                                      cudaMemcpyHostToDevice, ctx->stream));
+  if (!members.empty())
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(c.buf.as<char>() + c.off[1], members.data(),
+                                        members.size() * 4, cudaMemcpyHostToDevice,
+                                        ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // pageable sources
+  ctx->constraints.push_back(std::move(c));
+  ctx->DestroyGraph();
+  return DDSOLVE_OK;
+}
+
+int ddsolve_add_reference_antenna_constraint(ddsolve_ctx* ctx) {
+  if (!ctx) return DDSOLVE_E_INVALID;
+  cudaSetDevice(ctx->device);
+  DDS_CHECK_CUDA(ctx, ctx->d_ref_ant.Reserve(2 * sizeof(uint32_t)));
+  ddsolve_ctx::DeviceConstraint c;
+  c.kind = DDSOLVE_CONSTRAINT_REFERENCE_ANTENNA;
+  ctx->constraints.push_back(std::move(c));
+  ctx->DestroyGraph();
+  return DDSOLVE_OK;
+}
+
+int ddsolve_clear_constraints(ddsolve_ctx* ctx) {
+  if (!ctx) return DDSOLVE_E_INVALID;
+  ctx->constraints.clear();
+  ctx->DestroyGraph();
+  return DDSOLVE_OK;
 }
 
 int ddsolve_perform_iteration(ddsolve_ctx* ctx, const double* solutions,

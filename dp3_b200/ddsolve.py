@@ -26,7 +26,9 @@ EXPORTED_SYMBOLS = (
     "ddsolve_perform_iterations", "ddsolve_get_tuning", "ddsolve_set_plan_tuning",
     "ddsolve_autotune", "ddsolve_set_intervals", "ddsolve_solve_batch",
     "ddsolve_set_channel_block_regular_sky", "ddsolve_predict_regular",
-    "ddsolve_set_interval_buffers",
+    "ddsolve_set_interval_buffers", "ddsolve_add_smoothness_constraint",
+    "ddsolve_add_antenna_constraint", "ddsolve_add_reference_antenna_constraint",
+    "ddsolve_clear_constraints",
 )
 
 
@@ -102,6 +104,10 @@ def lib():
         L.ddsolve_perform_iterations.argtypes = [vp, vp, u32, vp]
         L.ddsolve_set_intervals.argtypes = [vp, u32, vp]
         L.ddsolve_solve_batch.argtypes = [vp, vp, vp, vp]
+        L.ddsolve_add_smoothness_constraint.argtypes = [vp, ctypes.POINTER(Smoothness)]
+        L.ddsolve_add_antenna_constraint.argtypes = [vp, u32, vp, vp]
+        L.ddsolve_add_reference_antenna_constraint.argtypes = [vp]
+        L.ddsolve_clear_constraints.argtypes = [vp]
         L.ddsolve_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
         L.ddsolve_set_plan_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
         L.ddsolve_autotune.argtypes = [vp, u32, ctypes.POINTER(Tuning),
@@ -140,6 +146,15 @@ class SkyDirection(ctypes.Structure):
     """ddsolve_sky_direction (include/ddsolve_b200.h)."""
     _fields_ = [("n_sources", ctypes.c_uint32), ("lmn", ctypes.c_void_p),
                 ("stokes", ctypes.c_void_p)]
+
+
+class Smoothness(ctypes.Structure):
+    """ddsolve_smoothness (include/ddsolve_b200.h)."""
+    _fields_ = [("frequencies", ctypes.c_void_p), ("bandwidth_hz", ctypes.c_double),
+                ("bandwidth_ref_frequency_hz", ctypes.c_double),
+                ("spectral_exponent", ctypes.c_double), ("kernel_truncation", ctypes.c_int32),
+                ("weights", ctypes.c_void_p), ("sub_solution_weights", ctypes.c_void_p),
+                ("antenna_factors", ctypes.c_void_p), ("dd_factors", ctypes.c_void_p)]
 
 
 class IntervalBuffers(ctypes.Structure):
@@ -320,13 +335,14 @@ class Context:
             model = np.ascontiguousarray(model, np.complex64)
             keep.append(model)
             ib.model = model.ctypes.data
-        else:
+        elif sky is not None:
             freqs = np.ascontiguousarray(frequencies, np.float64)
             uvw = np.ascontiguousarray(station_uvw, np.float64)
             sky_arr, sk = _sky_struct(sky)
             keep += [freqs, uvw, sky_arr, sk]
             ib.frequencies, ib.station_uvw = freqs.ctypes.data, uvw.ctypes.data
             ib.sky = ctypes.cast(sky_arr, ctypes.c_void_p).value
+        # (neither: the library refuses the call)
         ib.linear_weighting = int(linear_weighting)
         self._check(lib().ddsolve_set_interval_buffers(self._h, ctypes.byref(ib)),
                     "ddsolve_set_interval_buffers")
@@ -362,6 +378,45 @@ class Context:
         self._check(lib().ddsolve_set_intervals(self._h, len(f) - 1, _addr(f)),
                     "ddsolve_set_intervals")
         self.n_intervals = len(f) - 1
+
+    def add_smoothness_constraint(self, frequencies, bandwidth_hz, weights=None,
+                                  bandwidth_ref_frequency_hz=0.0, spectral_exponent=-1.0,
+                                  kernel_truncation=True, sub_solution_weights=None,
+                                  antenna_factors=None, dd_factors=None):
+        """Device SmoothnessConstraint (ddsolve_add_smoothness_constraint):
+        frequencies [n_cb] Hz; weights [n_ant * n_cb] or sub_solution_weights
+        [n_sub][n_ant * n_cb]; antenna_factors [n_ant]; dd_factors [n_sub]."""
+        arrays = [None if a is None else np.ascontiguousarray(a, np.float64)
+                  for a in (frequencies, weights, sub_solution_weights, antenna_factors,
+                            dd_factors)]
+        f, w, sw, af, dd = arrays
+        s = Smoothness(f.ctypes.data, float(bandwidth_hz), float(bandwidth_ref_frequency_hz),
+                       float(spectral_exponent), int(bool(kernel_truncation)),
+                       None if w is None else w.ctypes.data,
+                       None if sw is None else sw.ctypes.data,
+                       None if af is None else af.ctypes.data,
+                       None if dd is None else dd.ctypes.data)
+        self._check(lib().ddsolve_add_smoothness_constraint(self._h, ctypes.byref(s)),
+                    "ddsolve_add_smoothness_constraint")
+
+    def add_antenna_constraint(self, antenna_sets):
+        """Device AntennaConstraint over a list of antenna sets."""
+        sizes = [len(a) for a in antenna_sets]
+        off = np.ascontiguousarray(np.concatenate([[0], np.cumsum(sizes)]), np.uint32)
+        members = np.ascontiguousarray(
+            np.concatenate([np.asarray(a, np.uint32) for a in antenna_sets])
+            if antenna_sets else np.zeros(0, np.uint32), np.uint32)
+        self._check(lib().ddsolve_add_antenna_constraint(
+            self._h, len(antenna_sets), _addr(off), _addr(members)),
+            "ddsolve_add_antenna_constraint")
+
+    def add_reference_antenna_constraint(self):
+        """Device phase referencing (Constraint::ApplyReferenceAntenna)."""
+        self._check(lib().ddsolve_add_reference_antenna_constraint(self._h),
+                    "ddsolve_add_reference_antenna_constraint")
+
+    def clear_constraints(self):
+        self._check(lib().ddsolve_clear_constraints(self._h), "ddsolve_clear_constraints")
 
     def solve_batch(self, solutions, step_magnitudes=None):
         """Solves every interval; solutions [n_cb, ...] updated in place.

@@ -21,10 +21,13 @@
 // initial solutions with the iteration cap at that iteration, which gives
 // the solutions and the result of the stalled solve.
 //
-// Solve with constraints: DP3's own loop (IterativeDiagonalSolver.cc:38-97)
-// on the host -- MakeSolutionsFinite, Step, ApplyConstraints, AssignSolutions
-// and ReachedStoppingCriterion are SolverBase's own -- with PerformIteration
-// replaced by one device pass (ddsolve_perform_iteration).
+// Solve with constraints that all have a device form (DP3's AntennaConstraint
+// and SmoothnessConstraintB200 below): they become device constraints
+// (ddsolve_add_*_constraint) and the whole constrained loop runs on the
+// device as above. Otherwise DP3's own loop (IterativeDiagonalSolver.cc:
+// 38-97) on the host -- MakeSolutionsFinite, Step, ApplyConstraints,
+// AssignSolutions and ReachedStoppingCriterion are SolverBase's own -- with
+// PerformIteration replaced by one device pass (ddsolve_perform_iteration).
 //
 // The Solve(data, solutions, time, stat_stream) overload writes one line
 // "iteration step_magnitude" per iteration to stat_stream (cf. the
@@ -45,10 +48,89 @@
 #include <aocommon/matrix2x2diag.h>
 
 #include "ddsolve_b200.h"
+#include "ddecal/constraints/AntennaConstraint.h"
+#include "ddecal/constraints/SmoothnessConstraint.h"
 #include "ddecal/gain_solvers/SolveData.h"
 #include "ddecal/gain_solvers/SolverBase.h"
 
+// Progress hook (a no-op unless the includer defines it, e.g. a test
+// harness that logs where a solve is).
+#ifndef DP3B200_ADAPTER_TRACE
+#define DP3B200_ADAPTER_TRACE(what) ((void)0)
+#endif
+
 namespace dp3::ddecal {
+
+// DP3's SmoothnessConstraint with a device form. The same constructor and
+// setters (SmoothnessConstraint.h:18-75); Apply runs DP3's own
+// SmoothnessConstraint on the host (the host loop of IterativeSolverB200),
+// and IterativeSolverB200 hands the same settings to the device
+// (ddsolve_add_smoothness_constraint) when every constraint of a solve has a
+// device form, so that the constrained loop stays on the GPU. DP3's class is
+// final and keeps its settings private, hence a wrapper: SolverFactory
+// creates it in place of SmoothnessConstraint together with the B200 solver.
+class SmoothnessConstraintB200 final : public Constraint {
+ public:
+  SmoothnessConstraintB200(double bandwidth_hz, double bandwidth_ref_frequency_hz,
+                           double spectral_exponent, bool kernel_truncation)
+      : host_(bandwidth_hz, bandwidth_ref_frequency_hz, spectral_exponent, kernel_truncation),
+        bandwidth_hz_(bandwidth_hz),
+        bandwidth_ref_frequency_hz_(bandwidth_ref_frequency_hz),
+        spectral_exponent_(spectral_exponent),
+        kernel_truncation_(kernel_truncation) {}
+
+  void Initialize(size_t n_antennas, const std::vector<uint32_t>& solutions_per_direction,
+                  const std::vector<double>& frequencies) override {
+    Constraint::Initialize(n_antennas, solutions_per_direction, frequencies);
+    host_.Initialize(n_antennas, solutions_per_direction, frequencies);
+    frequencies_ = frequencies;
+  }
+  void SetWeights(const std::vector<double>& weights) override {
+    host_.SetWeights(weights);
+    weights_ = weights;
+  }
+  void SetSubSolutionWeights(const std::vector<std::vector<double>>& weights) override {
+    host_.SetSubSolutionWeights(weights);
+    sub_solution_weights_ = weights;
+  }
+  void SetAntennaFactors(std::vector<double>&& antenna_factors) {
+    antenna_factors_ = antenna_factors;
+    host_.SetAntennaFactors(std::move(antenna_factors));
+  }
+  const std::vector<double>& GetAntennaFactors() const { return antenna_factors_; }
+  void SetDdSmoothingFactors(std::vector<double> dd_smoothing_factors) {
+    host_.SetDdSmoothingFactors(dd_smoothing_factors);  // checks the size
+    dd_factors_ = std::move(dd_smoothing_factors);
+  }
+  const std::vector<double>& GetDdSmoothingFactors() const { return dd_factors_; }
+
+  void Apply(SolutionSpan& solutions, double time) override { host_.Apply(solutions, time); }
+
+  // Adds the device form to a context (status of the C ABI call).
+  int AddTo(ddsolve_ctx* ctx) const {
+    std::vector<double> flat_sub;
+    for (const std::vector<double>& w : sub_solution_weights_)
+      flat_sub.insert(flat_sub.end(), w.begin(), w.end());
+    ddsolve_smoothness s{};
+    s.frequencies = frequencies_.data();
+    s.bandwidth_hz = bandwidth_hz_;
+    s.bandwidth_ref_frequency_hz = bandwidth_ref_frequency_hz_;
+    s.spectral_exponent = spectral_exponent_;
+    s.kernel_truncation = kernel_truncation_ ? 1 : 0;
+    s.weights = weights_.empty() ? nullptr : weights_.data();
+    s.sub_solution_weights = flat_sub.empty() ? nullptr : flat_sub.data();
+    s.antenna_factors = antenna_factors_.empty() ? nullptr : antenna_factors_.data();
+    s.dd_factors = dd_factors_.empty() ? nullptr : dd_factors_.data();
+    return ddsolve_add_smoothness_constraint(ctx, &s);
+  }
+
+ private:
+  SmoothnessConstraint host_;
+  double bandwidth_hz_, bandwidth_ref_frequency_hz_, spectral_exponent_;
+  bool kernel_truncation_;
+  std::vector<double> frequencies_, weights_, antenna_factors_, dd_factors_;
+  std::vector<std::vector<double>> sub_solution_weights_;
+};
 
 template <typename VisMatrix, size_t NPol>
 class IterativeSolverB200 final : public SolverBase {
@@ -83,7 +165,7 @@ class IterativeSolverB200 final : public SolverBase {
                     std::vector<std::vector<DComplex>>& solutions, double time,
                     std::ostream* stat_stream) {
     Upload(data);
-    if (GetConstraints().empty()) return SolveOnDevice(solutions, stat_stream);
+    if (UploadDeviceConstraints()) return SolveOnDevice(solutions, stat_stream);
     return SolveWithHostConstraints(solutions, time, stat_stream);
   }
 
@@ -111,6 +193,7 @@ class IterativeSolverB200 final : public SolverBase {
                               uint32_t(NPol),
                               n_solutions_per_direction_.data()};
       Check(ddsolve_create(&dims, device_, &ctx_));
+      DP3B200_ADAPTER_TRACE("context created");
     }
     std::vector<uint32_t> pairs;
     for (size_t cb = 0; cb != data.NChannelBlocks(); ++cb) {
@@ -126,7 +209,34 @@ class IterativeSolverB200 final : public SolverBase {
           n ? reinterpret_cast<const float*>(&block.ModelVisibility(0, 0)) : nullptr;
       Check(ddsolve_set_channel_block(ctx_, uint32_t(cb), n, vis, model, pairs.data(),
                                       block.SolutionMapData()));
+      DP3B200_ADAPTER_TRACE("channel block uploaded");
     }
+  }
+
+  // The solver's constraints as device constraints, when every one has a
+  // device form (DP3's AntennaConstraint, SmoothnessConstraintB200); these
+  // are always satisfied (Constraint::Satisfied), so the device loop's
+  // stopping rule is DP3's. Returns false (device constraints cleared) when
+  // some constraint runs on the host only.
+  bool UploadDeviceConstraints() {
+    Check(ddsolve_clear_constraints(ctx_));
+    for (const std::unique_ptr<Constraint>& c : GetConstraints()) {
+      if (const auto* a = dynamic_cast<const AntennaConstraint*>(c.get())) {
+        std::vector<uint32_t> offsets{0}, antennas;
+        for (const std::set<size_t>& set : a->GetAntennaSets()) {
+          for (size_t ant : set) antennas.push_back(uint32_t(ant));
+          offsets.push_back(uint32_t(antennas.size()));
+        }
+        Check(ddsolve_add_antenna_constraint(ctx_, uint32_t(offsets.size() - 1),
+                                             offsets.data(), antennas.data()));
+      } else if (const auto* s = dynamic_cast<const SmoothnessConstraintB200*>(c.get())) {
+        Check(s->AddTo(ctx_));
+      } else {
+        Check(ddsolve_clear_constraints(ctx_));
+        return false;
+      }
+    }
+    return true;
   }
 
   ddsolve_settings DeviceSettings(uint32_t max_iterations) const {
@@ -169,7 +279,9 @@ class IterativeSolverB200 final : public SolverBase {
     ddsolve_settings s = DeviceSettings(max_it);
     Check(ddsolve_set_settings(ctx_, &s));
     ddsolve_result r;
+    DP3B200_ADAPTER_TRACE("device solve");
     Check(ddsolve_solve(ctx_, flat.data(), &r, mags.data()));
+    DP3B200_ADAPTER_TRACE("device solve done");
     size_t iteration = std::min<size_t>(r.has_converged ? r.iterations : r.iterations - 1,
                                         mags.size());
     bool has_converged = r.has_converged != 0;

@@ -143,6 +143,29 @@ auto reshape_view(E& e, const size_t (&shape)[M]) {
   return strided_view<T, M>(detail::DataOf(e), s, detail::RowMajorStrides<M>(s));
 }
 
+// xt::isfinite over a view: an owning boolean tensor of the view's shape.
+template <typename T, size_t M>
+xtensor<bool, M> isfinite(const strided_view<T, M>& v) {
+  xtensor<bool, M> out(v.shape());
+  v.for_each([&](T& x, size_t i) { out.data()[i] = detail::IsFiniteValue(x); });
+  return out;
+}
+
+// xt::sum(e)(): the sum of all elements (booleans count as 0 / 1), evaluated
+// when called, as DP3 uses the reducer.
+template <typename T>
+struct sum_result {
+  T value;
+  T operator()() const { return value; }
+};
+template <typename T, size_t N>
+auto sum(const xtensor<T, N>& t) {
+  using R = std::conditional_t<std::is_same_v<T, bool>, size_t, T>;
+  R s = R(0);
+  for (size_t i = 0; i != t.size(); ++i) s += R(t.data()[i]);
+  return sum_result<R>{s};
+}
+
 }  // namespace xt
 
 #endif

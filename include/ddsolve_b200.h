@@ -250,6 +250,67 @@ DDSOLVE_API int ddsolve_set_intervals(ddsolve_ctx* ctx, uint32_t n_intervals,
 DDSOLVE_API int ddsolve_solve_batch(ddsolve_ctx* ctx, double* solutions, ddsolve_result* results,
                                     double* step_magnitudes);
 
+/* Device-side constraints. SolverBase::ApplyConstraints (SolverBase.cc:
+ * 174-190) runs a solver's constraints on the host between SolverBase::Step
+ * and AssignSolutions (IterativeDiagonalSolver.cc:77-83); the constraints
+ * added here run on the device at that point of every iteration of
+ * ddsolve_solve, in the order they were added, so that a constrained solve
+ * stays in the device loop (one CUDA graph) instead of returning to the host
+ * once per iteration. All three are satisfied from the start
+ * (Constraint::Satisfied), so the stopping rule is the unconstrained one.
+ * The arithmetic is the reference's, in FP64, in its order of operations.
+ * Single-interval contexts only (DDSOLVE_E_UNSUPPORTED from
+ * ddsolve_solve_batch). Adding or clearing a constraint rebuilds the
+ * context's graph at the next solve. */
+#define DDSOLVE_CONSTRAINT_SMOOTHNESS 1
+#define DDSOLVE_CONSTRAINT_ANTENNA 2
+#define DDSOLVE_CONSTRAINT_REFERENCE_ANTENNA 3
+
+/* SmoothnessConstraint (ddecal/constraints/SmoothnessConstraint.cc:11-97)
+ * with its Gaussian KernelSmoother (KernelSmoother.h:69-160): every
+ * (antenna, sub-solution, polarization) series over channel blocks is
+ * replaced by its kernel-weighted mean; non-finite values get weight 0, and
+ * a mean over zero weight is NaN. */
+typedef struct {
+  const double* frequencies;          /* [n_channel_blocks] Hz, ascending
+                                         (Constraint::Initialize) */
+  double bandwidth_hz;                /* constructor arguments */
+  double bandwidth_ref_frequency_hz;
+  double spectral_exponent;
+  int32_t kernel_truncation;
+  const double* weights;              /* [n_antennas * n_channel_blocks]
+                                         (Constraint::SetWeights), or NULL
+                                         when sub_solution_weights is given */
+  const double* sub_solution_weights; /* NULL or [n_sub_solutions][n_antennas
+                                         * n_channel_blocks] (SetSubSolutionWeights,
+                                         used instead of weights) */
+  const double* antenna_factors;      /* [n_antennas] (SetAntennaFactors) or
+                                         NULL = all 1 */
+  const double* dd_factors;           /* NULL or [n_sub_solutions]
+                                         (SetDdSmoothingFactors) */
+} ddsolve_smoothness;
+
+DDSOLVE_API int ddsolve_add_smoothness_constraint(ddsolve_ctx* ctx,
+                                                  const ddsolve_smoothness* s);
+
+/* AntennaConstraint (ddecal/constraints/AntennaConstraint.h:29-82): set k
+ * holds antennas[set_offsets[k] .. set_offsets[k + 1]) (a std::set: order
+ * and repeats do not matter); per channel block, sub-solution and
+ * polarization every member gets the mean of the set's finite solutions. */
+DDSOLVE_API int ddsolve_add_antenna_constraint(ddsolve_ctx* ctx, uint32_t n_sets,
+                                               const uint32_t* set_offsets,
+                                               const uint32_t* antennas);
+
+/* Constraint::ApplyReferenceAntenna (ddecal/constraints/Constraint.cc:7-37),
+ * the phase referencing of DP3's TEC constraints: per polarization, every
+ * antenna's solutions divided by those of the first antenna whose
+ * sub-solution-0 solutions are finite in more than 20% of the channel
+ * blocks, which become 1. */
+DDSOLVE_API int ddsolve_add_reference_antenna_constraint(ddsolve_ctx* ctx);
+
+/* Removes every device constraint. */
+DDSOLVE_API int ddsolve_clear_constraints(ddsolve_ctx* ctx);
+
 /* One direction-iterative pass over every channel block:
  * next_solutions = sum(num) / sum(den) per antenna, sub-solution and
  * polarization, NaN where the denominator is zero -- exactly the

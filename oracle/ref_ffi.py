@@ -73,7 +73,10 @@ class Constraints(ctypes.Structure):
                 ("bandwidth_ref_frequency_hz", ctypes.c_double),
                 ("spectral_exponent", ctypes.c_double), ("kernel_truncation", ctypes.c_int32),
                 ("smoothness_weights", ctypes.c_void_p),
-                ("channel_block_frequencies", ctypes.c_void_p)]
+                ("channel_block_frequencies", ctypes.c_void_p),
+                ("antenna_factors", ctypes.c_void_p), ("dd_factors", ctypes.c_void_p),
+                ("sub_solution_weights", ctypes.c_void_p),
+                ("reference_antenna", ctypes.c_int32)]
 
 
 class Result(ctypes.Structure):
@@ -143,8 +146,8 @@ def _problem(cfg, antenna1, antenna2, data, model, ncorr):
     return p, (nspd, a1, a2, data, model, dp, mp)
 
 
-def _constraints(antenna_sets, smoothness, cb_frequencies):
-    if not (antenna_sets or smoothness):
+def _constraints(antenna_sets, smoothness, cb_frequencies, reference_antenna=False):
+    if not (antenna_sets or smoothness or reference_antenna):
         return None, ()
     freqs = np.ascontiguousarray(cb_frequencies, np.float64)
     keep = [freqs]
@@ -163,11 +166,20 @@ def _constraints(antenna_sets, smoothness, cb_frequencies):
         cons.bandwidth_ref_frequency_hz = smoothness.get("bandwidth_ref_frequency_hz", 0.0)
         cons.spectral_exponent = smoothness.get("spectral_exponent", -1.0)
         cons.kernel_truncation = int(smoothness.get("kernel_truncation", True))
+        for key, field in (("weights", "smoothness_weights"),
+                           ("antenna_factors", "antenna_factors"),
+                           ("dd_factors", "dd_factors"),
+                           ("sub_solution_weights", "sub_solution_weights")):
+            if smoothness.get(key) is not None:
+                a = np.ascontiguousarray(smoothness[key], np.float64)
+                keep.append(a)
+                setattr(cons, field, a.ctypes.data)
+    cons.reference_antenna = int(bool(reference_antenna))
     return cons, keep
 
 
 def solve(cfg, antenna1, antenna2, data, model, ncorr, npol, solutions, st, n_threads=1,
-          antenna_sets=None, smoothness=None, cb_frequencies=None):
+          antenna_sets=None, smoothness=None, cb_frequencies=None, reference_antenna=False):
     """Runs the reference's Solve on one regular interval.
 
     cfg: an ObservationConfig-like object (n_stations, n_times, n_baselines,
@@ -175,12 +187,15 @@ def solve(cfg, antenna1, antenna2, data, model, ncorr, npol, solutions, st, n_th
     updated in place. antenna_sets: list of antenna-index lists
     (AntennaConstraint); smoothness: dict(bandwidth_hz=...,
     bandwidth_ref_frequency_hz=0, spectral_exponent=-1, kernel_truncation=True)
-    (SmoothnessConstraint); cb_frequencies: mean frequency per channel block
-    (needed with any constraint). Returns the Result (iterations,
+    (SmoothnessConstraint; optional weights [n_ant * n_cb], antenna_factors
+    [n_ant], dd_factors [n_sub], sub_solution_weights [n_sub][n_ant * n_cb]);
+    reference_antenna: a last constraint that applies
+    Constraint::ApplyReferenceAntenna; cb_frequencies: mean frequency per
+    channel block (needed with any constraint). Returns the Result (iterations,
     constraint_iterations, seconds_packing, seconds_solve)."""
     assert solutions.dtype == np.complex128 and solutions.flags.c_contiguous
     p, keep = _problem(cfg, antenna1, antenna2, data, model, ncorr)
-    cons, keep_c = _constraints(antenna_sets, smoothness, cb_frequencies)
+    cons, keep_c = _constraints(antenna_sets, smoothness, cb_frequencies, reference_antenna)
     res = Result()
     rc = lib().ref_solve(ctypes.byref(p), ctypes.byref(st), kind_of(ncorr, npol), n_threads,
                          ctypes.byref(cons) if cons is not None else None,

@@ -75,6 +75,16 @@ typedef struct {
   const double* smoothness_weights;  // [n_antennas * n_channel_blocks] or NULL (all 1)
   // Mean frequency of each channel block (Constraint::Initialize).
   const double* channel_block_frequencies;  // [n_channel_blocks]
+  // SmoothnessConstraint::SetAntennaFactors [n_antennas] or NULL (all 1),
+  // SetDdSmoothingFactors [n_sub_solutions] or NULL (none), and
+  // SetSubSolutionWeights [n_sub_solutions][n_antennas * n_channel_blocks]
+  // or NULL (none).
+  const double* antenna_factors;
+  const double* dd_factors;
+  const double* sub_solution_weights;
+  // Appends a constraint whose Apply is Constraint::ApplyReferenceAntenna
+  // (the phase referencing of DP3's TEC constraints).
+  int32_t reference_antenna;
 } ref_constraints;
 
 typedef struct {
@@ -134,7 +144,20 @@ dp3::ddecal::SolveData<V> Pack(const ref_problem& p) {
                                    nspd, a1, a2);
 }
 
-// Initialize, setters and constraints, as SolverFactory does.
+// A constraint that only phase-references the solutions
+// (Constraint::ApplyReferenceAntenna, Constraint.cc:7-37), as DP3's TEC
+// constraints do when phase referencing is on.
+class ReferenceAntennaConstraint final : public dp3::ddecal::Constraint {
+ public:
+  void Apply(dp3::ddecal::SolutionSpan& solutions, double) override {
+    ApplyReferenceAntenna(solutions);
+  }
+};
+
+// Initialize, setters and constraints, as SolverFactory does. Smoothness: the
+// smoothness constraint class (DP3's, or one with the same constructor and
+// setters).
+template <typename Smoothness = dp3::ddecal::SmoothnessConstraint>
 inline void Configure(dp3::ddecal::SolverBase& solver, const ref_problem& p,
                       const ref_settings& s, const ref_constraints* c) {
   std::vector<size_t> nspd(p.n_solutions_per_direction,
@@ -164,15 +187,33 @@ inline void Configure(dp3::ddecal::SolverBase& solver, const ref_problem& p,
     solver.AddConstraint(std::move(ac));
   }
   if (c->smoothness) {
-    auto sc = std::make_unique<dp3::ddecal::SmoothnessConstraint>(
+    auto sc = std::make_unique<Smoothness>(
         c->bandwidth_hz, c->bandwidth_ref_frequency_hz, c->spectral_exponent,
         c->kernel_truncation != 0);
     sc->Initialize(p.n_antennas, spd, freqs);
     std::vector<double> w(size_t(p.n_antennas) * p.n_channel_blocks, 1.0);
     if (c->smoothness_weights) std::copy_n(c->smoothness_weights, w.size(), w.begin());
     sc->SetWeights(w);
-    sc->SetAntennaFactors(std::vector<double>(p.n_antennas, 1.0));
+    std::vector<double> af(p.n_antennas, 1.0);
+    if (c->antenna_factors) std::copy_n(c->antenna_factors, af.size(), af.begin());
+    sc->SetAntennaFactors(std::move(af));
+    size_t n_sub = 0;
+    for (uint32_t d = 0; d < p.n_directions; ++d) n_sub += p.n_solutions_per_direction[d];
+    if (c->dd_factors)
+      sc->SetDdSmoothingFactors(std::vector<double>(c->dd_factors, c->dd_factors + n_sub));
+    if (c->sub_solution_weights) {
+      std::vector<std::vector<double>> sw(n_sub);
+      for (size_t s = 0; s < n_sub; ++s)
+        sw[s].assign(c->sub_solution_weights + s * w.size(),
+                     c->sub_solution_weights + (s + 1) * w.size());
+      sc->SetSubSolutionWeights(sw);
+    }
     solver.AddConstraint(std::move(sc));
+  }
+  if (c->reference_antenna) {
+    auto rc = std::make_unique<ReferenceAntennaConstraint>();
+    rc->Initialize(p.n_antennas, spd, freqs);
+    solver.AddConstraint(std::move(rc));
   }
 }
 

@@ -9,10 +9,19 @@
 // libddsolve_b200.so on the GPU.
 //
 // TEST INFRASTRUCTURE: only tests/test_dp3_adapter.py loads this library.
+#include <execinfo.h>
+#include <signal.h>
+#include <unistd.h>
+
+#include <cstdlib>
 #include <sstream>
 #include <stdexcept>
 #include <string>
 
+namespace {
+void Trace(const char* what);
+}
+#define DP3B200_ADAPTER_TRACE(what) Trace(what)
 #include "dp3/IterativeSolverB200.h"
 #include "ddecal/gain_solvers/IterativeDiagonalSolver.h"
 #include "ddecal/gain_solvers/IterativeScalarSolver.h"
@@ -33,11 +42,54 @@ namespace {
 
 thread_local std::string g_error;
 
-template <typename Solver, typename V>
+// With DP3B200_HARNESS_BACKTRACE set: progress lines on stderr around the
+// solver calls, and a native backtrace when the process takes SIGSEGV /
+// SIGABRT (library offsets, resolvable with addr2line against the same
+// build), printed from an alternate signal stack so that a stack overflow is
+// reported too; then the default action.
+bool g_trace = false;
+void Trace(const char* what) {
+  if (!g_trace) return;
+  const std::string line = std::string("harness: ") + what + "\n";
+  (void)!write(2, line.data(), line.size());
+}
+void CrashReport(int sig, siginfo_t* info, void*) {
+  char head[96];
+  const int len = snprintf(head, sizeof(head), "harness: signal %d at address %p\n", sig,
+                           info ? info->si_addr : nullptr);
+  (void)!write(2, head, size_t(len));
+  void* frames[64];
+  const int n = backtrace(frames, 64);
+  backtrace_symbols_fd(frames, n, 2);
+  signal(sig, SIG_DFL);
+  raise(sig);
+}
+struct CrashReporter {
+  CrashReporter() {
+    if (!std::getenv("DP3B200_HARNESS_BACKTRACE")) return;
+    g_trace = true;
+    static char alt_stack[1 << 16];
+    stack_t ss{};
+    ss.ss_sp = alt_stack;
+    ss.ss_size = sizeof(alt_stack);
+    sigaltstack(&ss, nullptr);
+    struct sigaction sa {};
+    sa.sa_sigaction = CrashReport;
+    sa.sa_flags = SA_SIGINFO | SA_ONSTACK;
+    sigaction(SIGSEGV, &sa, nullptr);
+    sigaction(SIGABRT, &sa, nullptr);
+    sigaction(SIGBUS, &sa, nullptr);
+  }
+} g_crash_reporter;
+
+template <typename Solver, typename V,
+          typename Smoothness = dp3::ddecal::SmoothnessConstraint>
 int Run(Solver& solver, const ref_problem& p, const ref_settings& s, const ref_constraints* c,
         double* solutions, ref_result* out, double* step_magnitudes, uint32_t n_step_cap) {
+  Trace("pack");
   const dp3::ddecal::SolveData<V> data = dp3b200_ref::Pack<V>(p);
-  dp3b200_ref::Configure(solver, p, s, c);
+  Trace("configure");
+  dp3b200_ref::Configure<Smoothness>(solver, p, s, c);
   const size_t n_sub = std::accumulate(p.n_solutions_per_direction,
                                        p.n_solutions_per_direction + p.n_directions, size_t(0));
   const size_t per_cb = size_t(p.n_antennas) * n_sub * solver.NSolutionPolarizations();
@@ -46,7 +98,9 @@ int Run(Solver& solver, const ref_problem& p, const ref_settings& s, const ref_c
   if constexpr (std::is_same_v<Solver, dp3::ddecal::IterativeSolverB200<V, 2>> ||
                 std::is_same_v<Solver, dp3::ddecal::IterativeSolverB200<V, 1>>) {
     std::ostringstream stats;  // the statistics-stream overload
+    Trace("adapter solve");
     r = solver.Solve(data, sol, 0.0, &stats);
+    Trace("adapter solve done");
     std::istringstream in(stats.str());
     size_t it;
     double mag;
@@ -56,6 +110,7 @@ int Run(Solver& solver, const ref_problem& p, const ref_settings& s, const ref_c
     r = solver.Solve(data, sol, 0.0);
   }
   dp3b200_ref::FromVectors(sol, solutions);
+  Trace("results copied");
   out->iterations = uint32_t(r.iterations);
   out->constraint_iterations = uint32_t(r.constraint_iterations);
   return 0;
@@ -66,6 +121,12 @@ int Dispatch(int use_b200, int device, const ref_problem& p, const ref_settings&
              const ref_constraints* c, double* solutions, ref_result* out, double* mags,
              uint32_t cap) {
   using namespace dp3::ddecal;
+  if (use_b200 == 2) {  // smoothness through the adapter's device-capable class
+    IterativeSolverB200<V, NPol> solver(device);
+    return Run<IterativeSolverB200<V, NPol>, V, SmoothnessConstraintB200>(solver, p, s, c,
+                                                                         solutions, out, mags,
+                                                                         cap);
+  }
   if (use_b200) {
     IterativeSolverB200<V, NPol> solver(device);
     return Run<IterativeSolverB200<V, NPol>, V>(solver, p, s, c, solutions, out, mags, cap);
@@ -84,7 +145,10 @@ int Dispatch(int use_b200, int device, const ref_problem& p, const ref_settings&
 extern "C" HARNESS_API const char* adapter_last_error(void) { return g_error.c_str(); }
 
 // kind: REF_* of ref_problem.h; use_b200: 0 = DP3's own solver, 1 = the B200
-// adapter on CUDA device `device`. step_magnitudes (optional, adapter only):
+// adapter on CUDA device `device` with DP3's constraint classes (a
+// SmoothnessConstraint keeps the loop on the host), 2 = the adapter with its
+// SmoothnessConstraintB200 (with DP3's AntennaConstraint: device constraints,
+// the loop on the device). step_magnitudes (optional, adapter only):
 // the statistics stream's per-iteration step magnitudes, up to n_step_cap.
 extern "C" HARNESS_API int adapter_solve(const ref_problem* p, const ref_settings* s, int kind,
                                          int use_b200, int device, uint32_t n_threads,
