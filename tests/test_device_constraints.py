@@ -133,7 +133,7 @@ def test_device_constraints_match_reference(built, ncorr, npol, name):
     ctx.close()
     assert res.iterations == rr.iterations
     assert H.max_rel_diff(got, ref) < RTOL
-    if case.get("antenna_sets"):
+    if name == "antenna":  # the last constraint applied: the sets share one solution
         for s in case["antenna_sets"]:
             s = sorted(s)
             np.testing.assert_allclose(got[:, s[1:]], np.repeat(got[:, s[:1]], len(s) - 1, 1),
