@@ -436,6 +436,58 @@ def run_mlp_infer(args):
     return 0
 
 
+def run_predict_only(args):
+    """The GPU point-source predict alone on configuration `args.config`
+    (default the 62-station interval: 10 directions x 20 sources, 24 blocks
+    of 10 channels, 8 timesteps): every channel block's model visibilities
+    predicted into device memory (ddsolve_predict_regular, one predict_kernel
+    launch per block), timed with CUDA events on the context's stream; the
+    command the predict profile uses. Prints the device time per interval,
+    the source-visibility terms per second and the model bytes written."""
+    import torch
+    from dp3_b200 import build as native_build
+    from dp3_b200 import ddsolve, synth
+    native_build.build_all()
+    torch.cuda.set_device(0)
+    cfg = synth.benchmark_configs()[args.config]
+    ctx = ddsolve.Context(cfg.n_stations, cfg.nspd, cfg.n_channel_blocks, 2, 2)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device="cuda:0")
+    sky = synth.sky(cfg)
+    uvw = synth.station_uvw(cfg)
+    # cross baselines in the generator's order: (0, 1), (0, 2), ..., (1, 2), ...
+    a1, a2 = (np.ascontiguousarray(x, np.uint32) for x in np.triu_indices(cfg.n_stations, 1))
+    freqs = synth.frequencies(cfg)
+    edges = np.cumsum([0] + list(cfg.cb_channels))
+    cb_freqs = [np.ascontiguousarray(freqs[edges[i]:edges[i + 1]])
+                for i in range(cfg.n_channel_blocks)]
+    outs = [torch.empty((cfg.n_directions, cfg.n_times * cfg.n_baselines * len(f), 2, 2),
+                        dtype=torch.float32, device="cuda:0") for f in cb_freqs]
+
+    def predict():
+        for cb, f in enumerate(cb_freqs):
+            ctx.predict_regular(cfg.n_times, cfg.n_baselines, f, uvw, a1, a2, sky, out=outs[cb])
+
+    for _ in range(args.warmup):
+        predict()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        predict()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    terms = cfg.n_vis * sum(len(l) for l, _ in sky)  # sources x visibilities
+    out_bytes = sum(o.numel() * 4 for o in outs)
+    print(json.dumps({"config": cfg.name, "predict_ms_per_interval": ms,
+                      "source_visibility_terms_per_s": terms / (ms / 1e3),
+                      "model_bytes": out_bytes,
+                      "model_write_gbs": out_bytes / (ms / 1e3) / 1e9}), flush=True)
+    ctx.close()
+    return 0
+
+
 def run_fp64_check(args):
     """Solution error of the GPU solver against the FP64 oracle on
     configuration `args.config` (a numerical statement, not a timing): one
@@ -905,6 +957,8 @@ def main():
                     help="independent intervals of --config solved in one context")
     ap.add_argument("--mlp-infer", action="store_true",
                     help="time only the warm-start network's forward pass (for profiling)")
+    ap.add_argument("--predict-only", action="store_true",
+                    help="time only the GPU point-source predict of --config (for profiling)")
     ap.add_argument("--mlp-only", action="store_true",
                     help="time only the warm-start network's training (for profiling)")
     ap.add_argument("--mlp-rows", type=int, default=60000)
@@ -920,6 +974,8 @@ def main():
         return run_mlp_only(args)
     if args.mlp_infer:
         return run_mlp_infer(args)
+    if args.predict_only:
+        return run_predict_only(args)
     if args.fp64_check:
         return run_fp64_check(args)
     if args.batch > 1:
