@@ -331,6 +331,56 @@ struct PredictParams {
   double df;
 };
 
+// One source's phasor exp(i dphi nu) across the channels of a chunk and its
+// correlation fluxes (XX = I + Q, XY = U + iV, YX = U - iV, YY = I - Q; for 1
+// and 2 correlations real, so a term is two multiply-adds per correlation).
+template <int NCORR, int CH>
+struct PredictSource {
+  double dphi, zs, zc, ss = 0.0, sc = 1.0;
+  double re[NCORR], im[NCORR];
+  __device__ __forceinline__ void Start(const double* q, double du, double dv, double dw,
+                                        const PredictParams& p, uint32_t c0) {
+    dphi = kTwoPiOverC * (du * q[0] + dv * q[1] + dw * q[2]);  // phi_q - phi_p per Hz
+    sincos(dphi * p.freq[c0], &zs, &zc);
+    if (p.uniform) sincos(dphi * p.df, &ss, &sc);
+    if (NCORR == 1) {
+      re[0] = q[3];
+    } else if (NCORR == 2) {
+      re[0] = q[3] + q[4];
+      re[NCORR - 1] = q[3] - q[4];
+    } else {
+      re[0] = q[3] + q[4];
+      re[1] = q[5];
+      re[2] = q[5];
+      re[NCORR - 1] = q[3] - q[4];
+      im[0] = im[NCORR - 1] = 0.0;
+      im[1] = q[6];
+      im[2] = -q[6];
+    }
+  }
+  __device__ __forceinline__ void Advance(const PredictParams& p, uint32_t ch) {
+    if (p.uniform) {
+      const double r = zc * sc - zs * ss;
+      zs = zc * ss + zs * sc;
+      zc = r;
+    } else {
+      sincos(dphi * p.freq[ch], &zs, &zc);
+    }
+  }
+  __device__ __forceinline__ void AddTo(double2 (&acc)[NCORR]) const {
+#pragma unroll
+    for (int k = 0; k < NCORR; ++k) {
+      if (NCORR == 4) {
+        acc[k].x += re[k] * zc - im[k] * zs;
+        acc[k].y += re[k] * zs + im[k] * zc;
+      } else {
+        acc[k].x += re[k] * zc;
+        acc[k].y += re[k] * zs;
+      }
+    }
+  }
+};
+
 template <int NCORR>
 __global__ void __launch_bounds__(kPredictThreads) predict_kernel(const PredictParams p) {
   constexpr int CH = kPredictChunk / NCORR;
@@ -359,42 +409,34 @@ __global__ void __launch_bounds__(kPredictThreads) predict_kernel(const PredictP
     for (int c = 0; c < CH; ++c)
 #pragma unroll
       for (int k = 0; k < NCORR; ++k) acc[c][k] = make_double2(0.0, 0.0);
-    for (uint32_t s = 0; s < ns; ++s) {
-      const double* q = src + s * 8;
-      // phi_q - phi_p per Hz
-      const double dphi = kTwoPiOverC * (du * q[0] + dv * q[1] + dw * q[2]);
-      double zs, zc, ss = 0.0, sc = 1.0;
-      sincos(dphi * p.freq[c0], &zs, &zc);
-      if (p.uniform) sincos(dphi * p.df, &ss, &sc);
-      double2 stokes[NCORR];
-      if (NCORR == 1) {
-        stokes[0] = make_double2(q[3], 0.0);
-      } else if (NCORR == 2) {
-        stokes[0] = make_double2(q[3] + q[4], 0.0);
-        stokes[NCORR - 1] = make_double2(q[3] - q[4], 0.0);
-      } else {
-        stokes[0] = make_double2(q[3] + q[4], 0.0);
-        stokes[1] = make_double2(q[5], q[6]);
-        stokes[2] = make_double2(q[5], -q[6]);
-        stokes[NCORR - 1] = make_double2(q[3] - q[4], 0.0);
-      }
+    // Two sources at a time: their phasor chains are independent, so the
+    // FP64 rotations of one fill the latency of the other's. Per channel the
+    // sources are still added in order.
+    uint32_t s = 0;
+    for (; s + 2 <= ns; s += 2) {
+      PredictSource<NCORR, CH> a, b;
+      a.Start(src + s * 8, du, dv, dw, p, c0);
+      b.Start(src + (s + 1) * 8, du, dv, dw, p, c0);
 #pragma unroll
       for (int c = 0; c < CH; ++c) {
         if (c < int(nc)) {
           if (c > 0) {
-            if (p.uniform) {
-              const double r = zc * sc - zs * ss;
-              zs = zc * ss + zs * sc;
-              zc = r;
-            } else {
-              sincos(dphi * p.freq[c0 + c], &zs, &zc);
-            }
+            a.Advance(p, c0 + c);
+            b.Advance(p, c0 + c);
           }
+          a.AddTo(acc[c]);
+          b.AddTo(acc[c]);
+        }
+      }
+    }
+    if (s < ns) {
+      PredictSource<NCORR, CH> a;
+      a.Start(src + s * 8, du, dv, dw, p, c0);
 #pragma unroll
-          for (int k = 0; k < NCORR; ++k) {
-            acc[c][k].x += stokes[k].x * zc - stokes[k].y * zs;
-            acc[c][k].y += stokes[k].x * zs + stokes[k].y * zc;
-          }
+      for (int c = 0; c < CH; ++c) {
+        if (c < int(nc)) {
+          if (c > 0) a.Advance(p, c0 + c);
+          a.AddTo(acc[c]);
         }
       }
     }
@@ -2180,10 +2222,19 @@ __global__ void __launch_bounds__(kPipeThreads, 1) pipe_kernel(const PipeParams 
     t_pair[ctid] = active ? (a1 | (a2 << 16)) : 0xFFFFFFFFu;
     for (uint32_t i = ctid; i < p.n_ant; i += kPipeRuns) a_cnt[i] = 0;
     ConsumerBarrier();
+    // Ranks in run order (entries (run, side) of an antenna sorted by run, so
+    // that the owner's sum has a fixed order); the counts by atomics.
     uint32_t rank1 = 0, rank2 = 0;
     if (active) {
-      rank1 = atomicAdd(&a_cnt[a1], 1u);
-      rank2 = atomicAdd(&a_cnt[a2], 1u);
+      for (uint32_t j = 0; j < uint32_t(ctid); ++j) {
+        const uint32_t pr = t_pair[j];
+        if (pr == 0xFFFFFFFFu) continue;
+        const uint32_t x1 = pr & 0xFFFFu, x2 = pr >> 16;
+        rank1 += uint32_t(x1 == a1) + uint32_t(x2 == a1);
+        rank2 += uint32_t(x1 == a2) + uint32_t(x2 == a2);
+      }
+      atomicAdd(&a_cnt[a1], 1u);
+      atomicAdd(&a_cnt[a2], 1u);
     }
     ConsumerBarrier();
     {
@@ -2487,6 +2538,386 @@ __global__ void __launch_bounds__(256)
 }
 
 // ---------------------------------------------------------------------------
+// Full-Jones solver: IterativeFullJonesSolver (ddecal/gain_solvers/
+// IterativeFullJonesSolver.cc:17-228). 2x2 complex gains J per antenna and
+// sub-solution on 4-correlation data; the model correction of direction d is
+// J_1 M_d J_2^H. Per antenna a and sub-solution, with the residual R = D -
+// sum_d J_1 M_d J_2^H and the add-back identity R_d = R + J_1 M_d J_2^H:
+//   side 1 (a = antenna 1): X = J_2 M^H,  num = sum R_d X   = P_1 + J_a den_1,
+//                           den_1 = sum X^H X
+//   side 2 (a = antenna 2): Y = J_1 M,    num = sum R_d^H Y = P_2 + J_a den_2,
+//                           den_2 = sum Y^H Y
+// (IterativeFullJonesSolver.cc:107-187), next = num den^-1 (NaN where den is
+// singular). fj_pass_kernel: one thread per run of visibilities (fixed
+// baseline and sub-solutions), FP32 products and sums as the reference's
+// MC2x2F arithmetic, the run's P and den of every direction and side written
+// to its own partial slot (no atomics); fj_finalize_kernel: one thread per
+// (channel block, antenna, sub-solution), the slots of its list summed in
+// FP64 in run order, the 2x2 inverse and product in FP64, then Step, the
+// 4-polarization AssignSolutions norm (SolverBase.cc:268-284) and the loop
+// control, as finalize_kernel does for 1 and 2 polarizations.
+// ---------------------------------------------------------------------------
+struct C22 {  // row-major [m0 m1; m2 m3]
+  float2 m[4];
+};
+__device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 c) {  // a b + c
+  return make_float2(fmaf(a.x, b.x, fmaf(-a.y, b.y, c.x)), fmaf(a.x, b.y, fmaf(a.y, b.x, c.y)));
+}
+__device__ __forceinline__ float2 cfma_conj(float2 a, float2 b, float2 c) {  // a conj(b) + c
+  return make_float2(fmaf(a.x, b.x, fmaf(a.y, b.y, c.x)), fmaf(a.y, b.x, fmaf(-a.x, b.y, c.y)));
+}
+__device__ __forceinline__ float2 cconj_fma(float2 a, float2 b, float2 c) {  // conj(a) b + c
+  return make_float2(fmaf(a.x, b.x, fmaf(a.y, b.y, c.x)), fmaf(a.x, b.y, fmaf(-a.y, b.x, c.y)));
+}
+__device__ __forceinline__ C22 Mul22(const C22& x, const C22& y) {  // x y
+  C22 r;
+  const float2 z = make_float2(0.f, 0.f);
+  r.m[0] = cfma(x.m[1], y.m[2], cmul(x.m[0], y.m[0]));
+  r.m[1] = cfma(x.m[1], y.m[3], cmul(x.m[0], y.m[1]));
+  r.m[2] = cfma(x.m[3], y.m[2], cmul(x.m[2], y.m[0]));
+  r.m[3] = cfma(x.m[3], y.m[3], cmul(x.m[2], y.m[1]));
+  (void)z;
+  return r;
+}
+__device__ __forceinline__ C22 MulHerm22(const C22& x, const C22& y) {  // x y^H
+  C22 r;
+  r.m[0] = cfma_conj(x.m[1], y.m[1], cmul_conj(x.m[0], y.m[0]));
+  r.m[1] = cfma_conj(x.m[1], y.m[3], cmul_conj(x.m[0], y.m[2]));
+  r.m[2] = cfma_conj(x.m[3], y.m[1], cmul_conj(x.m[2], y.m[0]));
+  r.m[3] = cfma_conj(x.m[3], y.m[3], cmul_conj(x.m[2], y.m[2]));
+  return r;
+}
+// acc += x^H y
+__device__ __forceinline__ void AddHermMul22(C22& acc, const C22& x, const C22& y) {
+  acc.m[0] = cconj_fma(x.m[2], y.m[2], cconj_fma(x.m[0], y.m[0], acc.m[0]));
+  acc.m[1] = cconj_fma(x.m[2], y.m[3], cconj_fma(x.m[0], y.m[1], acc.m[1]));
+  acc.m[2] = cconj_fma(x.m[3], y.m[2], cconj_fma(x.m[1], y.m[0], acc.m[2]));
+  acc.m[3] = cconj_fma(x.m[3], y.m[3], cconj_fma(x.m[1], y.m[1], acc.m[3]));
+}
+// acc += x y
+__device__ __forceinline__ void AddMul22(C22& acc, const C22& x, const C22& y) {
+  acc.m[0] = cfma(x.m[1], y.m[2], cfma(x.m[0], y.m[0], acc.m[0]));
+  acc.m[1] = cfma(x.m[1], y.m[3], cfma(x.m[0], y.m[1], acc.m[1]));
+  acc.m[2] = cfma(x.m[3], y.m[2], cfma(x.m[2], y.m[0], acc.m[2]));
+  acc.m[3] = cfma(x.m[3], y.m[3], cfma(x.m[2], y.m[1], acc.m[3]));
+}
+__device__ __forceinline__ C22 LoadC22(const float2* p) {
+  C22 r;
+  const float4 a = reinterpret_cast<const float4*>(p)[0];
+  const float4 b = reinterpret_cast<const float4*>(p)[1];
+  r.m[0] = make_float2(a.x, a.y);
+  r.m[1] = make_float2(a.z, a.w);
+  r.m[2] = make_float2(b.x, b.y);
+  r.m[3] = make_float2(b.z, b.w);
+  return r;
+}
+__device__ __forceinline__ C22 LoadJones(const double2* s) {  // FP32, as MC2x2F(&solutions[..])
+  C22 r;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) r.m[k] = make_float2(float(s[k].x), float(s[k].y));
+  return r;
+}
+
+constexpr int kFjThreads = 128;
+constexpr int kFjMaxDirections = 4;
+constexpr uint32_t kFjSlotFloats = 32;  // per run and direction: P and den of both sides
+
+struct FjPassParams {
+  const SlabDesc* slabs;
+  const uint32_t* slab_sol;   // [slab][n_dir]
+  const uint32_t* run_start;  // [n_slabs + 1]: first global run of each slab
+  const double2* solutions;   // [cb][ant][sub][4]
+  float* partials;            // [global run][direction][kFjSlotFloats]
+  uint32_t n_slabs, n_runs, n_ant, n_sub, n_dir;
+  const LoopState* state;
+  int32_t use_handle;
+};
+
+template <int ND>
+__global__ void __launch_bounds__(kFjThreads) fj_pass_kernel(const FjPassParams p) {
+  if (SolveStopped(p.state, p.use_handle)) return;
+  const uint32_t gr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gr >= p.n_runs) return;
+  uint32_t lo = 0, hi = p.n_slabs;  // the slab holding global run gr
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) / 2;
+    if (p.run_start[mid] <= gr)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const SlabDesc sl = p.slabs[lo];
+  const uint32_t r = gr - p.run_start[lo];
+  const uint32_t ap = sl.run_ant[r];
+  const uint32_t a1 = ap & 0xFFFFu, a2 = ap >> 16;
+  const size_t cb_off = size_t(sl.cb) * p.n_ant * p.n_sub;
+  C22 J1[ND], J2[ND], P1[ND], D1[ND], P2[ND], D2[ND];
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    const uint32_t s = p.slab_sol[sl.sol_off + d];
+    J1[d] = LoadJones(p.solutions + (cb_off + size_t(a1) * p.n_sub + s) * 4);
+    J2[d] = LoadJones(p.solutions + (cb_off + size_t(a2) * p.n_sub + s) * 4);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      P1[d].m[k] = D1[d].m[k] = P2[d].m[k] = D2[d].m[k] = make_float2(0.f, 0.f);
+  }
+  const float2* vis = static_cast<const float2*>(sl.vis);
+  const uint64_t rows = uint64_t(sl.T) * sl.L;
+  for (uint64_t row = 0; row < rows; ++row) {
+    C22 M[ND];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) M[d] = LoadC22(vis + SlabElem(sl.R, sl.W, ND + 1, row, 1 + d, r) * 4);
+    C22 R = LoadC22(vis + SlabElem(sl.R, sl.W, ND + 1, row, 0, r) * 4);
+    C22 Y[ND];  // J_1 M
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      Y[d] = Mul22(J1[d], M[d]);
+      const C22 t = MulHerm22(Y[d], J2[d]);  // J_1 M J_2^H
+#pragma unroll
+      for (int k = 0; k < 4; ++k) R.m[k] = make_float2(R.m[k].x - t.m[k].x, R.m[k].y - t.m[k].y);
+    }
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      const C22 X = MulHerm22(J2[d], M[d]);  // J_2 M^H
+      AddMul22(P1[d], R, X);
+      AddHermMul22(D1[d], X, X);
+      AddHermMul22(P2[d], R, Y[d]);
+      AddHermMul22(D2[d], Y[d], Y[d]);
+    }
+  }
+  float* out = p.partials + size_t(gr) * ND * kFjSlotFloats;
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    const C22* parts[4] = {&P1[d], &D1[d], &P2[d], &D2[d]};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      float4* o = reinterpret_cast<float4*>(out + d * kFjSlotFloats + q * 8);
+      o[0] = make_float4(parts[q]->m[0].x, parts[q]->m[0].y, parts[q]->m[1].x, parts[q]->m[1].y);
+      o[1] = make_float4(parts[q]->m[2].x, parts[q]->m[2].y, parts[q]->m[3].x, parts[q]->m[3].y);
+    }
+  }
+}
+
+struct D22 {
+  double2 m[4];
+};
+__device__ __forceinline__ D22 DMul22(const D22& x, const D22& y) {
+  D22 r;
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const double2 a = dmul(x.m[2 * i], y.m[j]), b = dmul(x.m[2 * i + 1], y.m[2 + j]);
+      r.m[2 * i + j] = make_double2(a.x + b.x, a.y + b.y);
+    }
+  return r;
+}
+// x^-1, false when singular (det == 0), as aocommon's Matrix2x2::Invert.
+__device__ __forceinline__ bool DInvert22(D22& x) {
+  const double2 a = dmul(x.m[0], x.m[3]), b = dmul(x.m[1], x.m[2]);
+  const double2 det = make_double2(a.x - b.x, a.y - b.y);
+  if (det.x == 0.0 && det.y == 0.0) return false;
+  const double2 inv = dinv(det);
+  const double2 m0 = x.m[0];
+  x.m[0] = dmul(x.m[3], inv);
+  x.m[1] = dmul(make_double2(-x.m[1].x, -x.m[1].y), inv);
+  x.m[2] = dmul(make_double2(-x.m[2].x, -x.m[2].y), inv);
+  x.m[3] = dmul(m0, inv);
+  return true;
+}
+
+struct FjFinParams {
+  const float* partials;
+  const uint32_t* list_off;   // [n_cb * n_ant * n_sub + 1]
+  const uint32_t* list_ent;   // (slot index << 1) | side, slot = global run * n_dir + d
+  double2* solutions;         // [cb][ant][sub][4]
+  double2* next_out;          // host mode
+  uint32_t n_items, n_dir;
+  uint32_t n_ant, n_sub;
+  int32_t host_mode;
+  const DevSettings* settings;
+  double* block_sum;
+  uint32_t* block_cnt;
+  LoopState* state;
+  uint32_t* nonfinite;        // [n_cb]
+  double* step_magnitudes;
+  cudaGraphConditionalHandle handle;
+  int32_t use_handle;
+  uint32_t* blocks_done;
+};
+
+__global__ void __launch_bounds__(kThreads) fj_finalize_kernel(const FjFinParams p) {
+  const uint32_t item = blockIdx.x * blockDim.x + threadIdx.x;
+  const DevSettings st = *p.settings;
+  const bool stopped = !p.host_mode && p.state->done;
+  double norm_sum = 0.0;
+  uint32_t norm_cnt = 0;
+  if (item < p.n_items && !stopped) {
+    // the item's slots, in run order: P and den of its side
+    double pn[8], dn[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) pn[k] = dn[k] = 0.0;
+    for (uint32_t e = p.list_off[item]; e < p.list_off[item + 1]; ++e) {
+      const uint32_t en = p.list_ent[e];
+      const float* slot = p.partials + size_t(en >> 1) * kFjSlotFloats + (en & 1u) * 16;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        pn[k] += double(__ldcg(slot + k));
+        dn[k] += double(__ldcg(slot + 8 + k));
+      }
+    }
+    double2* sol = p.solutions + size_t(item) * 4;
+    D22 old, ja, den, num;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      old.m[k] = sol[k];
+      ja.m[k] = make_double2(double(float(old.m[k].x)), double(float(old.m[k].y)));
+      den.m[k] = make_double2(dn[2 * k], dn[2 * k + 1]);
+    }
+    // num = P + J_a den (the add-back of the item's own direction)
+    num = DMul22(ja, den);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) num.m[k] = make_double2(num.m[k].x + pn[2 * k], num.m[k].y + pn[2 * k + 1]);
+    D22 nxt;
+    if (DInvert22(den)) {
+      nxt = DMul22(num, den);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) nxt.m[k] = make_double2(nan(""), nan(""));
+    }
+    if (p.host_mode) {
+      double2* out = p.next_out + size_t(item) * 4;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) out[k] = nxt.m[k];
+    } else {
+      // SolverBase::Step (SolverBase.cc:88-158), element by element
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (!st.phase_only) {
+          nxt.m[k] = make_double2(old.m[k].x * (1.0 - st.step_size) + nxt.m[k].x * st.step_size,
+                                  old.m[k].y * (1.0 - st.step_size) + nxt.m[k].y * st.step_size);
+        } else {
+          const double from = atan2(old.m[k].y, old.m[k].x);
+          double dist = atan2(nxt.m[k].y, nxt.m[k].x) - from;
+          if (dist > M_PI)
+            dist -= 2.0 * M_PI;
+          else if (dist < -M_PI)
+            dist += 2.0 * M_PI;
+          double sn, cs;
+          sincos(from + st.step_size * dist, &sn, &cs);
+          nxt.m[k] = make_double2(cs, sn);
+        }
+      }
+      // AssignSolutions, 4 polarizations (SolverBase.cc:268-284):
+      // |(new - old) old^-1| summed over the four elements
+      D22 inv = old;
+      if (DInvert22(inv)) {
+        D22 diff;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          diff.m[k] = make_double2(nxt.m[k].x - old.m[k].x, nxt.m[k].y - old.m[k].y);
+        const D22 ns = DMul22(diff, inv);
+        double sumabs = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) sumabs += hypot(ns.m[k].x, ns.m[k].y);
+        if (isfinite(sumabs)) {
+          norm_sum += sumabs;
+          norm_cnt += 4;
+        }
+      }
+      bool all_finite = true;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        sol[k] = nxt.m[k];
+        all_finite = all_finite && dfinite(nxt.m[k]);
+      }
+      if (!all_finite) p.nonfinite[item / (p.n_ant * p.n_sub)] = 1u;
+    }
+  }
+  if (p.host_mode) return;
+  __shared__ double s_sum[kThreads];
+  __shared__ uint32_t s_cnt[kThreads];
+  __shared__ bool s_last;
+  s_sum[threadIdx.x] = norm_sum;
+  s_cnt[threadIdx.x] = norm_cnt;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      s_sum[threadIdx.x] += s_sum[threadIdx.x + w];
+      s_cnt[threadIdx.x] += s_cnt[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    p.block_sum[blockIdx.x] = s_sum[0];
+    p.block_cnt[blockIdx.x] = s_cnt[0];
+    __threadfence();
+    s_last = atomicAdd(p.blocks_done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last || threadIdx.x != 0) return;
+  __threadfence();
+  *p.blocks_done = 0;
+  LoopState& ls = *p.state;
+  bool go = false;
+  if (!ls.done) {
+    double sum = 0.0;
+    uint64_t cnt = 0;
+    for (uint32_t b = 0; b < gridDim.x; ++b) {
+      sum += reinterpret_cast<volatile double*>(p.block_sum)[b];
+      cnt += reinterpret_cast<volatile uint32_t*>(p.block_cnt)[b];
+    }
+    go = !ControlStep(ls, st, sum, cnt, p.step_magnitudes);
+  }
+  if (p.use_handle) cudaGraphSetConditional(p.handle, go ? 1u : 0u);
+}
+
+// SolverBase::MakeSolutionsFinite4Pol (SolverBase.cc:372-403), one block per
+// channel block flagged non-finite: matrices with a non-finite element get
+// the mean |J_00| over the finite matrices in every element (the reference
+// averages element 0 for all four), 1 where none is finite... as the
+// reference: (1, 0, 0, 1) when no matrix is finite.
+__global__ void __launch_bounds__(kThreads)
+    make_finite4_kernel(double2* __restrict__ sols, uint32_t* nonfinite, uint32_t per_cb,
+                        cudaGraphConditionalHandle handle, int use_handle, const LoopState* state) {
+  if (use_handle && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(handle, 0);
+  if (use_handle && state->done) return;
+  const uint32_t cb = blockIdx.x;
+  if (nonfinite[cb] == 0) return;
+  double2* s = sols + size_t(cb) * per_cb;
+  __shared__ double red_sum[kThreads];
+  __shared__ uint32_t red_cnt[kThreads];
+  auto finite4 = [&](uint32_t i) {
+    return dfinite(s[i]) && dfinite(s[i + 1]) && dfinite(s[i + 2]) && dfinite(s[i + 3]);
+  };
+  double sum = 0.0;
+  uint32_t cnt = 0;
+  for (uint32_t i = threadIdx.x * 4; i < per_cb; i += blockDim.x * 4)
+    if (finite4(i)) {
+      sum += hypot(s[i].x, s[i].y);
+      ++cnt;
+    }
+  red_sum[threadIdx.x] = sum;
+  red_cnt[threadIdx.x] = cnt;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      red_sum[threadIdx.x] += red_sum[threadIdx.x + w];
+      red_cnt[threadIdx.x] += red_cnt[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  const bool none = red_cnt[0] == 0;
+  const double avg = none ? 0.0 : red_sum[0] / double(red_cnt[0]);
+  for (uint32_t i = threadIdx.x * 4; i < per_cb; i += blockDim.x * 4)
+    if (!finite4(i))
+      for (int k = 0; k < 4; ++k)
+        s[i + k] = none ? make_double2(k == 0 || k == 3 ? 1.0 : 0.0, 0.0) : make_double2(avg, 0.0);
+  __syncthreads();
+  if (threadIdx.x == 0) nonfinite[cb] = 0;
+}
+
+// ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
 thread_local std::string g_last_error = "no error";
@@ -2594,6 +3025,11 @@ struct ddsolve_ctx {
   std::vector<ChannelBlockStore> cbs;
   DevBuf staging, pack_desc, run_src_dev, run_len_dev;
   DevBuf predict_in;  // station UVW, sky, frequencies and antennas of a predict
+  // Pinned host image of predict_in (one copy per predict), reusable once
+  // the copy recorded in predict_copied has run.
+  void* predict_host = nullptr;
+  size_t predict_host_bytes = 0;
+  cudaEvent_t predict_copied = nullptr;
   DevBuf raw_in;      // DP3-layout interval buffers (ddsolve_set_interval_buffers)
   DevBuf raw_model;   // the 4-correlation predicted model of one block
 
@@ -2638,6 +3074,10 @@ struct ddsolve_ctx {
   };
   std::vector<DeviceConstraint> constraints;
   DevBuf d_cons, d_ref_ant;  // second next-solutions buffer; reference antennas
+  // full-Jones plan: first global run of each slab, per (cb, antenna,
+  // sub-solution) item the list of its partial slots
+  DevBuf d_fj_run_start, d_fj_list_off, d_fj_list_ent;
+  uint32_t fj_n_slabs = 0, fj_n_runs = 0, fj_blocks = 0;
   // independent solution intervals (ddsolve_set_intervals): interval g owns
   // channel blocks [group_first_cb[g], group_first_cb[g + 1])
   uint32_t n_groups = 1;
@@ -2672,6 +3112,25 @@ struct ddsolve_ctx {
     if (graph) cudaGraphDestroy(graph);
     if (stream) cudaStreamDestroy(stream);
     if (h_stage) cudaFreeHost(h_stage);
+    if (predict_copied) cudaEventDestroy(predict_copied);
+    if (predict_host) cudaFreeHost(predict_host);
+  }
+  // The pinned predict image, at least n bytes, free to overwrite.
+  cudaError_t ReservePredictHost(size_t n) {
+    if (predict_copied) {
+      const cudaError_t e = cudaEventSynchronize(predict_copied);
+      if (e != cudaSuccess) return e;
+    } else {
+      const cudaError_t e = cudaEventCreateWithFlags(&predict_copied, cudaEventDisableTiming);
+      if (e != cudaSuccess) return e;
+    }
+    if (predict_host && n <= predict_host_bytes) return cudaSuccess;
+    if (predict_host) cudaFreeHost(predict_host);
+    predict_host = nullptr;
+    predict_host_bytes = 0;
+    const cudaError_t e = cudaMallocHost(&predict_host, std::max<size_t>(n, 1 << 16));
+    if (e == cudaSuccess) predict_host_bytes = std::max<size_t>(n, 1 << 16);
+    return e;
   }
   cudaError_t ReserveStage(size_t n_mags) {
     if (h_stage && n_mags <= mags_cap) return cudaSuccess;
@@ -2844,8 +3303,10 @@ int CheckDims(const ddsolve_dims* dims) {
   if (!dims->n_solutions_per_direction) return DDSOLVE_E_INVALID;
   const uint32_t nc = dims->n_correlations, np = dims->n_solution_polarizations;
   if (!((nc == 2 && np == 2) || (nc == 4 && np == 2) || (nc == 1 && np == 1) ||
-        (nc == 2 && np == 1) || (nc == 4 && np == 1)))
+        (nc == 2 && np == 1) || (nc == 4 && np == 1) || (nc == 4 && np == 4)))
     return DDSOLVE_E_UNSUPPORTED;
+  // full-Jones: the gains of every direction held per thread
+  if (np == 4 && dims->n_directions > uint32_t(kFjMaxDirections)) return DDSOLVE_E_UNSUPPORTED;
   for (uint32_t d = 0; d < dims->n_directions; ++d)
     if (dims->n_solutions_per_direction[d] == 0) return DDSOLVE_E_INVALID;
   return DDSOLVE_OK;
@@ -2931,15 +3392,38 @@ int LaunchPredict(ddsolve_ctx* ctx, const PredictJob& j, float2* model, uint32_t
   const size_t o_a1 = o_f + align(b_f), o_a2 = o_a1 + align(b_a), total = o_a2 + align(b_a);
   DDS_CHECK_CUDA(ctx, ctx->predict_in.Reserve(total));
   char* base = ctx->predict_in.as<char>();
-  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base, j.uvw, b_uvw, cudaMemcpyDefault, ctx->stream));
-  if (!src.empty())
-    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_src, src.data(), src.size() * 8,
-                                        cudaMemcpyHostToDevice, ctx->stream));
-  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_off, off.data(), b_off, cudaMemcpyHostToDevice,
-                                      ctx->stream));
-  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_f, j.freq, b_f, cudaMemcpyDefault, ctx->stream));
-  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_a1, j.a1, b_a, cudaMemcpyDefault, ctx->stream));
-  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_a2, j.a2, b_a, cudaMemcpyDefault, ctx->stream));
+  // Host inputs go through one pinned image and one copy (each small copy
+  // from pageable memory costs a staged transfer of its own); inputs in
+  // device memory are copied device to device.
+  auto on_host = [](const void* ptr) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+      cudaGetLastError();
+      return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered || a.type == cudaMemoryTypeHost;
+  };
+  DDS_CHECK_CUDA(ctx, ctx->ReservePredictHost(total));
+  char* host = static_cast<char*>(ctx->predict_host);
+  struct Piece {
+    const void* src;
+    size_t off, bytes;
+  };
+  const Piece pieces[6] = {{j.uvw, 0, b_uvw},           {src.data(), o_src, src.size() * 8},
+                           {off.data(), o_off, b_off},  {j.freq, o_f, b_f},
+                           {j.a1, o_a1, b_a},           {j.a2, o_a2, b_a}};
+  bool device_piece[6];
+  for (int k = 0; k < 6; ++k) {
+    const Piece& pc = pieces[k];
+    device_piece[k] = pc.bytes > 0 && !on_host(pc.src);
+    if (pc.bytes > 0 && !device_piece[k]) std::memcpy(host + pc.off, pc.src, pc.bytes);
+  }
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base, host, total, cudaMemcpyHostToDevice, ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaEventRecord(ctx->predict_copied, ctx->stream));
+  for (int k = 0; k < 6; ++k)  // after the image, which they overwrite
+    if (device_piece[k])
+      DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + pieces[k].off, pieces[k].src, pieces[k].bytes,
+                                          cudaMemcpyDeviceToDevice, ctx->stream));
   PredictParams p;
   p.uvw = reinterpret_cast<const double*>(base);
   p.src = reinterpret_cast<const double*>(base + o_src);
@@ -3385,11 +3869,86 @@ int BuildPipePlan(ddsolve_ctx* ctx, std::vector<SlabDesc>& descs,
 
 // Builds the streaming plan: kernel choice, CTA work split, partial slots and
 // the finalisation lists.
+// Plan of the full-Jones path: every slab's runs numbered globally (one
+// fj_pass_kernel thread each) and, per (channel block, antenna,
+// sub-solution) item, the list of partial slots (run, direction, side) that
+// add up to its normal equations, in run order.
+int BuildFullJonesPlan(ddsolve_ctx* ctx) {
+  const uint32_t n_dir = ctx->n_dir, n_ant = ctx->n_ant, n_sub = ctx->n_sub;
+  std::vector<SlabDesc> descs;
+  std::vector<uint32_t> slab_sol, run_start{0};
+  std::vector<std::vector<uint32_t>> lists(size_t(ctx->n_cb) * n_ant * n_sub);
+  uint64_t n_runs = 0;
+  for (uint32_t c = 0; c < ctx->n_cb; ++c) {
+    ChannelBlockStore& cb = ctx->cbs[c];
+    for (const HostSlab& s : cb.slabs) {
+      SlabDesc sd{};
+      sd.vis = cb.vis.as<char>() + s.elem_off * (1 + n_dir) * ctx->elem_bytes;
+      sd.W = s.W;
+      sd.run_ant = cb.run_ant_dev.as<uint32_t>() + s.run_off;
+      sd.cb = c;
+      sd.T = s.T;
+      sd.L = s.L;
+      sd.R = s.R;
+      sd.sol_off = uint32_t(slab_sol.size());
+      slab_sol.insert(slab_sol.end(), s.sol.begin(), s.sol.end());
+      descs.push_back(sd);
+      for (uint32_t r = 0; r < s.R; ++r) {
+        const uint32_t ap = cb.run_ant[s.run_off + r];
+        const uint32_t a1 = ap & 0xFFFFu, a2 = ap >> 16;
+        for (uint32_t d = 0; d < n_dir; ++d) {
+          const uint64_t slot = (n_runs + r) * n_dir + d;
+          if (slot >= (uint64_t(1) << 31))
+            return ctx->Fail(DDSOLVE_E_UNSUPPORTED, "full-Jones: too many runs");
+          const size_t base = size_t(c) * n_ant;
+          lists[(base + a1) * n_sub + s.sol[d]].push_back(uint32_t(slot << 1));
+          lists[(base + a2) * n_sub + s.sol[d]].push_back(uint32_t(slot << 1) | 1u);
+        }
+      }
+      n_runs += s.R;
+      run_start.push_back(uint32_t(n_runs));
+    }
+  }
+  std::vector<uint32_t> off(lists.size() + 1, 0), ent;
+  for (size_t i = 0; i < lists.size(); ++i) {
+    off[i] = uint32_t(ent.size());
+    ent.insert(ent.end(), lists[i].begin(), lists[i].end());
+  }
+  off[lists.size()] = uint32_t(ent.size());
+  if (ent.empty()) ent.push_back(0);
+  auto up = [&](DevBuf& b, const void* src, size_t bytes) -> int {
+    DDS_CHECK_CUDA(ctx, b.Reserve(bytes));
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(b.ptr, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    return DDSOLVE_OK;
+  };
+  int rc;
+  if ((rc = up(ctx->d_slabs, descs.data(), descs.size() * sizeof(SlabDesc))) != DDSOLVE_OK ||
+      (rc = up(ctx->d_slab_sol, slab_sol.data(), slab_sol.size() * 4)) != DDSOLVE_OK ||
+      (rc = up(ctx->d_fj_run_start, run_start.data(), run_start.size() * 4)) != DDSOLVE_OK ||
+      (rc = up(ctx->d_fj_list_off, off.data(), off.size() * 4)) != DDSOLVE_OK ||
+      (rc = up(ctx->d_fj_list_ent, ent.data(), ent.size() * 4)) != DDSOLVE_OK)
+    return rc;
+  DDS_CHECK_CUDA(ctx, ctx->d_partials.Reserve(
+                          std::max<uint64_t>(n_runs, 1) * n_dir * kFjSlotFloats * 4));
+  const uint32_t n_items = ctx->n_cb * n_ant * n_sub;
+  ctx->fj_blocks = (n_items + kThreads - 1) / kThreads;
+  DDS_CHECK_CUDA(ctx, ctx->d_block_sum.Reserve(size_t(ctx->fj_blocks) * 8));
+  DDS_CHECK_CUDA(ctx, ctx->d_block_cnt.Reserve(size_t(ctx->fj_blocks) * 4));
+  // keep the host vectors alive until the copies have been issued from pageable memory
+  DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->fj_n_slabs = uint32_t(descs.size());
+  ctx->fj_n_runs = uint32_t(n_runs);
+  ctx->use_pipe = false;
+  ctx->plan_dirty = false;
+  return DDSOLVE_OK;
+}
+
 int BuildPlanImpl(ddsolve_ctx* ctx, bool allow_pipe) {
   for (uint32_t c = 0; c < ctx->n_cb; ++c)
     if (!ctx->cbs[c].set)
       return ctx->Fail(DDSOLVE_E_STATE,
                        "channel block " + std::to_string(c) + " has no data");
+  if (ctx->n_pol == 4) return BuildFullJonesPlan(ctx);
   int max_optin = 0;
   DDS_CHECK_CUDA(ctx, cudaDeviceGetAttribute(
                           &max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
@@ -3877,8 +4436,64 @@ uint32_t ConstraintLaunches(const ddsolve_ctx* ctx) {
 // constraints (solve mode) the finalisation is split around them: the pass
 // finalises in step-only mode, the constraints run, and an assignment pass
 // (assign_kernel, or finalize_kernel again) finishes the iteration.
+// One full-Jones iteration: MakeSolutionsFinite4Pol, the pass, the
+// finalisation (or, in host mode, the next solutions only).
+int LaunchFullJones(ddsolve_ctx* ctx, bool host_mode, bool use_handle, bool with_make_finite) {
+  if (with_make_finite) {
+    make_finite4_kernel<<<ctx->n_cb, kThreads, 0, ctx->stream>>>(
+        ctx->d_sol.as<double2>(), ctx->d_nonfinite.as<uint32_t>(), ctx->n_ant * ctx->n_sub * 4,
+        ctx->handle, use_handle ? 1 : 0, ctx->d_state.as<LoopState>());
+    DDS_CHECK_CUDA(ctx, cudaGetLastError());
+  }
+  FjPassParams pp;
+  pp.slabs = ctx->d_slabs.as<SlabDesc>();
+  pp.slab_sol = ctx->d_slab_sol.as<uint32_t>();
+  pp.run_start = ctx->d_fj_run_start.as<uint32_t>();
+  pp.solutions = ctx->d_sol.as<double2>();
+  pp.partials = ctx->d_partials.as<float>();
+  pp.n_slabs = ctx->fj_n_slabs;
+  pp.n_runs = ctx->fj_n_runs;
+  pp.n_ant = ctx->n_ant;
+  pp.n_sub = ctx->n_sub;
+  pp.n_dir = ctx->n_dir;
+  pp.state = ctx->d_state.as<LoopState>();
+  pp.use_handle = (use_handle && !host_mode) ? 1 : 0;
+  const uint32_t blocks = std::max<uint32_t>(1, (ctx->fj_n_runs + kFjThreads - 1) / kFjThreads);
+  switch (ctx->n_dir) {
+    case 1: fj_pass_kernel<1><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
+    case 2: fj_pass_kernel<2><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
+    case 3: fj_pass_kernel<3><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
+    default: fj_pass_kernel<4><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
+  }
+  DDS_CHECK_CUDA(ctx, cudaGetLastError());
+  FjFinParams fp;
+  fp.partials = ctx->d_partials.as<float>();
+  fp.list_off = ctx->d_fj_list_off.as<uint32_t>();
+  fp.list_ent = ctx->d_fj_list_ent.as<uint32_t>();
+  fp.solutions = ctx->d_sol.as<double2>();
+  fp.next_out = ctx->d_next.as<double2>();
+  fp.n_items = ctx->n_cb * ctx->n_ant * ctx->n_sub;
+  fp.n_dir = ctx->n_dir;
+  fp.n_ant = ctx->n_ant;
+  fp.n_sub = ctx->n_sub;
+  fp.host_mode = host_mode ? 1 : 0;
+  fp.settings = ctx->d_settings.as<DevSettings>();
+  fp.block_sum = ctx->d_block_sum.as<double>();
+  fp.block_cnt = ctx->d_block_cnt.as<uint32_t>();
+  fp.state = ctx->d_state.as<LoopState>();
+  fp.nonfinite = ctx->d_nonfinite.as<uint32_t>();
+  fp.step_magnitudes = ctx->d_mags.as<double>();
+  fp.handle = ctx->handle;
+  fp.use_handle = use_handle ? 1 : 0;
+  fp.blocks_done = &ctx->d_state.as<LoopState>()->blocks_done;
+  fj_finalize_kernel<<<ctx->fj_blocks, kThreads, 0, ctx->stream>>>(fp);
+  DDS_CHECK_CUDA(ctx, cudaGetLastError());
+  return DDSOLVE_OK;
+}
+
 int LaunchIteration(ddsolve_ctx* ctx, bool host_mode, bool use_handle,
                     bool with_make_finite) {
+  if (ctx->n_pol == 4) return LaunchFullJones(ctx, host_mode, use_handle, with_make_finite);
   const bool constrained = !host_mode && !ctx->constraints.empty();
   if (ctx->use_pipe) {
     // Cooperative launch: pipe_kernel has a grid barrier, so all CTAs must be
@@ -4541,6 +5156,9 @@ int SolveImpl(ddsolve_ctx* ctx, double* solutions, ddsolve_result* results,
   if (ctx->n_groups > 1 && !ctx->constraints.empty())
     return ctx->Fail(DDSOLVE_E_UNSUPPORTED,
                      "device constraints apply to single-interval contexts");
+  if (ctx->n_pol == 4 && (ctx->n_groups > 1 || !ctx->constraints.empty()))
+    return ctx->Fail(DDSOLVE_E_UNSUPPORTED,
+                     "the full-Jones solver runs single intervals without device constraints");
   if (ctx->plan_dirty && (rc = BuildPlan(ctx)) != DDSOLVE_OK) return rc;
   const uint32_t n_groups = ctx->n_groups;
   const size_t n_sol = size_t(ctx->n_cb) * ctx->n_ant * ctx->n_sub * ctx->n_pol;
@@ -5076,6 +5694,14 @@ int ddsolve_autotune(ddsolve_ctx* ctx, uint32_t launches, ddsolve_tuning* chosen
   int rc;
   for (uint32_t c = 0; c < ctx->n_cb; ++c)
     if (!ctx->cbs[c].set) return ctx->Fail(DDSOLVE_E_STATE, "autotune needs uploaded data");
+  if (ctx->n_pol == 4) {  // the full-Jones path has one plan: time it
+    if ((rc = BuildPlan(ctx)) != DDSOLVE_OK) return rc;
+    float ms = 0.f;
+    if ((rc = TimeIteration(ctx, launches, &ms)) != DDSOLVE_OK) return rc;
+    if (chosen) *chosen = CurrentTuning(ctx);
+    if (iteration_ms) *iteration_ms = ms;
+    return DDSOLVE_OK;
+  }
   const TuneKey key = MakeTuneKey(ctx);
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);

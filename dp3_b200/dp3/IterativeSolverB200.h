@@ -134,9 +134,12 @@ class SmoothnessConstraintB200 final : public Constraint {
 
 template <typename VisMatrix, size_t NPol>
 class IterativeSolverB200 final : public SolverBase {
-  static_assert(NPol == 1 || NPol == 2, "diagonal (2) or scalar (1) solutions");
+  static_assert(NPol == 1 || NPol == 2 || NPol == 4,
+                "scalar (1), diagonal (2) or full-Jones (4) solutions");
   static_assert(NPol == 1 || !std::is_same_v<VisMatrix, std::complex<float>>,
                 "the diagonal solver needs 2 or 4 correlations");
+  static_assert(NPol != 4 || std::is_same_v<VisMatrix, aocommon::MC2x2F>,
+                "the full-Jones solver needs 4 correlations");
 
  public:
   explicit IterativeSolverB200(int device = 0) : device_(device) {}
@@ -165,7 +168,9 @@ class IterativeSolverB200 final : public SolverBase {
                     std::vector<std::vector<DComplex>>& solutions, double time,
                     std::ostream* stat_stream) {
     Upload(data);
-    if (UploadDeviceConstraints()) return SolveOnDevice(solutions, stat_stream);
+    // (the full-Jones device path has no device constraints)
+    const bool device_loop = NPol == 4 ? GetConstraints().empty() : UploadDeviceConstraints();
+    if (device_loop) return SolveOnDevice(solutions, stat_stream);
     return SolveWithHostConstraints(solutions, time, stat_stream);
   }
 
@@ -325,7 +330,9 @@ class IterativeSolverB200 final : public SolverBase {
     std::vector<double> step_magnitudes;
     step_magnitudes.reserve(GetMaxIterations());
     do {
-      if constexpr (NPol == 2)
+      if constexpr (NPol == 4)
+        MakeSolutionsFinite4Pol(solutions);
+      else if constexpr (NPol == 2)
         MakeSolutionsFinite2Pol(solutions);
       else
         MakeSolutionsFinite1Pol(solutions);
@@ -357,6 +364,8 @@ template <typename VisMatrix>
 using IterativeDiagonalSolverB200 = IterativeSolverB200<VisMatrix, 2>;
 template <typename VisMatrix>
 using IterativeScalarSolverB200 = IterativeSolverB200<VisMatrix, 1>;
+// Drop-in for IterativeFullJonesSolver (IterativeFullJonesSolver.h:15-47).
+using IterativeFullJonesSolverB200 = IterativeSolverB200<aocommon::MC2x2F, 4>;
 
 }  // namespace dp3::ddecal
 

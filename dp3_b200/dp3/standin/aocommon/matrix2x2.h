@@ -13,6 +13,7 @@
 
 #include <cmath>
 #include <complex>
+#include <limits>
 
 namespace aocommon {
 
@@ -34,6 +35,23 @@ class MC2x2Base {
 
   static MC2x2Base Zero() { return MC2x2Base(0, 0, 0, 0); }
   static MC2x2Base Unity() { return MC2x2Base(1, 0, 0, 1); }
+  static MC2x2Base NaN() {
+    const T n = std::numeric_limits<T>::quiet_NaN();
+    return MC2x2Base(value_type(n, n), value_type(n, n), value_type(n, n), value_type(n, n));
+  }
+
+  // this * rhs^H
+  MC2x2Base MultiplyHerm(const MC2x2Base& r) const {
+    return MC2x2Base(v_[0] * std::conj(r.v_[0]) + v_[1] * std::conj(r.v_[1]),
+                     v_[0] * std::conj(r.v_[2]) + v_[1] * std::conj(r.v_[3]),
+                     v_[2] * std::conj(r.v_[0]) + v_[3] * std::conj(r.v_[1]),
+                     v_[2] * std::conj(r.v_[2]) + v_[3] * std::conj(r.v_[3]));
+  }
+  // The four elements, converted, into dest[0..3].
+  template <typename U>
+  void AssignTo(std::complex<U>* dest) const {
+    for (int i = 0; i != 4; ++i) dest[i] = std::complex<U>(v_[i]);
+  }
 
   const value_type& Get(size_t i) const { return v_[i]; }
   void Set(size_t i, value_type value) { v_[i] = value; }

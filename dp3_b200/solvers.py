@@ -452,3 +452,21 @@ class IterativeScalarSolver(SolverBase):
 
     def SupportsDdSolutionIntervals(self):
         return True
+
+
+class IterativeFullJonesSolver(SolverBase):
+    """IterativeFullJonesSolver (ddecal/gain_solvers/IterativeFullJonesSolver.h:
+    15-47): 2x2 gains on 4-correlation data (MC2x2F), solutions [.., 4] in
+    the order XX XY YX YY. The loop runs on the device; host constraints are
+    not supported for this solver here."""
+
+    def NSolutionPolarizations(self):
+        return 4
+
+    def SupportsDdSolutionIntervals(self):
+        return True
+
+    def Solve(self, data, solutions, time=0.0, stat_stream=None):
+        if self.constraints:
+            raise NotImplementedError("constraints with the full-Jones solver")
+        return super().Solve(data, solutions, time, stat_stream)

@@ -65,7 +65,13 @@ typedef struct {
   uint32_t n_channel_blocks;
   uint32_t n_correlations;           /* 1, 2 or 4, see above */
   uint32_t n_solution_polarizations; /* 2 = IterativeDiagonalSolver,
-                                        1 = IterativeScalarSolver */
+                                        1 = IterativeScalarSolver,
+                                        4 = IterativeFullJonesSolver
+                                        (IterativeFullJonesSolver.cc:17-228;
+                                        4 correlations, at most 4
+                                        directions, single intervals, no
+                                        device constraints; solutions
+                                        [.., 4] = J_00 J_01 J_10 J_11) */
   const uint32_t* n_solutions_per_direction; /* [n_directions], >= 1 */
 } ddsolve_dims;
 

@@ -27,7 +27,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libddecal_ref.so")
 REFERENCE = os.environ.get("DP3_REFERENCE", "/root/reference")
 
-DIAGONAL_DUO, DIAGONAL_FULL, SCALAR_UNI, SCALAR_DUO, SCALAR_FULL = range(5)
+DIAGONAL_DUO, DIAGONAL_FULL, SCALAR_UNI, SCALAR_DUO, SCALAR_FULL, FULL_JONES = range(6)
 
 
 def available():
@@ -118,6 +118,9 @@ def settings(max_iterations=50, min_iterations=0, accuracy=1e-5, constraint_accu
 
 
 def kind_of(ncorr, npol):
+    if npol == 4:
+        assert ncorr == 4, "the full-Jones solver needs 4 correlations"
+        return FULL_JONES
     if npol == 2:
         return {2: DIAGONAL_DUO, 4: DIAGONAL_FULL}[ncorr]
     return {1: SCALAR_UNI, 2: SCALAR_DUO, 4: SCALAR_FULL}[ncorr]

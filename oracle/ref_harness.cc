@@ -21,6 +21,7 @@
 #include <string>
 
 #include "ddecal/gain_solvers/IterativeDiagonalSolver.h"
+#include "ddecal/gain_solvers/IterativeFullJonesSolver.h"
 #include "ddecal/gain_solvers/IterativeScalarSolver.h"
 #include "ddecal/linear_solvers/LLSSolver.h"
 #include "ref_problem.h"
@@ -109,6 +110,8 @@ PreparedBase* Prepare(const ref_problem& p, int kind) {
       return new Prepared<IterativeScalarSolver<aocommon::MC2x2FDiag>, aocommon::MC2x2FDiag>(p);
     case REF_SCALAR_FULL:
       return new Prepared<IterativeScalarSolver<aocommon::MC2x2F>, aocommon::MC2x2F>(p);
+    case REF_FULL_JONES:
+      return new Prepared<IterativeFullJonesSolver, aocommon::MC2x2F>(p);
     default:
       throw std::runtime_error("unknown solver kind");
   }
@@ -189,6 +192,9 @@ extern "C" REF_API int ref_solve(const ref_problem* p, const ref_settings* s, in
       case REF_SCALAR_FULL:
         return Run<IterativeScalarSolver<aocommon::MC2x2F>, aocommon::MC2x2F>(
             *p, *s, n_threads, c, solutions, out);
+      case REF_FULL_JONES:
+        return Run<IterativeFullJonesSolver, aocommon::MC2x2F>(*p, *s, n_threads, c, solutions,
+                                                                out);
       default:
         g_error = "unknown solver kind";
         return 1;

@@ -34,6 +34,7 @@ enum {
   REF_SCALAR_UNI = 2,     // IterativeScalarSolver<std::complex<float>>
   REF_SCALAR_DUO = 3,     // IterativeScalarSolver<MC2x2FDiag>
   REF_SCALAR_FULL = 4,    // IterativeScalarSolver<MC2x2F>
+  REF_FULL_JONES = 5,     // IterativeFullJonesSolver (MC2x2F data, 2x2 gains)
 };
 
 typedef struct {

@@ -24,6 +24,7 @@ void Trace(const char* what);
 #define DP3B200_ADAPTER_TRACE(what) Trace(what)
 #include "dp3/IterativeSolverB200.h"
 #include "ddecal/gain_solvers/IterativeDiagonalSolver.h"
+#include "ddecal/gain_solvers/IterativeFullJonesSolver.h"
 #include "ddecal/gain_solvers/IterativeScalarSolver.h"
 #include "ddecal/linear_solvers/LLSSolver.h"
 #include "ref_problem.h"
@@ -96,7 +97,8 @@ int Run(Solver& solver, const ref_problem& p, const ref_settings& s, const ref_c
   auto sol = dp3b200_ref::ToVectors(solutions, p.n_channel_blocks, per_cb);
   dp3::ddecal::SolverBase::SolveResult r;
   if constexpr (std::is_same_v<Solver, dp3::ddecal::IterativeSolverB200<V, 2>> ||
-                std::is_same_v<Solver, dp3::ddecal::IterativeSolverB200<V, 1>>) {
+                std::is_same_v<Solver, dp3::ddecal::IterativeSolverB200<V, 1>> ||
+                std::is_same_v<Solver, dp3::ddecal::IterativeSolverB200<V, 4>>) {
     std::ostringstream stats;  // the statistics-stream overload
     Trace("adapter solve");
     r = solver.Solve(data, sol, 0.0, &stats);
@@ -131,7 +133,10 @@ int Dispatch(int use_b200, int device, const ref_problem& p, const ref_settings&
     IterativeSolverB200<V, NPol> solver(device);
     return Run<IterativeSolverB200<V, NPol>, V>(solver, p, s, c, solutions, out, mags, cap);
   }
-  if constexpr (NPol == 2) {
+  if constexpr (NPol == 4) {
+    IterativeFullJonesSolver solver;
+    return Run<IterativeFullJonesSolver, V>(solver, p, s, c, solutions, out, mags, cap);
+  } else if constexpr (NPol == 2) {
     IterativeDiagonalSolver<V> solver;
     return Run<IterativeDiagonalSolver<V>, V>(solver, p, s, c, solutions, out, mags, cap);
   } else {
@@ -176,6 +181,9 @@ extern "C" HARNESS_API int adapter_solve(const ref_problem* p, const ref_setting
                                                  step_magnitudes, n_step_cap);
       case REF_SCALAR_FULL:
         return Dispatch<aocommon::MC2x2F, 1>(use_b200, device, *p, *s, c, solutions, out,
+                                             step_magnitudes, n_step_cap);
+      case REF_FULL_JONES:
+        return Dispatch<aocommon::MC2x2F, 4>(use_b200, device, *p, *s, c, solutions, out,
                                              step_magnitudes, n_step_cap);
       default:
         g_error = "unknown solver kind";
