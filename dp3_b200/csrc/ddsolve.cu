@@ -2619,6 +2619,9 @@ __device__ __forceinline__ C22 LoadJones(const double2* s) {  // FP32, as MC2x2F
 }
 
 constexpr int kFjThreads = 128;
+// Directions whose gains and sums one thread holds in registers: up to this
+// many, fj_pass_kernel does everything in one read of the visibilities; more
+// directions go through fj_chunk_kernel, one launch per group of this many.
 constexpr int kFjMaxDirections = 4;
 constexpr uint32_t kFjSlotFloats = 32;  // per run and direction: P and den of both sides
 
@@ -2629,16 +2632,14 @@ struct FjPassParams {
   const double2* solutions;   // [cb][ant][sub][4]
   float* partials;            // [global run][direction][kFjSlotFloats]
   uint32_t n_slabs, n_runs, n_ant, n_sub, n_dir;
+  uint32_t d0;                // fj_chunk_kernel: first direction of the launch
   const LoopState* state;
   int32_t use_handle;
 };
 
-template <int ND>
-__global__ void __launch_bounds__(kFjThreads) fj_pass_kernel(const FjPassParams p) {
-  if (SolveStopped(p.state, p.use_handle)) return;
-  const uint32_t gr = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gr >= p.n_runs) return;
-  uint32_t lo = 0, hi = p.n_slabs;  // the slab holding global run gr
+// The slab holding global run gr (run_start is ascending).
+__device__ __forceinline__ uint32_t FjSlabOf(const FjPassParams& p, uint32_t gr) {
+  uint32_t lo = 0, hi = p.n_slabs;
   while (hi - lo > 1) {
     const uint32_t mid = (lo + hi) / 2;
     if (p.run_start[mid] <= gr)
@@ -2646,6 +2647,86 @@ __global__ void __launch_bounds__(kFjThreads) fj_pass_kernel(const FjPassParams 
     else
       hi = mid;
   }
+  return lo;
+}
+
+template <int N>
+__device__ __forceinline__ void FjStoreSlots(float* out, const C22* P1, const C22* D1,
+                                             const C22* P2, const C22* D2) {
+#pragma unroll
+  for (int d = 0; d < N; ++d) {
+    const C22* parts[4] = {&P1[d], &D1[d], &P2[d], &D2[d]};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      float4* o = reinterpret_cast<float4*>(out + d * kFjSlotFloats + q * 8);
+      o[0] = make_float4(parts[q]->m[0].x, parts[q]->m[0].y, parts[q]->m[1].x, parts[q]->m[1].y);
+      o[1] = make_float4(parts[q]->m[2].x, parts[q]->m[2].y, parts[q]->m[3].x, parts[q]->m[3].y);
+    }
+  }
+}
+
+// More than kFjMaxDirections directions: the launch for directions
+// [d0, d0 + NC) recomputes each visibility's residual over all n_dir
+// directions, in direction order with the same FP32 operations as
+// fj_pass_kernel (the gains of the other directions are read per visibility
+// from the solutions, which stay in L1), then accumulates its own NC
+// directions. Each launch reads the data and all models once, so a pass of
+// n_dir directions reads the visibilities ceil(n_dir / kFjMaxDirections) times.
+template <int NC>
+__global__ void __launch_bounds__(kFjThreads) fj_chunk_kernel(const FjPassParams p) {
+  if (SolveStopped(p.state, p.use_handle)) return;
+  const uint32_t gr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gr >= p.n_runs) return;
+  const uint32_t si = FjSlabOf(p, gr);
+  const SlabDesc sl = p.slabs[si];
+  const uint32_t r = gr - p.run_start[si];
+  const uint32_t ap = sl.run_ant[r];
+  const uint32_t a1 = ap & 0xFFFFu, a2 = ap >> 16;
+  const uint32_t nd = p.n_dir;
+  const double2* sol1 = p.solutions + (size_t(sl.cb) * p.n_ant + a1) * p.n_sub * 4;
+  const double2* sol2 = p.solutions + (size_t(sl.cb) * p.n_ant + a2) * p.n_sub * 4;
+  C22 J1[NC], J2[NC], P1[NC], D1[NC], P2[NC], D2[NC];
+#pragma unroll
+  for (int d = 0; d < NC; ++d) {
+    const uint32_t s = p.slab_sol[sl.sol_off + p.d0 + d];
+    J1[d] = LoadJones(sol1 + size_t(s) * 4);
+    J2[d] = LoadJones(sol2 + size_t(s) * 4);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      P1[d].m[k] = D1[d].m[k] = P2[d].m[k] = D2[d].m[k] = make_float2(0.f, 0.f);
+  }
+  const float2* vis = static_cast<const float2*>(sl.vis);
+  const uint64_t rows = uint64_t(sl.T) * sl.L;
+  for (uint64_t row = 0; row < rows; ++row) {
+    C22 R = LoadC22(vis + SlabElem(sl.R, sl.W, nd + 1, row, 0, r) * 4);
+    for (uint32_t e = 0; e < nd; ++e) {
+      const uint32_t s = p.slab_sol[sl.sol_off + e];
+      const C22 M = LoadC22(vis + SlabElem(sl.R, sl.W, nd + 1, row, 1 + e, r) * 4);
+      const C22 t = MulHerm22(Mul22(LoadJones(sol1 + size_t(s) * 4), M),
+                              LoadJones(sol2 + size_t(s) * 4));
+#pragma unroll
+      for (int k = 0; k < 4; ++k) R.m[k] = make_float2(R.m[k].x - t.m[k].x, R.m[k].y - t.m[k].y);
+    }
+#pragma unroll
+    for (int d = 0; d < NC; ++d) {
+      const C22 M = LoadC22(vis + SlabElem(sl.R, sl.W, nd + 1, row, 1 + p.d0 + d, r) * 4);
+      const C22 Y = Mul22(J1[d], M);
+      const C22 X = MulHerm22(J2[d], M);
+      AddMul22(P1[d], R, X);
+      AddHermMul22(D1[d], X, X);
+      AddHermMul22(P2[d], R, Y);
+      AddHermMul22(D2[d], Y, Y);
+    }
+  }
+  FjStoreSlots<NC>(p.partials + (size_t(gr) * nd + p.d0) * kFjSlotFloats, P1, D1, P2, D2);
+}
+
+template <int ND>
+__global__ void __launch_bounds__(kFjThreads) fj_pass_kernel(const FjPassParams p) {
+  if (SolveStopped(p.state, p.use_handle)) return;
+  const uint32_t gr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gr >= p.n_runs) return;
+  const uint32_t lo = FjSlabOf(p, gr);
   const SlabDesc sl = p.slabs[lo];
   const uint32_t r = gr - p.run_start[lo];
   const uint32_t ap = sl.run_ant[r];
@@ -2685,17 +2766,7 @@ __global__ void __launch_bounds__(kFjThreads) fj_pass_kernel(const FjPassParams 
       AddHermMul22(D2[d], Y[d], Y[d]);
     }
   }
-  float* out = p.partials + size_t(gr) * ND * kFjSlotFloats;
-#pragma unroll
-  for (int d = 0; d < ND; ++d) {
-    const C22* parts[4] = {&P1[d], &D1[d], &P2[d], &D2[d]};
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      float4* o = reinterpret_cast<float4*>(out + d * kFjSlotFloats + q * 8);
-      o[0] = make_float4(parts[q]->m[0].x, parts[q]->m[0].y, parts[q]->m[1].x, parts[q]->m[1].y);
-      o[1] = make_float4(parts[q]->m[2].x, parts[q]->m[2].y, parts[q]->m[3].x, parts[q]->m[3].y);
-    }
-  }
+  FjStoreSlots<ND>(p.partials + size_t(gr) * ND * kFjSlotFloats, P1, D1, P2, D2);
 }
 
 struct D22 {
@@ -3305,8 +3376,6 @@ int CheckDims(const ddsolve_dims* dims) {
   if (!((nc == 2 && np == 2) || (nc == 4 && np == 2) || (nc == 1 && np == 1) ||
         (nc == 2 && np == 1) || (nc == 4 && np == 1) || (nc == 4 && np == 4)))
     return DDSOLVE_E_UNSUPPORTED;
-  // full-Jones: the gains of every direction held per thread
-  if (np == 4 && dims->n_directions > uint32_t(kFjMaxDirections)) return DDSOLVE_E_UNSUPPORTED;
   for (uint32_t d = 0; d < dims->n_directions; ++d)
     if (dims->n_solutions_per_direction[d] == 0) return DDSOLVE_E_INVALID;
   return DDSOLVE_OK;
@@ -4438,6 +4507,14 @@ uint32_t ConstraintLaunches(const ddsolve_ctx* ctx) {
 // (assign_kernel, or finalize_kernel again) finishes the iteration.
 // One full-Jones iteration: MakeSolutionsFinite4Pol, the pass, the
 // finalisation (or, in host mode, the next solutions only).
+// Launches of the full-Jones streaming pass: one, or one per group of
+// kFjMaxDirections directions.
+uint32_t FjPassLaunches(const ddsolve_ctx* ctx) {
+  return ctx->n_dir <= uint32_t(kFjMaxDirections)
+             ? 1u
+             : (ctx->n_dir + kFjMaxDirections - 1) / kFjMaxDirections;
+}
+
 int LaunchFullJones(ddsolve_ctx* ctx, bool host_mode, bool use_handle, bool with_make_finite) {
   if (with_make_finite) {
     make_finite4_kernel<<<ctx->n_cb, kThreads, 0, ctx->stream>>>(
@@ -4458,12 +4535,23 @@ int LaunchFullJones(ddsolve_ctx* ctx, bool host_mode, bool use_handle, bool with
   pp.n_dir = ctx->n_dir;
   pp.state = ctx->d_state.as<LoopState>();
   pp.use_handle = (use_handle && !host_mode) ? 1 : 0;
+  pp.d0 = 0;
   const uint32_t blocks = std::max<uint32_t>(1, (ctx->fj_n_runs + kFjThreads - 1) / kFjThreads);
   switch (ctx->n_dir) {
     case 1: fj_pass_kernel<1><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
     case 2: fj_pass_kernel<2><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
     case 3: fj_pass_kernel<3><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
-    default: fj_pass_kernel<4><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
+    case 4: fj_pass_kernel<4><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
+    default:
+      for (uint32_t d0 = 0; d0 < ctx->n_dir; d0 += kFjMaxDirections) {
+        pp.d0 = d0;
+        switch (std::min<uint32_t>(kFjMaxDirections, ctx->n_dir - d0)) {
+          case 1: fj_chunk_kernel<1><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
+          case 2: fj_chunk_kernel<2><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
+          case 3: fj_chunk_kernel<3><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
+          default: fj_chunk_kernel<4><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
+        }
+      }
   }
   DDS_CHECK_CUDA(ctx, cudaGetLastError());
   FjFinParams fp;
@@ -5248,13 +5336,15 @@ int SolveImpl(ddsolve_ctx* ctx, double* solutions, ddsolve_result* results,
     }
   }
   // pipe path: make_finite + build_tables (+ power_kernel) + one pipe_kernel
-  // per iteration; else three kernels per iteration; with device constraints
-  // also their kernels and the assignment pass, every iteration
+  // per iteration; else three kernels per iteration (full-Jones: make_finite,
+  // the pass launches and the finalisation); with device constraints also
+  // their kernels and the assignment pass, every iteration
   const uint64_t per_it_cons =
       ctx->constraints.empty() ? 0u : uint64_t(ConstraintLaunches(ctx)) + 1u;
+  const uint64_t per_it = ctx->n_pol == 4 ? 2u + FjPassLaunches(ctx) : 3u;
   ctx->last_launches = ctx->use_pipe
                            ? uint64_t(max_it) * (1 + per_it_cons) + 2 + (solve_powers ? 1 : 0)
-                           : uint64_t(max_it) * (3 + per_it_cons);
+                           : uint64_t(max_it) * (per_it + per_it_cons);
   // the model powers are fresh for one solve only (see LaunchPowers)
   ctx->powers_dirty = true;
   if ((rc = CheckDeviceError(ctx, staged)) != DDSOLVE_OK) return rc;
@@ -5462,8 +5552,11 @@ int ddsolve_perform_iteration(ddsolve_ctx* ctx, const double* solutions,
                                       ctx->stream));
   DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   // pipe path: build_tables (+ power_kernel) + pipe_kernel; else
-  // stream_kernel + finalize_kernel
-  ctx->last_launches = ctx->use_pipe ? 2 + (powers_launched ? 1 : 0) : 2;
+  // stream_kernel + finalize_kernel (full-Jones: the pass launches +
+  // fj_finalize_kernel)
+  ctx->last_launches = ctx->n_pol == 4 ? 1 + FjPassLaunches(ctx)
+                       : ctx->use_pipe  ? 2 + (powers_launched ? 1 : 0)
+                                        : 2;
   return CheckDeviceError(ctx);
 }
 
@@ -5552,8 +5645,14 @@ int ddsolve_time_stream_kernel(ddsolve_ctx* ctx, uint32_t n_launches, float* mea
   DDS_CHECK_CUDA(ctx, cudaEventCreate(&a));
   DDS_CHECK_CUDA(ctx, cudaEventCreate(&b));
   // warm-up launch, then n_launches timed launches of the streaming pass
-  // (pipe_kernel in next-solutions mode, or stream_kernel alone).
-  if (ctx->use_pipe) {
+  // (pipe_kernel in next-solutions mode, stream_kernel alone, or the
+  // full-Jones pass and its finalisation).
+  if (ctx->n_pol == 4) {
+    if ((rc = LaunchIteration(ctx, true, false, false)) != DDSOLVE_OK) return rc;
+    DDS_CHECK_CUDA(ctx, cudaEventRecord(a, ctx->stream));
+    for (uint32_t i = 0; i < n_launches; ++i)
+      if ((rc = LaunchIteration(ctx, true, false, false)) != DDSOLVE_OK) return rc;
+  } else if (ctx->use_pipe) {
     DDS_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_cb_flag.ptr, 0, size_t(ctx->n_cb) * 4,
                                         ctx->stream));
     if ((rc = LaunchBuildTables(ctx)) != DDSOLVE_OK) return rc;

@@ -68,9 +68,9 @@ typedef struct {
                                         1 = IterativeScalarSolver,
                                         4 = IterativeFullJonesSolver
                                         (IterativeFullJonesSolver.cc:17-228;
-                                        4 correlations, at most 4
-                                        directions, single intervals, no
-                                        device constraints; solutions
+                                        4 correlations, single
+                                        intervals, no device
+                                        constraints; solutions
                                         [.., 4] = J_00 J_01 J_10 J_11) */
   const uint32_t* n_solutions_per_direction; /* [n_directions], >= 1 */
 } ddsolve_dims;
@@ -386,7 +386,9 @@ DDSOLVE_API int ddsolve_autotune(ddsolve_ctx* ctx, uint32_t launches, ddsolve_tu
 
 /* Device time of the streaming kernel: launches it n_launches times on the
  * context stream with the current solutions and returns the mean duration in
- * milliseconds, measured with CUDA events. Solutions are not modified. */
+ * milliseconds, measured with CUDA events. Solutions are not modified. With
+ * four solution polarizations this times the full-Jones pass together with
+ * its finalisation (two launches per pass). */
 DDSOLVE_API int ddsolve_time_stream_kernel(ddsolve_ctx* ctx, uint32_t n_launches,
                                float* mean_ms);
 

@@ -155,11 +155,18 @@ def test_reference_full_jones_recovers_true_gains(built):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["plain", "dd", "phase_only", "three_dirs"])
+@pytest.mark.parametrize("case", ["plain", "dd", "phase_only", "three_dirs", "six_dirs_dd",
+                                  "nine_dirs"])
 def test_full_jones_matches_reference(built, case):
+    """Full solves against the reference; six and nine directions take the
+    chunked pass (directions in launches of four)."""
     kw = dict(nspd=[2, 1]) if case == "dd" else {}
     if case == "three_dirs":
         kw = dict(n_directions=3)
+    if case == "six_dirs_dd":
+        kw = dict(n_directions=6, nspd=[1, 2, 1, 3, 1, 2])
+    if case == "nine_dirs":
+        kw = dict(n_directions=9, n_stations=10)
     obs, prob, truth = full_jones_problem(noise=0.01, **kw)
     st = rf.settings(max_iterations=80, accuracy=1e-5, phase_only=case == "phase_only")
     start = perturbed(truth, 0.05)
@@ -176,10 +183,11 @@ def test_full_jones_matches_reference(built, case):
 
 
 @pytest.mark.gpu
-def test_full_jones_one_pass_matches_reference_first_iteration(built):
+@pytest.mark.parametrize("n_directions", [2, 7])
+def test_full_jones_one_pass_matches_reference_first_iteration(built, n_directions):
     """ddsolve_perform_iteration (the undamped next solutions) stepped by
     hand equals the reference's first iteration (max_iterations = 1)."""
-    obs, prob, truth = full_jones_problem(noise=0.01)
+    obs, prob, truth = full_jones_problem(noise=0.01, n_directions=n_directions)
     st = rf.settings(max_iterations=1, accuracy=1e-12, step_size=1.0)
     start = perturbed(truth, 0.1)
     ref = start.copy()
