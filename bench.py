@@ -495,6 +495,106 @@ def run_predict_only(args):
     return 0
 
 
+def run_correct_subtract(args):
+    """DDECal's CorrectAndSubtractModels (the step after the solve) on the GPU
+    through ddsolve_correct_and_subtract, on configuration `args.config`: the
+    interval in DP3's buffer layout with four correlations ([t][bl][ch][4]
+    data, [dir][t][bl][ch][4] models; XX / YY from the synthetic
+    observation, XY = YX = 0), the true gains of each channel block as the
+    solutions, every direction's model corrected and the sum subtracted from
+    the data in place. Device-resident: buffers and solutions in device
+    memory, each call timed with CUDA events on the context's stream (the
+    call also copies the two antenna arrays to the device). End to end:
+    pinned host buffers, the copies to and from the device inside the timed
+    call. Algorithmic bytes per visibility: 32 x (2 + n_dir) (data read and
+    written, every model read once). The CPU figure is the numpy oracle on
+    one time step of the interval, scaled to the interval."""
+    import ctypes
+    import torch
+    from dp3_b200 import build as native_build
+    from dp3_b200 import ddsolve, synth
+    from oracle import subtract_oracle
+    native_build.build_all()
+    torch.cuda.set_device(0)
+    cfg = synth.benchmark_configs()[args.config]
+    obs = synth.observe(cfg)
+    n_t, n_bl, n_dir = cfg.n_times, cfg.n_baselines, cfg.n_directions
+    n_ch, n_cb = sum(cfg.cb_channels), cfg.n_channel_blocks
+    data = np.zeros((n_t, n_bl, n_ch, 4), np.complex64)
+    model = np.zeros((n_dir, n_t, n_bl, n_ch, 4), np.complex64)
+    c0 = 0
+    for cb, nc in enumerate(cfg.cb_channels):
+        d = obs.data[cb].reshape(n_t, n_bl, nc, 2, 2)
+        m = obs.model[cb].reshape(n_dir, n_t, n_bl, nc, 2, 2)
+        data[:, :, c0:c0 + nc, 0] = d[..., 0, 0] + 1j * d[..., 0, 1]
+        data[:, :, c0:c0 + nc, 3] = d[..., 1, 0] + 1j * d[..., 1, 1]
+        model[..., c0:c0 + nc, 0] = m[..., 0, 0] + 1j * m[..., 0, 1]
+        model[..., c0:c0 + nc, 3] = m[..., 1, 0] + 1j * m[..., 1, 1]
+        c0 += nc
+    starts = np.cumsum([0] + list(cfg.cb_channels))[:-1]
+    sol = np.ascontiguousarray(obs.true_gains[starts], np.complex128)  # [cb][st][dir][2]
+    a1 = np.ascontiguousarray(obs.antenna1, np.uint32)
+    a2 = np.ascontiguousarray(obs.antenna2, np.uint32)
+    ctx = ddsolve.Context(cfg.n_stations, [1] * n_dir, n_cb, 2, 2)
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device="cuda:0")
+    n_vis = n_t * n_bl * n_ch
+    algo = n_vis * 32 * (2 + n_dir)
+
+    def call(d_in, m_in, s, d_out):
+        ib = ddsolve.IntervalBuffers()
+        ib.n_times, ib.n_baselines, ib.n_channels = n_t, n_bl, n_ch
+        ib.antenna1, ib.antenna2 = a1.ctypes.data, a2.ctypes.data
+        ib.data, ib.model = d_in, m_in
+        rc = ddsolve.lib().ddsolve_correct_and_subtract(ctx._h, ctypes.byref(ib), s, d_out, None)
+        if rc != 0:
+            raise RuntimeError(ddsolve.lib().ddsolve_last_error(ctx._h).decode())
+
+    def timed(d_in, m_in, s, d_out, steps):
+        ms = []
+        for _ in range(steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            call(d_in, m_in, s, d_out)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms))
+
+    dev = torch.device("cuda", 0)
+    t_data = torch.from_numpy(data.view(np.float32)).to(dev)
+    t_model = torch.from_numpy(model.view(np.float32)).to(dev)
+    t_sol = torch.from_numpy(sol.view(np.float64)).to(dev)
+    torch.cuda.synchronize()
+    args_dev = (t_data.data_ptr(), t_model.data_ptr(), t_sol.data_ptr(), t_data.data_ptr())
+    timed(*args_dev, args.warmup)
+    dev_ms = timed(*args_dev, args.steps)
+    h_data = torch.from_numpy(data.view(np.float32)).pin_memory()
+    h_model = torch.from_numpy(model.view(np.float32)).pin_memory()
+    h_out = torch.empty_like(h_data).pin_memory()
+    args_host = (h_data.data_ptr(), h_model.data_ptr(), sol.ctypes.data, h_out.data_ptr())
+    timed(*args_host, args.warmup)
+    e2e_ms = timed(*args_host, max(3, args.steps // 4))
+    ctx.close()
+    peak, peak_kind = _peaks()
+    achieved = algo / (dev_ms / 1e3) / 1e9
+    # CPU: the numpy oracle on the first time step, scaled to the interval
+    t0 = time.perf_counter()
+    subtract_oracle.correct_and_subtract(data[:1], model[:, :1], sol, a1, a2, True, False)
+    cpu_s = (time.perf_counter() - t0) * n_t
+    print(json.dumps({
+        "config": cfg.name, "step": "DDECal::CorrectAndSubtractModels",
+        "n_vis": n_vis, "ms_per_interval": dev_ms, "algorithmic_bytes": algo,
+        "achieved_gbs": achieved, "peak_gbs": peak, "peak_kind": peak_kind,
+        "frac": achieved / peak,
+        "e2e_ms_per_interval": e2e_ms,
+        "e2e_bytes": {"h2d": data.nbytes + model.nbytes + sol.nbytes, "d2h": data.nbytes},
+        "cpu_oracle_s_per_interval": cpu_s,
+        "cpu_oracle_sample": "numpy restatement, 1 thread, first time step scaled to the interval",
+    }), flush=True)
+    return 0
+
+
 def run_fp64_check(args):
     """Solution error of the GPU solver against the FP64 oracle on
     configuration `args.config` (a numerical statement, not a timing): one
@@ -966,6 +1066,8 @@ def main():
                     help="time only the warm-start network's forward pass (for profiling)")
     ap.add_argument("--predict-only", action="store_true",
                     help="time only the GPU point-source predict of --config (for profiling)")
+    ap.add_argument("--correct-subtract", action="store_true",
+                    help="time only the GPU CorrectAndSubtractModels step of --config")
     ap.add_argument("--mlp-only", action="store_true",
                     help="time only the warm-start network's training (for profiling)")
     ap.add_argument("--mlp-rows", type=int, default=60000)
@@ -983,6 +1085,8 @@ def main():
         return run_mlp_infer(args)
     if args.predict_only:
         return run_predict_only(args)
+    if args.correct_subtract:
+        return run_correct_subtract(args)
     if args.fp64_check:
         return run_fp64_check(args)
     if args.batch > 1:

@@ -402,6 +402,10 @@ __global__ void __launch_bounds__(kPredictThreads) predict_kernel(const PredictP
   const uint64_t n_vis = uint64_t(p.n_times) * p.n_bl * p.L;
   const uint64_t v0 = (uint64_t(t) * p.n_bl + bl) * p.L;
   float2* out = p.model + (uint64_t(d) * n_vis + v0) * NCORR;
+  if (ap == aq) {  // autocorrelations stay zero (Simulator.cc:162-163)
+    for (uint32_t i = 0; i < p.L * NCORR; ++i) out[i] = make_float2(0.f, 0.f);
+    return;
+  }
   for (uint32_t c0 = 0; c0 < p.L; c0 += CH) {
     const uint32_t nc = min(uint32_t(CH), p.L - c0);
     double2 acc[CH][NCORR];
@@ -536,6 +540,110 @@ __global__ void weigh_kernel(const WeighParams p) {
                     : make_float2(__fmul_rn(mk.x, pw[k]), __fmul_rn(mk.y, pw[k]));
       }
       put(p.out + (n_vis * (1 + d) + v) * NCORR, z);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// correct_subtract_kernel: DDECal::CorrectAndSubtractModels
+// (steps/DDECal.cc:1081-1125) with ApplySolutionAndSubtract (:1031-1079) for
+// one interval in DP3's buffer layout. Per visibility (autocorrelations
+// included) and direction the corrected model C = G_1 M G_2^H in FP64, as the
+// reference's aocommon::MC2x2 (complex<double>) arithmetic: full-Jones
+// J_1.Multiply(M).MultiplyHerm(J_2) (:1004-1011), diagonal
+// (diag(g_1) M) diag(g_2)^H (:1013-1019), scalar M (g_1 conj(g_2))
+// (:1021-1027), every product and sum rounded on its own (no fused
+// multiply-add, as the host's separate multiplies and adds). C is summed over
+// directions from zero in direction order; kept models are stored as
+// complex<float> (AssignTo), and the data become
+// float(double(data) - sum) (complex<float> -= complex<double>). Channel ch
+// belongs to the even-split channel block of the solve (DDECal.cc:308-313).
+// One thread per (time, baseline, channel): 32 bytes of data and 32 bytes of
+// model per direction read, the same written back: an HBM-bound stream.
+// ---------------------------------------------------------------------------
+struct CorrectParams {
+  const float4* data;        // [n_vis][2]: XX XY | YX YY
+  const float4* model;       // [n_dir][n_vis][2]
+  float4* data_out;          // or null (no subtraction)
+  float4* model_out;         // or null (models not kept)
+  const double2* solutions;  // [n_cb][n_ant][n_dir][NPOL]
+  const uint32_t* a1;        // [n_bl]
+  const uint32_t* a2;
+  uint64_t n_vis;
+  uint32_t n_bl, n_ch, n_cb, n_ant, n_dir;
+};
+
+__device__ __forceinline__ double2 zmul_rn(double2 a, double2 b) {
+  return make_double2(__dsub_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)),
+                      __dadd_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x)));
+}
+__device__ __forceinline__ double2 zadd_rn(double2 a, double2 b) {
+  return make_double2(__dadd_rn(a.x, b.x), __dadd_rn(a.y, b.y));
+}
+__device__ __forceinline__ double2 zconj(double2 a) { return make_double2(a.x, -a.y); }
+
+template <int NPOL>
+__global__ void __launch_bounds__(256) correct_subtract_kernel(const CorrectParams p) {
+  for (uint64_t v = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; v < p.n_vis;
+       v += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t ch = uint32_t(v % p.n_ch);
+    const uint32_t bl = uint32_t((v / p.n_ch) % p.n_bl);
+    // the block cb with cb n_ch / n_cb <= ch < (cb + 1) n_ch / n_cb
+    const uint32_t cb = uint32_t((uint64_t(ch + 1) * p.n_cb - 1) / p.n_ch);
+    const double2* s1 = p.solutions + (size_t(cb) * p.n_ant + p.a1[bl]) * p.n_dir * NPOL;
+    const double2* s2 = p.solutions + (size_t(cb) * p.n_ant + p.a2[bl]) * p.n_dir * NPOL;
+    double2 sum[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) sum[k] = make_double2(0.0, 0.0);
+#pragma unroll 2
+    for (uint32_t d = 0; d < p.n_dir; ++d) {
+      const size_t mi = (size_t(d) * p.n_vis + v) * 2;
+      const float4 ma = __ldcs(p.model + mi), mb = __ldcs(p.model + mi + 1);
+      const double2 m[4] = {make_double2(ma.x, ma.y), make_double2(ma.z, ma.w),
+                            make_double2(mb.x, mb.y), make_double2(mb.z, mb.w)};
+      double2 c[4];
+      if constexpr (NPOL == 4) {
+        const double2* j1 = s1 + size_t(d) * 4;
+        const double2* j2 = s2 + size_t(d) * 4;
+        const double2 t0 = zadd_rn(zmul_rn(j1[0], m[0]), zmul_rn(j1[1], m[2]));
+        const double2 t1 = zadd_rn(zmul_rn(j1[0], m[1]), zmul_rn(j1[1], m[3]));
+        const double2 t2 = zadd_rn(zmul_rn(j1[2], m[0]), zmul_rn(j1[3], m[2]));
+        const double2 t3 = zadd_rn(zmul_rn(j1[2], m[1]), zmul_rn(j1[3], m[3]));
+        const double2 h0 = zconj(j2[0]), h1 = zconj(j2[1]), h2 = zconj(j2[2]),
+                      h3 = zconj(j2[3]);
+        c[0] = zadd_rn(zmul_rn(t0, h0), zmul_rn(t1, h1));
+        c[1] = zadd_rn(zmul_rn(t0, h2), zmul_rn(t1, h3));
+        c[2] = zadd_rn(zmul_rn(t2, h0), zmul_rn(t3, h1));
+        c[3] = zadd_rn(zmul_rn(t2, h2), zmul_rn(t3, h3));
+      } else if constexpr (NPOL == 2) {
+        const double2 g0 = s1[size_t(d) * 2], g1 = s1[size_t(d) * 2 + 1];
+        const double2 h0 = zconj(s2[size_t(d) * 2]), h1 = zconj(s2[size_t(d) * 2 + 1]);
+        c[0] = zmul_rn(zmul_rn(g0, m[0]), h0);
+        c[1] = zmul_rn(zmul_rn(g0, m[1]), h1);
+        c[2] = zmul_rn(zmul_rn(g1, m[2]), h0);
+        c[3] = zmul_rn(zmul_rn(g1, m[3]), h1);
+      } else {
+        const double2 f = zmul_rn(s1[d], zconj(s2[d]));
+#pragma unroll
+        for (int k = 0; k < 4; ++k) c[k] = zmul_rn(m[k], f);
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) sum[k] = zadd_rn(sum[k], c[k]);
+      if (p.model_out) {
+        __stcs(p.model_out + mi, make_float4(float(c[0].x), float(c[0].y), float(c[1].x),
+                                             float(c[1].y)));
+        __stcs(p.model_out + mi + 1, make_float4(float(c[2].x), float(c[2].y), float(c[3].x),
+                                                 float(c[3].y)));
+      }
+    }
+    if (p.data_out) {
+      const float4 da = __ldcs(p.data + v * 2), db = __ldcs(p.data + v * 2 + 1);
+      __stcs(p.data_out + v * 2,
+             make_float4(float(__dsub_rn(da.x, sum[0].x)), float(__dsub_rn(da.y, sum[0].y)),
+                         float(__dsub_rn(da.z, sum[1].x)), float(__dsub_rn(da.w, sum[1].y))));
+      __stcs(p.data_out + v * 2 + 1,
+             make_float4(float(__dsub_rn(db.x, sum[2].x)), float(__dsub_rn(db.y, sum[2].y)),
+                         float(__dsub_rn(db.z, sum[3].x)), float(__dsub_rn(db.w, sum[3].y))));
     }
   }
 }
@@ -3103,6 +3211,7 @@ struct ddsolve_ctx {
   cudaEvent_t predict_copied = nullptr;
   DevBuf raw_in;      // DP3-layout interval buffers (ddsolve_set_interval_buffers)
   DevBuf raw_model;   // the 4-correlation predicted model of one block
+  DevBuf cs_out;      // outputs of ddsolve_correct_and_subtract bound for the host
 
   // plan
   bool plan_dirty = true;
@@ -5104,6 +5213,129 @@ int ddsolve_set_interval_buffers(ddsolve_ctx* ctx, const ddsolve_interval_buffer
   }
   // The kernels just enqueued read raw_in; returning after them lets the
   // caller reuse its buffers and keeps raw_in free for the next call.
+  DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return DDSOLVE_OK;
+}
+
+int ddsolve_correct_and_subtract(ddsolve_ctx* ctx, const ddsolve_interval_buffers* in,
+                                 const double* solutions, float* data_out, float* model_out) {
+  if (!ctx) return DDSOLVE_E_INVALID;
+  if (!in || !in->antenna1 || !in->antenna2 || !solutions || in->n_times == 0 ||
+      in->n_baselines == 0 || in->n_channels < ctx->n_cb)
+    return ctx->Fail(DDSOLVE_E_INVALID, "correct and subtract: NULL pointer or empty interval");
+  if (!data_out && !model_out) return DDSOLVE_OK;  // neither subtract nor keepmodel
+  if (data_out && !in->data)
+    return ctx->Fail(DDSOLVE_E_INVALID, "correct and subtract: subtracting needs the data");
+  if (!in->model && (!in->sky || !in->frequencies || !in->station_uvw))
+    return ctx->Fail(DDSOLVE_E_INVALID,
+                     "correct and subtract: no model and no sky to predict it");
+  // DDECal.cc:1085-1090
+  if (ctx->n_sub != ctx->n_dir)
+    return ctx->Fail(DDSOLVE_E_UNSUPPORTED,
+                     "Model correction is not implemented for DDECal with direction "
+                     "dependent solution intervals");
+  for (uint32_t b = 0; b < in->n_baselines; ++b)
+    if (in->antenna1[b] >= ctx->n_ant || in->antenna2[b] >= ctx->n_ant)
+      return ctx->Fail(DDSOLVE_E_INVALID, "correct and subtract: antenna index out of range");
+  cudaSetDevice(ctx->device);
+  const uint32_t n_t = in->n_times, n_bl = in->n_baselines, n_ch = in->n_channels;
+  const uint64_t n_vis = uint64_t(n_t) * n_bl * n_ch;
+  const size_t b_data = n_vis * 32, b_m = n_vis * 32 * ctx->n_dir;
+  const size_t b_sol = size_t(ctx->n_cb) * ctx->n_ant * ctx->n_dir * ctx->n_pol * 16;
+  const size_t b_a = size_t(n_bl) * 4;
+  auto align = [](size_t x) { return (x + 255) / 256 * 256; };
+  const size_t o_sol = data_out ? align(b_data) : 0, o_a1 = o_sol + align(b_sol);
+  const size_t o_a2 = o_a1 + align(b_a);
+  DDS_CHECK_CUDA(ctx, ctx->raw_in.Reserve(o_a2 + align(b_a)));
+  DDS_CHECK_CUDA(ctx, ctx->raw_model.Reserve(b_m));
+  int rc;
+  const void *d_data = nullptr, *d_m = nullptr, *d_sol = nullptr;
+  if (data_out && (rc = DeviceView(ctx, in->data, b_data, ctx->raw_in, 0, &d_data)) != DDSOLVE_OK)
+    return rc;
+  if ((rc = DeviceView(ctx, solutions, b_sol, ctx->raw_in, o_sol, &d_sol)) != DDSOLVE_OK) return rc;
+  char* base = ctx->raw_in.as<char>();
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_a1, in->antenna1, b_a, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_a2, in->antenna2, b_a, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+  if (in->model) {
+    if ((rc = DeviceView(ctx, in->model, b_m, ctx->raw_model, 0, &d_m)) != DDSOLVE_OK) return rc;
+  } else {  // the unweighted 4-correlation model of every baseline and channel
+    const PredictJob job{n_t, n_bl, n_ch, in->frequencies, in->station_uvw,
+                         in->antenna1, in->antenna2, in->sky};
+    if ((rc = CheckPredictJob(ctx, job)) != DDSOLVE_OK) return rc;
+    if ((rc = LaunchPredict(ctx, job, ctx->raw_model.as<float2>(), 4)) != DDSOLVE_OK) return rc;
+    d_m = ctx->raw_model.ptr;
+  }
+  // Outputs in device memory are written in place; host outputs go through
+  // device memory of the context (the staged data and model when they were
+  // staged, else cs_out) and one copy back each.
+  auto on_device = [&](const void* ptr) {
+    cudaPointerAttributes a{};
+    const bool dev = cudaPointerGetAttributes(&a, ptr) == cudaSuccess &&
+                     a.type == cudaMemoryTypeDevice && a.device == ctx->device;
+    cudaGetLastError();
+    return dev;
+  };
+  const bool data_dev = data_out && on_device(data_out);
+  const bool model_dev = model_out && on_device(model_out);
+  float4* k_data = nullptr;
+  float4* k_model = nullptr;
+  size_t cs_bytes = 0;
+  if (data_out) {
+    if (data_dev)
+      k_data = reinterpret_cast<float4*>(data_out);
+    else if (d_data == base)
+      k_data = reinterpret_cast<float4*>(base);
+    else
+      cs_bytes += align(b_data);
+  }
+  if (model_out) {
+    if (model_dev)
+      k_model = reinterpret_cast<float4*>(model_out);
+    else if (d_m == ctx->raw_model.ptr)
+      k_model = ctx->raw_model.as<float4>();
+    else
+      cs_bytes += b_m;
+  }
+  if (cs_bytes) {
+    DDS_CHECK_CUDA(ctx, ctx->cs_out.Reserve(cs_bytes));
+    size_t o = 0;
+    if (data_out && !k_data) {
+      k_data = ctx->cs_out.as<float4>();
+      o = align(b_data);
+    }
+    if (model_out && !k_model) k_model = reinterpret_cast<float4*>(ctx->cs_out.as<char>() + o);
+  }
+  CorrectParams p;
+  p.data = static_cast<const float4*>(d_data);
+  p.model = static_cast<const float4*>(d_m);
+  p.data_out = k_data;
+  p.model_out = k_model;
+  p.solutions = static_cast<const double2*>(d_sol);
+  p.a1 = reinterpret_cast<const uint32_t*>(base + o_a1);
+  p.a2 = reinterpret_cast<const uint32_t*>(base + o_a2);
+  p.n_vis = n_vis;
+  p.n_bl = n_bl;
+  p.n_ch = n_ch;
+  p.n_cb = ctx->n_cb;
+  p.n_ant = ctx->n_ant;
+  p.n_dir = ctx->n_dir;
+  const uint32_t blocks =
+      uint32_t(std::min<uint64_t>((n_vis + 255) / 256, uint64_t(ctx->n_sm) * 8));
+  if (ctx->n_pol == 4)
+    correct_subtract_kernel<4><<<blocks, 256, 0, ctx->stream>>>(p);
+  else if (ctx->n_pol == 2)
+    correct_subtract_kernel<2><<<blocks, 256, 0, ctx->stream>>>(p);
+  else
+    correct_subtract_kernel<1><<<blocks, 256, 0, ctx->stream>>>(p);
+  DDS_CHECK_CUDA(ctx, cudaGetLastError());
+  if (data_out && !data_dev)
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(data_out, k_data, b_data, cudaMemcpyDeviceToHost,
+                                        ctx->stream));
+  if (model_out && !model_dev)
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(model_out, k_model, b_m, cudaMemcpyDeviceToHost,
+                                        ctx->stream));
   DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return DDSOLVE_OK;
 }

@@ -28,7 +28,7 @@ EXPORTED_SYMBOLS = (
     "ddsolve_set_channel_block_regular_sky", "ddsolve_predict_regular",
     "ddsolve_set_interval_buffers", "ddsolve_add_smoothness_constraint",
     "ddsolve_add_antenna_constraint", "ddsolve_add_reference_antenna_constraint",
-    "ddsolve_clear_constraints",
+    "ddsolve_clear_constraints", "ddsolve_correct_and_subtract",
 )
 
 
@@ -99,6 +99,7 @@ def lib():
                                                             vp, vp, vp, vp]
         L.ddsolve_predict_regular.argtypes = [vp, u32, u32, u32, vp, vp, vp, vp, vp, vp]
         L.ddsolve_set_interval_buffers.argtypes = [vp, vp]
+        L.ddsolve_correct_and_subtract.argtypes = [vp, vp, vp, vp, vp]
         L.ddsolve_solve.argtypes = [vp, vp, ctypes.POINTER(Result), vp]
         L.ddsolve_perform_iteration.argtypes = [vp, vp, vp]
         L.ddsolve_perform_iterations.argtypes = [vp, vp, u32, vp]
@@ -166,6 +167,37 @@ class IntervalBuffers(ctypes.Structure):
                 ("model", ctypes.c_void_p), ("frequencies", ctypes.c_void_p),
                 ("station_uvw", ctypes.c_void_p), ("sky", ctypes.c_void_p),
                 ("linear_weighting", ctypes.c_int32)]
+
+
+def _interval_struct(antenna1, antenna2, data, model, frequencies, station_uvw, sky,
+                     n_times=None, n_baselines=None, n_channels=None):
+    """ddsolve_interval_buffers of numpy arrays (weights and flags unset)
+    and the arrays it points into."""
+    a1 = np.ascontiguousarray(antenna1, dtype=np.uint32)
+    a2 = np.ascontiguousarray(antenna2, dtype=np.uint32)
+    keep = [a1, a2]
+    ib = IntervalBuffers()
+    if data is not None:
+        n_times, n_baselines, n_channels, _ = data.shape
+        keep.append(data)
+        ib.data = data.ctypes.data
+    elif model is not None:
+        _, n_times, n_baselines, n_channels, _ = np.shape(model)
+    ib.n_times, ib.n_baselines, ib.n_channels = n_times, n_baselines, n_channels
+    ib.antenna1, ib.antenna2 = a1.ctypes.data, a2.ctypes.data
+    if model is not None:
+        model = np.ascontiguousarray(model, np.complex64)
+        keep.append(model)
+        ib.model = model.ctypes.data
+    elif sky is not None:
+        freqs = np.ascontiguousarray(frequencies, np.float64)
+        uvw = np.ascontiguousarray(station_uvw, np.float64)
+        sky_arr, sk = _sky_struct(sky)
+        keep += [freqs, uvw, sky_arr, sk]
+        ib.frequencies, ib.station_uvw = freqs.ctypes.data, uvw.ctypes.data
+        ib.sky = ctypes.cast(sky_arr, ctypes.c_void_p).value
+    # (neither model nor sky: the library refuses the call)
+    return ib, keep
 
 
 def _sky_struct(sky):
@@ -319,33 +351,43 @@ class Context:
         None with frequencies / station_uvw / sky to predict it)."""
         data = np.ascontiguousarray(data, np.complex64)
         weights = np.ascontiguousarray(weights, np.float32)
-        n_t, n_bl, n_ch, _ = data.shape
-        a1 = np.ascontiguousarray(antenna1, dtype=np.uint32)
-        a2 = np.ascontiguousarray(antenna2, dtype=np.uint32)
-        keep = [data, weights, a1, a2]
-        ib = IntervalBuffers()
-        ib.n_times, ib.n_baselines, ib.n_channels = n_t, n_bl, n_ch
-        ib.antenna1, ib.antenna2 = a1.ctypes.data, a2.ctypes.data
-        ib.data, ib.weights = data.ctypes.data, weights.ctypes.data
+        ib, keep = _interval_struct(antenna1, antenna2, data, model, frequencies,
+                                    station_uvw, sky)
+        ib.weights = weights.ctypes.data
+        keep.append(weights)
         if flags is not None:
             flags = np.ascontiguousarray(flags, np.uint8)
             keep.append(flags)
             ib.flags = flags.ctypes.data
-        if model is not None:
-            model = np.ascontiguousarray(model, np.complex64)
-            keep.append(model)
-            ib.model = model.ctypes.data
-        elif sky is not None:
-            freqs = np.ascontiguousarray(frequencies, np.float64)
-            uvw = np.ascontiguousarray(station_uvw, np.float64)
-            sky_arr, sk = _sky_struct(sky)
-            keep += [freqs, uvw, sky_arr, sk]
-            ib.frequencies, ib.station_uvw = freqs.ctypes.data, uvw.ctypes.data
-            ib.sky = ctypes.cast(sky_arr, ctypes.c_void_p).value
-        # (neither: the library refuses the call)
         ib.linear_weighting = int(linear_weighting)
         self._check(lib().ddsolve_set_interval_buffers(self._h, ctypes.byref(ib)),
                     "ddsolve_set_interval_buffers")
+
+    def correct_and_subtract(self, antenna1, antenna2, solutions, data=None, model=None,
+                             frequencies=None, station_uvw=None, sky=None,
+                             subtract=True, keep_model=False, n_times=None,
+                             n_baselines=None, n_channels=None):
+        """ddsolve_correct_and_subtract (DDECal::CorrectAndSubtractModels):
+        data complex64 [n_t][n_bl][n_ch][4], model complex64
+        [n_dir][n_t][n_bl][n_ch][4] or None with frequencies / station_uvw /
+        sky to predict it, solutions complex128 [n_cb][n_ant][n_dir][n_pol].
+        Returns (data - sum of corrected models or None, corrected models or
+        None) as new arrays."""
+        data = None if data is None else np.ascontiguousarray(data, np.complex64)
+        ib, keep = _interval_struct(antenna1, antenna2, data, model, frequencies,
+                                    station_uvw, sky, n_times, n_baselines, n_channels)
+        sol = np.ascontiguousarray(solutions, np.complex128)
+        d_out = np.empty((ib.n_times, ib.n_baselines, ib.n_channels, 4), np.complex64) \
+            if subtract else None
+        m_out = np.empty((self.n_directions, ib.n_times, ib.n_baselines, ib.n_channels, 4),
+                         np.complex64) if keep_model else None
+        assert not subtract or data is not None, "subtracting needs the data"
+        assert sol.size == self.n_channel_blocks * self.n_antennas * self.n_directions * \
+            self.n_pol
+        self._check(lib().ddsolve_correct_and_subtract(self._h, ctypes.byref(ib), _addr(sol),
+                                                       _addr(d_out), _addr(m_out)),
+                    "ddsolve_correct_and_subtract")
+        return d_out, m_out
 
     def solve(self, solutions, step_magnitudes=None):
         """solutions: complex128 [n_cb, n_ant, n_sub, n_pol], updated in place

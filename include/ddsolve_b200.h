@@ -177,7 +177,9 @@ DDSOLVE_API int ddsolve_set_channel_block_regular_sky(
 
 /* The same prediction alone: model [n_directions][n_times * n_baselines *
  * n_channels][n_correlations][2] float32, in host memory or device memory of
- * the context's device; returns after the model is written. */
+ * the context's device; returns after the model is written.
+ * Autocorrelation baselines (antenna1 == antenna2) get a zero model, as the
+ * reference's Simulator skips them (Simulator.cc:162-163). */
 DDSOLVE_API int ddsolve_predict_regular(ddsolve_ctx* ctx, uint32_t n_times,
                                         uint32_t n_baselines, uint32_t n_channels,
                                         const double* frequencies, const double* station_uvw,
@@ -221,6 +223,39 @@ typedef struct {
  * context's device; the call returns when the interval is in place. */
 DDSOLVE_API int ddsolve_set_interval_buffers(ddsolve_ctx* ctx,
                                              const ddsolve_interval_buffers* buffers);
+
+/* The step after the solve: applies the solutions to every direction's model
+ * and subtracts the corrected models from the data. Replaces
+ * DDECal::CorrectAndSubtractModels (steps/DDECal.cc:1081-1125) with
+ * ApplySolutionAndSubtract and its ApplyFullJones/Diagonal/ScalarSolution
+ * helpers (:1004-1079), for one interval in the buffer layout of
+ * ddsolve_interval_buffers. Per visibility (autocorrelations included) and
+ * direction the corrected model is G_1 M G_2^H in FP64, as the reference's
+ * complex<double> arithmetic. Of `buffers` it reads the interval sizes,
+ * antenna1 / antenna2, data (when subtracting) and model, or with model ==
+ * NULL predicts the unweighted model of every baseline from sky /
+ * frequencies / station_uvw first (as ddsolve_set_interval_buffers); weights,
+ * flags and linear_weighting are not used (the reference corrects the
+ * unweighted buffers and leaves the flags alone). Channel block cb of the
+ * context covers channels [cb n_ch / n_cb, (cb + 1) n_ch / n_cb).
+ *   solutions: complex float64 [n_channel_blocks][n_antennas][n_directions]
+ *              [n_pol] (DDECal's solutions_ of the interval); the context
+ *              must have one solution per direction (otherwise
+ *              DDSOLVE_E_UNSUPPORTED, as the reference throws).
+ *   data_out:  [n_times][n_baselines][n_channels][4][2]: data - sum over
+ *              directions of the corrected models ("subtract"); may equal
+ *              buffers->data; NULL = no subtraction.
+ *   model_out: [n_directions][n_times][n_baselines][n_channels][4][2]: the
+ *              corrected models ("keepmodel"); may equal buffers->model;
+ *              NULL = not kept.
+ * antenna1 / antenna2 are host memory; every other array may be host or
+ * device memory of the context's device. The call returns when the outputs
+ * are written. Independent of the context's uploaded visibilities and
+ * solutions. */
+DDSOLVE_API int ddsolve_correct_and_subtract(ddsolve_ctx* ctx,
+                                             const ddsolve_interval_buffers* buffers,
+                                             const double* solutions, float* data_out,
+                                             float* model_out);
 
 /* Full iterate-until-converged solve on the device with no host constraints:
  * replaces IterativeDiagonalSolver<V>::Solve
