@@ -541,10 +541,12 @@ def run_correct_subtract(args):
     algo = n_vis * 32 * (2 + n_dir)
 
     def call(d_in, m_in, s, d_out):
-        ib = ddsolve.IntervalBuffers()
+        # one model buffer per direction, as DDECal keeps them
+        ptrs = (ctypes.c_void_p * n_dir)(*[m_in + d * (n_vis * 32) for d in range(n_dir)])
+        ib = ddsolve.SubtractBuffers()
         ib.n_times, ib.n_baselines, ib.n_channels = n_t, n_bl, n_ch
         ib.antenna1, ib.antenna2 = a1.ctypes.data, a2.ctypes.data
-        ib.data, ib.model = d_in, m_in
+        ib.data, ib.models = d_in, ctypes.cast(ptrs, ctypes.c_void_p).value
         rc = ddsolve.lib().ddsolve_correct_and_subtract(ctx._h, ctypes.byref(ib), s, d_out, None)
         if rc != 0:
             raise RuntimeError(ddsolve.lib().ddsolve_last_error(ctx._h).decode())

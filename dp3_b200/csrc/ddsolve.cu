@@ -270,13 +270,11 @@ __device__ __forceinline__ void CopyVis(const float2* __restrict__ src, float2* 
 }
 
 template <int NCORR>
-__global__ void pack_kernel(const PackSlab* __restrict__ slabs, uint32_t slab,
-                            const uint32_t* __restrict__ run_src,
+__global__ void pack_kernel(const PackSlab s, const uint32_t* __restrict__ run_src,
                             const uint32_t* __restrict__ run_len,
                             const float2* __restrict__ src_data,
                             const float2* __restrict__ src_model, uint64_t n_vis,
                             uint32_t n_dir, float2* __restrict__ dst_vis) {
-  const PackSlab s = slabs[slab];
   const uint64_t tlr = uint64_t(s.T) * s.L * s.R;
   for (uint64_t e = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; e < tlr;
        e += uint64_t(gridDim.x) * blockDim.x) {
@@ -302,47 +300,105 @@ __global__ void pack_kernel(const PackSlab* __restrict__ slabs, uint32_t slab,
 // channel block, written in the reference layout model[dir][vis][corr] that
 // pack_kernel reads -- DP3's predict of a point source (base/Simulator.cc:
 // 112-245 visit(PointSource), station phases :477-520, flat Stokes spectrum
-// :522-547): per source, phi_p = 2 pi / c (u_p l + v_p m + w_p (n - 1)) and
-// V_pq(nu) += S exp(i (phi_q - phi_p) nu), with S = I + Q, U + iV, U - iV,
-// I - Q for XX, XY, YX, YY (NCORR = 4), XX and YY (NCORR = 2) or I
-// (NCORR = 1: DP3's single-correlation data is (XX + YY) / 2). FP64
-// throughout, stored complex64. One thread per (time, baseline, direction);
-// channels in chunks of kPredictChunk / NCORR held in registers. Where the
-// block's channels are evenly spaced the phasor advances by one complex
-// multiplication per channel (exp(i dphi (nu0 + k df)) = exp(i dphi nu0)
-// exp(i dphi df)^k, restarted per chunk; relative drift ~ chunk * 1e-16,
-// far below the complex64 rounding of the result), else one sincos per
-// channel.
+// :522-547): per source and station phi_p = 2 pi / c (u_p l + v_p m + w_p
+// (n - 1)), the station shift exp(i phi_p nu), and V_pq(nu) += S shift_q(nu)
+// conj(shift_p(nu)), with S = I + Q, U + iV, U - iV, I - Q for XX, XY, YX,
+// YY (NCORR = 4), XX and YY (NCORR = 2) or I (NCORR = 1: DP3's
+// single-correlation data is (XX + YY) / 2). FP64 throughout, stored
+// complex64.
+//
+// station_phasor_kernel evaluates the station shifts once per (time,
+// direction, source, station), as the reference's Simulator does, into a
+// table: where the block's channels are evenly spaced, exp(i phi_p nu) at
+// the first channel of every chunk of CH = kPredictChunk / NCORR channels
+// and the per-channel step exp(i phi_p df); else exp(i phi_p nu) at every
+// channel. predict_kernel (one thread per (time, baseline, direction),
+// channels of a chunk in registers) forms each source's baseline phasor
+// shift_q conj(shift_p) from the table and, for even spacing, advances it
+// by the baseline step per channel (exp(i dphi (nu0 + k df)) = exp(i dphi
+// nu0) exp(i dphi df)^k, restarted per chunk; relative drift ~ chunk *
+// 1e-16, far below the complex64 rounding of the result). The sincos work
+// is per station instead of per baseline.
 // ---------------------------------------------------------------------------
 constexpr int kPredictChunk = 16;
 constexpr int kPredictThreads = 128;
 constexpr double kTwoPiOverC = 2.0 * 3.14159265358979323846 / 299792458.0;
 
 struct PredictParams {
-  const double* uvw;        // [n_times][n_ant][3] station UVW (m)
   const double* src;        // [n_src_total][8]: l, m, n - 1, I, Q, U, V, 0
   const uint32_t* src_off;  // [n_dir + 1]: sources of direction d
-  const double* freq;       // [L] channel frequencies of the block (Hz)
+  const double2* table;     // [n_times][n_dir][max_src][n_ant][n_slots] station phasors
   const uint32_t* a1;       // [n_bl]
   const uint32_t* a2;
   float2* model;            // [n_dir][n_times * n_bl * L][NCORR]
-  uint32_t n_times, n_bl, L, n_ant, n_dir, max_src;
-  int uniform;              // channels evenly spaced: df between them
+  uint32_t n_times, n_bl, L, n_ant, n_dir, max_src, n_slots;
+  int uniform;              // channels evenly spaced: chunk starts + step in the table
+};
+
+struct PhasorParams {
+  const double* uvw;        // [n_times][n_ant][3] station UVW (m)
+  const double* src;
+  const uint32_t* src_off;
+  const double* freq;       // [L] channel frequencies of the block (Hz)
+  double2* table;
+  uint32_t n_times, n_ant, n_dir, max_src, L, n_slots, chunk;
+  int uniform;
   double df;
 };
 
-// One source's phasor exp(i dphi nu) across the channels of a chunk and its
+__global__ void __launch_bounds__(kPredictThreads) station_phasor_kernel(const PhasorParams p) {
+  const uint32_t st = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t t = blockIdx.y;
+  if (st >= p.n_ant) return;
+  const double* u = p.uvw + (size_t(t) * p.n_ant + st) * 3;
+  for (uint32_t z = blockIdx.z; z < p.n_dir * p.max_src; z += gridDim.z) {
+    const uint32_t d = z / p.max_src, s = z % p.max_src;
+    const uint32_t s0 = p.src_off[d];
+    if (s >= p.src_off[d + 1] - s0) continue;
+    const double* q = p.src + size_t(s0 + s) * 8;
+    const double phi = kTwoPiOverC * (u[0] * q[0] + u[1] * q[1] + u[2] * q[2]);
+    double2* out =
+        p.table + (((size_t(t) * p.n_dir + d) * p.max_src + s) * p.n_ant + st) * p.n_slots;
+    double sn, cs;
+    if (p.uniform) {
+      const uint32_t n_chunks = p.n_slots - 1;
+      for (uint32_t k = 0; k < n_chunks; ++k) {
+        sincos(phi * p.freq[k * p.chunk], &sn, &cs);
+        out[k] = make_double2(cs, sn);
+      }
+      sincos(phi * p.df, &sn, &cs);
+      out[n_chunks] = make_double2(cs, sn);
+    } else {
+      for (uint32_t c = 0; c < p.L; ++c) {
+        sincos(phi * p.freq[c], &sn, &cs);
+        out[c] = make_double2(cs, sn);
+      }
+    }
+  }
+}
+
+// a conj(b) of two unit phasors (cos, sin)
+__device__ __forceinline__ void PhasorProduct(double2 a, double2 b, double& c, double& s) {
+  c = a.x * b.x + a.y * b.y;
+  s = a.y * b.x - a.x * b.y;
+}
+
+// One source's baseline phasor across the channels of a chunk and its
 // correlation fluxes (XX = I + Q, XY = U + iV, YX = U - iV, YY = I - Q; for 1
 // and 2 correlations real, so a term is two multiply-adds per correlation).
 template <int NCORR, int CH>
 struct PredictSource {
-  double dphi, zs, zc, ss = 0.0, sc = 1.0;
+  double zs, zc, ss = 0.0, sc = 1.0;
+  const double2* tp;
+  const double2* tq;
   double re[NCORR], im[NCORR];
-  __device__ __forceinline__ void Start(const double* q, double du, double dv, double dw,
+  __device__ __forceinline__ void Start(const double* q, const double2* tp_, const double2* tq_,
                                         const PredictParams& p, uint32_t c0) {
-    dphi = kTwoPiOverC * (du * q[0] + dv * q[1] + dw * q[2]);  // phi_q - phi_p per Hz
-    sincos(dphi * p.freq[c0], &zs, &zc);
-    if (p.uniform) sincos(dphi * p.df, &ss, &sc);
+    tp = tp_;
+    tq = tq_;
+    const uint32_t k = p.uniform ? c0 / CH : c0;
+    PhasorProduct(__ldg(tq + k), __ldg(tp + k), zc, zs);
+    if (p.uniform) PhasorProduct(__ldg(tq + p.n_slots - 1), __ldg(tp + p.n_slots - 1), sc, ss);
     if (NCORR == 1) {
       re[0] = q[3];
     } else if (NCORR == 2) {
@@ -364,7 +420,7 @@ struct PredictSource {
       zs = zc * ss + zs * sc;
       zc = r;
     } else {
-      sincos(dphi * p.freq[ch], &zs, &zc);
+      PhasorProduct(__ldg(tq + ch), __ldg(tp + ch), zc, zs);
     }
   }
   __device__ __forceinline__ void AddTo(double2 (&acc)[NCORR]) const {
@@ -386,19 +442,13 @@ __global__ void __launch_bounds__(kPredictThreads) predict_kernel(const PredictP
   constexpr int CH = kPredictChunk / NCORR;
   extern __shared__ double predict_smem[];
   const uint32_t t = blockIdx.y, d = blockIdx.z;
-  double* uvw = predict_smem;                          // [n_ant][3]
-  double* src = predict_smem + size_t(p.n_ant) * 3;    // [n_src][8]
+  double* src = predict_smem;  // [n_src][8]
   const uint32_t s0 = p.src_off[d], ns = p.src_off[d + 1] - s0;
-  for (uint32_t i = threadIdx.x; i < p.n_ant * 3; i += blockDim.x)
-    uvw[i] = p.uvw[size_t(t) * p.n_ant * 3 + i];
   for (uint32_t i = threadIdx.x; i < ns * 8; i += blockDim.x) src[i] = p.src[size_t(s0) * 8 + i];
   __syncthreads();
   const uint32_t bl = blockIdx.x * blockDim.x + threadIdx.x;
   if (bl >= p.n_bl) return;
   const uint32_t ap = p.a1[bl], aq = p.a2[bl];
-  const double du = uvw[aq * 3] - uvw[ap * 3];
-  const double dv = uvw[aq * 3 + 1] - uvw[ap * 3 + 1];
-  const double dw = uvw[aq * 3 + 2] - uvw[ap * 3 + 2];
   const uint64_t n_vis = uint64_t(p.n_times) * p.n_bl * p.L;
   const uint64_t v0 = (uint64_t(t) * p.n_bl + bl) * p.L;
   float2* out = p.model + (uint64_t(d) * n_vis + v0) * NCORR;
@@ -406,6 +456,11 @@ __global__ void __launch_bounds__(kPredictThreads) predict_kernel(const PredictP
     for (uint32_t i = 0; i < p.L * NCORR; ++i) out[i] = make_float2(0.f, 0.f);
     return;
   }
+  // this (time, direction)'s table: [source][station][slot]
+  const size_t src_stride = size_t(p.n_ant) * p.n_slots;
+  const double2* tab = p.table + (size_t(t) * p.n_dir + d) * p.max_src * src_stride;
+  const double2* tp0 = tab + size_t(ap) * p.n_slots;
+  const double2* tq0 = tab + size_t(aq) * p.n_slots;
   for (uint32_t c0 = 0; c0 < p.L; c0 += CH) {
     const uint32_t nc = min(uint32_t(CH), p.L - c0);
     double2 acc[CH][NCORR];
@@ -419,8 +474,8 @@ __global__ void __launch_bounds__(kPredictThreads) predict_kernel(const PredictP
     uint32_t s = 0;
     for (; s + 2 <= ns; s += 2) {
       PredictSource<NCORR, CH> a, b;
-      a.Start(src + s * 8, du, dv, dw, p, c0);
-      b.Start(src + (s + 1) * 8, du, dv, dw, p, c0);
+      a.Start(src + s * 8, tp0 + s * src_stride, tq0 + s * src_stride, p, c0);
+      b.Start(src + (s + 1) * 8, tp0 + (s + 1) * src_stride, tq0 + (s + 1) * src_stride, p, c0);
 #pragma unroll
       for (int c = 0; c < CH; ++c) {
         if (c < int(nc)) {
@@ -435,7 +490,7 @@ __global__ void __launch_bounds__(kPredictThreads) predict_kernel(const PredictP
     }
     if (s < ns) {
       PredictSource<NCORR, CH> a;
-      a.Start(src + s * 8, du, dv, dw, p, c0);
+      a.Start(src + s * 8, tp0 + s * src_stride, tq0 + s * src_stride, p, c0);
 #pragma unroll
       for (int c = 0; c < CH; ++c) {
         if (c < int(nc)) {
@@ -562,10 +617,10 @@ __global__ void weigh_kernel(const WeighParams p) {
 // model per direction read, the same written back: an HBM-bound stream.
 // ---------------------------------------------------------------------------
 struct CorrectParams {
-  const float4* data;        // [n_vis][2]: XX XY | YX YY
-  const float4* model;       // [n_dir][n_vis][2]
-  float4* data_out;          // or null (no subtraction)
-  float4* model_out;         // or null (models not kept)
+  const float4* data;                // [n_vis][2]: XX XY | YX YY
+  const float4* const* model;        // [n_dir] -> [n_vis][2]
+  float4* data_out;                  // or null (no subtraction)
+  float4* const* model_out;          // [n_dir] -> [n_vis][2], or null (models not kept)
   const double2* solutions;  // [n_cb][n_ant][n_dir][NPOL]
   const uint32_t* a1;        // [n_bl]
   const uint32_t* a2;
@@ -597,8 +652,8 @@ __global__ void __launch_bounds__(256) correct_subtract_kernel(const CorrectPara
     for (int k = 0; k < 4; ++k) sum[k] = make_double2(0.0, 0.0);
 #pragma unroll 2
     for (uint32_t d = 0; d < p.n_dir; ++d) {
-      const size_t mi = (size_t(d) * p.n_vis + v) * 2;
-      const float4 ma = __ldcs(p.model + mi), mb = __ldcs(p.model + mi + 1);
+      const float4* md = p.model[d] + v * 2;
+      const float4 ma = __ldcs(md), mb = __ldcs(md + 1);
       const double2 m[4] = {make_double2(ma.x, ma.y), make_double2(ma.z, ma.w),
                             make_double2(mb.x, mb.y), make_double2(mb.z, mb.w)};
       double2 c[4];
@@ -630,10 +685,9 @@ __global__ void __launch_bounds__(256) correct_subtract_kernel(const CorrectPara
 #pragma unroll
       for (int k = 0; k < 4; ++k) sum[k] = zadd_rn(sum[k], c[k]);
       if (p.model_out) {
-        __stcs(p.model_out + mi, make_float4(float(c[0].x), float(c[0].y), float(c[1].x),
-                                             float(c[1].y)));
-        __stcs(p.model_out + mi + 1, make_float4(float(c[2].x), float(c[2].y), float(c[3].x),
-                                                 float(c[3].y)));
+        float4* mo = p.model_out[d] + v * 2;
+        __stcs(mo, make_float4(float(c[0].x), float(c[0].y), float(c[1].x), float(c[1].y)));
+        __stcs(mo + 1, make_float4(float(c[2].x), float(c[2].y), float(c[3].x), float(c[3].y)));
       }
     }
     if (p.data_out) {
@@ -2656,10 +2710,11 @@ __global__ void __launch_bounds__(256)
 //   side 2 (a = antenna 2): Y = J_1 M,    num = sum R_d^H Y = P_2 + J_a den_2,
 //                           den_2 = sum Y^H Y
 // (IterativeFullJonesSolver.cc:107-187), next = num den^-1 (NaN where den is
-// singular). fj_pass_kernel: one thread per run of visibilities (fixed
-// baseline and sub-solutions), FP32 products and sums as the reference's
-// MC2x2F arithmetic, the run's P and den of every direction and side written
-// to its own partial slot (no atomics); fj_finalize_kernel: one thread per
+// singular). fj_pass_kernel: one thread per part of a run of visibilities
+// (fixed baseline and sub-solutions; the rows of a run are split into
+// n_parts parts), FP32 products and sums as the reference's MC2x2F
+// arithmetic, the part's P and den of every direction and side written to its
+// own partial slot (no atomics); fj_finalize_kernel: one thread per
 // (channel block, antenna, sub-solution), the slots of its list summed in
 // FP64 in run order, the 2x2 inverse and product in FP64, then Step, the
 // 4-polarization AssignSolutions norm (SolverBase.cc:268-284) and the loop
@@ -2738,8 +2793,9 @@ struct FjPassParams {
   const uint32_t* slab_sol;   // [slab][n_dir]
   const uint32_t* run_start;  // [n_slabs + 1]: first global run of each slab
   const double2* solutions;   // [cb][ant][sub][4]
-  float* partials;            // [global run][direction][kFjSlotFloats]
+  float* partials;            // [part][global run][direction][kFjSlotFloats]
   uint32_t n_slabs, n_runs, n_ant, n_sub, n_dir;
+  uint32_t n_parts;           // each run's rows split into this many parts
   uint32_t d0;                // fj_chunk_kernel: first direction of the launch
   const LoopState* state;
   int32_t use_handle;
@@ -2783,8 +2839,9 @@ __device__ __forceinline__ void FjStoreSlots(float* out, const C22* P1, const C2
 template <int NC>
 __global__ void __launch_bounds__(kFjThreads) fj_chunk_kernel(const FjPassParams p) {
   if (SolveStopped(p.state, p.use_handle)) return;
-  const uint32_t gr = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gr >= p.n_runs) return;
+  const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gt >= p.n_runs * p.n_parts) return;
+  const uint32_t gr = gt % p.n_runs, part = gt / p.n_runs;
   const uint32_t si = FjSlabOf(p, gr);
   const SlabDesc sl = p.slabs[si];
   const uint32_t r = gr - p.run_start[si];
@@ -2805,7 +2862,8 @@ __global__ void __launch_bounds__(kFjThreads) fj_chunk_kernel(const FjPassParams
   }
   const float2* vis = static_cast<const float2*>(sl.vis);
   const uint64_t rows = uint64_t(sl.T) * sl.L;
-  for (uint64_t row = 0; row < rows; ++row) {
+  const uint64_t row_end = rows * (part + 1) / p.n_parts;
+  for (uint64_t row = rows * part / p.n_parts; row < row_end; ++row) {
     C22 R = LoadC22(vis + SlabElem(sl.R, sl.W, nd + 1, row, 0, r) * 4);
     for (uint32_t e = 0; e < nd; ++e) {
       const uint32_t s = p.slab_sol[sl.sol_off + e];
@@ -2826,14 +2884,15 @@ __global__ void __launch_bounds__(kFjThreads) fj_chunk_kernel(const FjPassParams
       AddHermMul22(D2[d], Y, Y);
     }
   }
-  FjStoreSlots<NC>(p.partials + (size_t(gr) * nd + p.d0) * kFjSlotFloats, P1, D1, P2, D2);
+  FjStoreSlots<NC>(p.partials + (size_t(gt) * nd + p.d0) * kFjSlotFloats, P1, D1, P2, D2);
 }
 
 template <int ND>
 __global__ void __launch_bounds__(kFjThreads) fj_pass_kernel(const FjPassParams p) {
   if (SolveStopped(p.state, p.use_handle)) return;
-  const uint32_t gr = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gr >= p.n_runs) return;
+  const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gt >= p.n_runs * p.n_parts) return;
+  const uint32_t gr = gt % p.n_runs, part = gt / p.n_runs;
   const uint32_t lo = FjSlabOf(p, gr);
   const SlabDesc sl = p.slabs[lo];
   const uint32_t r = gr - p.run_start[lo];
@@ -2852,7 +2911,8 @@ __global__ void __launch_bounds__(kFjThreads) fj_pass_kernel(const FjPassParams 
   }
   const float2* vis = static_cast<const float2*>(sl.vis);
   const uint64_t rows = uint64_t(sl.T) * sl.L;
-  for (uint64_t row = 0; row < rows; ++row) {
+  const uint64_t row_end = rows * (part + 1) / p.n_parts;
+  for (uint64_t row = rows * part / p.n_parts; row < row_end; ++row) {
     C22 M[ND];
 #pragma unroll
     for (int d = 0; d < ND; ++d) M[d] = LoadC22(vis + SlabElem(sl.R, sl.W, ND + 1, row, 1 + d, r) * 4);
@@ -2874,7 +2934,7 @@ __global__ void __launch_bounds__(kFjThreads) fj_pass_kernel(const FjPassParams 
       AddHermMul22(D2[d], Y[d], Y[d]);
     }
   }
-  FjStoreSlots<ND>(p.partials + size_t(gr) * ND * kFjSlotFloats, P1, D1, P2, D2);
+  FjStoreSlots<ND>(p.partials + size_t(gt) * ND * kFjSlotFloats, P1, D1, P2, D2);
 }
 
 struct D22 {
@@ -2926,25 +2986,45 @@ struct FjFinParams {
 };
 
 __global__ void __launch_bounds__(kThreads) fj_finalize_kernel(const FjFinParams p) {
-  const uint32_t item = blockIdx.x * blockDim.x + threadIdx.x;
+  // one warp per item: the lanes sum interleaved entries of its list, a
+  // butterfly combines them (a fixed order, so the result is reproducible),
+  // lane 0 does the rest
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const DevSettings st = *p.settings;
   const bool stopped = !p.host_mode && p.state->done;
   double norm_sum = 0.0;
   uint32_t norm_cnt = 0;
   if (item < p.n_items && !stopped) {
-    // the item's slots, in run order: P and den of its side
+    // the item's slots: P and den of its side
     double pn[8], dn[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) pn[k] = dn[k] = 0.0;
-    for (uint32_t e = p.list_off[item]; e < p.list_off[item + 1]; ++e) {
+    for (uint32_t e = p.list_off[item] + lane; e < p.list_off[item + 1]; e += 32) {
       const uint32_t en = p.list_ent[e];
-      const float* slot = p.partials + size_t(en >> 1) * kFjSlotFloats + (en & 1u) * 16;
+      const float4* slot = reinterpret_cast<const float4*>(
+          p.partials + size_t(en >> 1) * kFjSlotFloats + (en & 1u) * 16);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        pn[k] += double(__ldcg(slot + k));
-        dn[k] += double(__ldcg(slot + 8 + k));
+      for (int q = 0; q < 2; ++q) {
+        const float4 a = __ldcg(slot + q), b = __ldcg(slot + 2 + q);
+        pn[4 * q] += a.x;
+        pn[4 * q + 1] += a.y;
+        pn[4 * q + 2] += a.z;
+        pn[4 * q + 3] += a.w;
+        dn[4 * q] += b.x;
+        dn[4 * q + 1] += b.y;
+        dn[4 * q + 2] += b.z;
+        dn[4 * q + 3] += b.w;
       }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        pn[k] += __shfl_xor_sync(0xffffffffu, pn[k], o);
+        dn[k] += __shfl_xor_sync(0xffffffffu, dn[k], o);
+      }
+    if (lane == 0) {
     double2* sol = p.solutions + size_t(item) * 4;
     D22 old, ja, den, num;
 #pragma unroll
@@ -3012,6 +3092,7 @@ __global__ void __launch_bounds__(kThreads) fj_finalize_kernel(const FjFinParams
       }
       if (!all_finite) p.nonfinite[item / (p.n_ant * p.n_sub)] = 1u;
     }
+    }  // lane 0
   }
   if (p.host_mode) return;
   __shared__ double s_sum[kThreads];
@@ -3202,8 +3283,15 @@ struct ddsolve_ctx {
   uint32_t tune_stages = 0, tune_gbuf = 0;
 
   std::vector<ChannelBlockStore> cbs;
-  DevBuf staging, pack_desc, run_src_dev, run_len_dev;
+  DevBuf staging, run_src_dev, run_len_dev;
+  // host copies of what run_src_dev / run_len_dev hold
+  std::vector<uint32_t> staged_run_src, staged_run_len;
+  // SetRegularBlock's baseline order for the antenna arrays it was made for
+  // (every channel block and interval of one layout repeats them)
+  std::vector<uint32_t> order_a1, order_a2, order_bl, order_ant;
+  std::vector<uint8_t> order_flip;
   DevBuf predict_in;  // station UVW, sky, frequencies and antennas of a predict
+  DevBuf predict_table;  // station phasors of a predict (station_phasor_kernel)
   // Pinned host image of predict_in (one copy per predict), reusable once
   // the copy recorded in predict_copied has run.
   void* predict_host = nullptr;
@@ -3257,7 +3345,7 @@ struct ddsolve_ctx {
   // full-Jones plan: first global run of each slab, per (cb, antenna,
   // sub-solution) item the list of its partial slots
   DevBuf d_fj_run_start, d_fj_list_off, d_fj_list_ent;
-  uint32_t fj_n_slabs = 0, fj_n_runs = 0, fj_blocks = 0;
+  uint32_t fj_n_slabs = 0, fj_n_runs = 0, fj_blocks = 0, fj_parts = 1;
   // independent solution intervals (ddsolve_set_intervals): interval g owns
   // channel blocks [group_first_cb[g], group_first_cb[g + 1])
   uint32_t n_groups = 1;
@@ -3272,7 +3360,7 @@ struct ddsolve_ctx {
   cudaGraphConditionalHandle handle = 0;
   bool graph_ok = false;
   uint64_t last_launches = 0;
-  uint64_t last_predict_launches = 0;  // predict_kernel launches since creation
+  uint64_t last_predict_launches = 0;  // predict launches (phasor table + model) since creation
   // Pinned host staging of the per-call read-backs (error counters, loop
   // state, step magnitudes), copied before the call's single synchronization.
   struct HostStage {
@@ -3525,11 +3613,11 @@ int CheckPredictJob(ddsolve_ctx* ctx, const PredictJob& j) {
       return ctx->Fail(DDSOLVE_E_INVALID, "predict: NULL source arrays");
     max_src = std::max(max_src, j.sky[d].n_sources);
   }
-  const size_t smem = (size_t(ctx->n_ant) * 3 + size_t(max_src) * 8) * sizeof(double);
+  const size_t smem = size_t(max_src) * 8 * sizeof(double);
   if (smem > kPredictMaxSmem)
     return ctx->Fail(DDSOLVE_E_UNSUPPORTED,
-                     "predict: stations x 3 + sources x 8 doubles exceed 200 KiB of shared "
-                     "memory (too many sources in one direction)");
+                     "predict: sources x 8 doubles exceed 200 KiB of shared memory (more than "
+                     "3200 sources in one direction)");
   for (uint32_t b = 0; b < j.n_bl; ++b)
     if (j.a1[b] >= ctx->n_ant || j.a2[b] >= ctx->n_ant)
       return ctx->Fail(DDSOLVE_E_INVALID, "predict: antenna index out of range");
@@ -3602,11 +3690,37 @@ int LaunchPredict(ddsolve_ctx* ctx, const PredictJob& j, float2* model, uint32_t
     if (device_piece[k])
       DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + pieces[k].off, pieces[k].src, pieces[k].bytes,
                                           cudaMemcpyDeviceToDevice, ctx->stream));
+  // station phasors of every (time, direction, source, station)
+  const uint32_t chunk = uint32_t(kPredictChunk) / nc;
+  const uint32_t n_slots = uniform ? (j.L + chunk - 1) / chunk + 1 : j.L;
+  const size_t table_entries =
+      size_t(j.n_times) * ctx->n_dir * std::max(max_src, 1u) * ctx->n_ant * n_slots;
+  DDS_CHECK_CUDA(ctx, ctx->predict_table.Reserve(table_entries * sizeof(double2)));
+  PhasorParams ph;
+  ph.uvw = reinterpret_cast<const double*>(base);
+  ph.src = reinterpret_cast<const double*>(base + o_src);
+  ph.src_off = reinterpret_cast<const uint32_t*>(base + o_off);
+  ph.freq = reinterpret_cast<const double*>(base + o_f);
+  ph.table = ctx->predict_table.as<double2>();
+  ph.n_times = j.n_times;
+  ph.n_ant = ctx->n_ant;
+  ph.n_dir = ctx->n_dir;
+  ph.max_src = max_src;
+  ph.L = j.L;
+  ph.n_slots = n_slots;
+  ph.chunk = chunk;
+  ph.uniform = uniform;
+  ph.df = df;
+  if (max_src > 0) {
+    const dim3 pgrid((ctx->n_ant + kPredictThreads - 1) / kPredictThreads, j.n_times,
+                     std::min<uint32_t>(ctx->n_dir * max_src, 65535u));
+    station_phasor_kernel<<<pgrid, kPredictThreads, 0, ctx->stream>>>(ph);
+    DDS_CHECK_CUDA(ctx, cudaGetLastError());
+  }
   PredictParams p;
-  p.uvw = reinterpret_cast<const double*>(base);
   p.src = reinterpret_cast<const double*>(base + o_src);
   p.src_off = reinterpret_cast<const uint32_t*>(base + o_off);
-  p.freq = reinterpret_cast<const double*>(base + o_f);
+  p.table = ctx->predict_table.as<double2>();
   p.a1 = reinterpret_cast<const uint32_t*>(base + o_a1);
   p.a2 = reinterpret_cast<const uint32_t*>(base + o_a2);
   p.model = model;
@@ -3616,9 +3730,9 @@ int LaunchPredict(ddsolve_ctx* ctx, const PredictJob& j, float2* model, uint32_t
   p.n_ant = ctx->n_ant;
   p.n_dir = ctx->n_dir;
   p.max_src = max_src;
+  p.n_slots = n_slots;
   p.uniform = uniform;
-  p.df = df;
-  const size_t smem = (size_t(ctx->n_ant) * 3 + size_t(max_src) * 8) * sizeof(double);
+  const size_t smem = size_t(max_src) * 8 * sizeof(double);
   const dim3 grid((j.n_bl + kPredictThreads - 1) / kPredictThreads, j.n_times, ctx->n_dir);
   const void* fn = nc == 1   ? reinterpret_cast<const void*>(predict_kernel<1>)
                    : nc == 2 ? reinterpret_cast<const void*>(predict_kernel<2>)
@@ -3628,7 +3742,7 @@ int LaunchPredict(ddsolve_ctx* ctx, const PredictJob& j, float2* model, uint32_t
   void* args[] = {&p};
   DDS_CHECK_CUDA(ctx, cudaLaunchKernel(fn, grid, dim3(kPredictThreads), args, smem,
                                        ctx->stream));
-  ctx->last_predict_launches += 1;
+  ctx->last_predict_launches += max_src > 0 ? 2 : 1;
   return DDSOLVE_OK;
 }
 
@@ -3655,24 +3769,32 @@ int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const StageFn& stage)
     s.W = LayoutTileRuns(ctx, s.R);
     ps[i] = PackSlab{s.elem_off, s.src_base, s.tstride, s.T, s.L, s.R, s.run_off, s.W};
   }
-  DDS_CHECK_CUDA(ctx, ctx->pack_desc.Reserve(ps.size() * sizeof(PackSlab)));
   char* st = ctx->staging.as<char>();
   if (cb.n_vis) {
     const int rc = stage(st);
     if (rc != DDSOLVE_OK) return rc;
   }
-  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(cb.run_ant_dev.ptr, cb.run_ant.data(),
-                                      cb.run_ant.size() * 4,
-                                      cudaMemcpyHostToDevice, ctx->stream));
-  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->run_src_dev.ptr, cb.run_src.data(),
-                                      cb.run_src.size() * 4,
-                                      cudaMemcpyHostToDevice, ctx->stream));
-  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->run_len_dev.ptr, cb.run_len.data(),
-                                      cb.run_len.size() * 4,
-                                      cudaMemcpyHostToDevice, ctx->stream));
-  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->pack_desc.ptr, ps.data(),
-                                      ps.size() * sizeof(PackSlab),
-                                      cudaMemcpyHostToDevice, ctx->stream));
+  // The run arrays are copied only when they changed: a copy from pageable
+  // memory waits for the stream, which would hold this host thread behind
+  // the kernels already queued (the previous block's predict and pack, or a
+  // solve of the other context). Consecutive blocks and intervals of one
+  // layout repeat them.
+  if (cb.run_ant_dev.realloc_flag || !cb.set || cb.run_ant != cb.prev_run_ant)
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(cb.run_ant_dev.ptr, cb.run_ant.data(),
+                                        cb.run_ant.size() * 4,
+                                        cudaMemcpyHostToDevice, ctx->stream));
+  if (ctx->run_src_dev.realloc_flag || ctx->run_len_dev.realloc_flag ||
+      cb.run_src != ctx->staged_run_src || cb.run_len != ctx->staged_run_len) {
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->run_src_dev.ptr, cb.run_src.data(),
+                                        cb.run_src.size() * 4,
+                                        cudaMemcpyHostToDevice, ctx->stream));
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->run_len_dev.ptr, cb.run_len.data(),
+                                        cb.run_len.size() * 4,
+                                        cudaMemcpyHostToDevice, ctx->stream));
+    ctx->staged_run_src = cb.run_src;
+    ctx->staged_run_len = cb.run_len;
+  }
+  ctx->run_src_dev.realloc_flag = ctx->run_len_dev.realloc_flag = false;
   for (size_t i = 0; i < cb.slabs.size(); ++i) {
     const uint64_t tlr = uint64_t(cb.slabs[i].T) * cb.slabs[i].L * cb.slabs[i].R;
     if (tlr == 0) continue;
@@ -3683,15 +3805,15 @@ int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const StageFn& stage)
     float2* dst = cb.vis.as<float2>();
     if (E == 8)
       pack_kernel<1><<<blocks, 256, 0, ctx->stream>>>(
-          ctx->pack_desc.as<PackSlab>(), uint32_t(i), ctx->run_src_dev.as<uint32_t>(),
+          ps[i], ctx->run_src_dev.as<uint32_t>(),
           ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir, dst);
     else if (E == 16)
       pack_kernel<2><<<blocks, 256, 0, ctx->stream>>>(
-          ctx->pack_desc.as<PackSlab>(), uint32_t(i), ctx->run_src_dev.as<uint32_t>(),
+          ps[i], ctx->run_src_dev.as<uint32_t>(),
           ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir, dst);
     else
       pack_kernel<4><<<blocks, 256, 0, ctx->stream>>>(
-          ctx->pack_desc.as<PackSlab>(), uint32_t(i), ctx->run_src_dev.as<uint32_t>(),
+          ps[i], ctx->run_src_dev.as<uint32_t>(),
           ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir, dst);
     DDS_CHECK_CUDA(ctx, cudaGetLastError());
   }
@@ -4056,6 +4178,21 @@ int BuildFullJonesPlan(ddsolve_ctx* ctx) {
   std::vector<SlabDesc> descs;
   std::vector<uint32_t> slab_sol, run_start{0};
   std::vector<std::vector<uint32_t>> lists(size_t(ctx->n_cb) * n_ant * n_sub);
+  // Rows of a run split into parts (one thread each) so that the grid has
+  // about four times the threads one wave holds (a thread of the four-
+  // direction kernel needs most of its 255 registers: 256 threads per SM),
+  // keeping at least 16 rows per part (the parts' slots then add at most a
+  // quarter to the pass's bytes).
+  uint64_t total_runs = 0, max_rows = 1;
+  for (uint32_t c = 0; c < ctx->n_cb; ++c)
+    for (const HostSlab& s : ctx->cbs[c].slabs) {
+      total_runs += s.R;
+      max_rows = std::max<uint64_t>(max_rows, uint64_t(s.T) * s.L);
+    }
+  const uint64_t want_threads = uint64_t(std::max(ctx->n_sm, 1)) * 256 * 4;
+  uint64_t parts = total_runs ? (want_threads + total_runs - 1) / total_runs : 1;
+  parts = std::max<uint64_t>(1, std::min<uint64_t>({parts, max_rows / 16, 16}));
+  if (total_runs * parts * n_dir >= (uint64_t(1) << 31)) parts = 1;
   uint64_t n_runs = 0;
   for (uint32_t c = 0; c < ctx->n_cb; ++c) {
     ChannelBlockStore& cb = ctx->cbs[c];
@@ -4074,14 +4211,15 @@ int BuildFullJonesPlan(ddsolve_ctx* ctx) {
       for (uint32_t r = 0; r < s.R; ++r) {
         const uint32_t ap = cb.run_ant[s.run_off + r];
         const uint32_t a1 = ap & 0xFFFFu, a2 = ap >> 16;
-        for (uint32_t d = 0; d < n_dir; ++d) {
-          const uint64_t slot = (n_runs + r) * n_dir + d;
-          if (slot >= (uint64_t(1) << 31))
-            return ctx->Fail(DDSOLVE_E_UNSUPPORTED, "full-Jones: too many runs");
-          const size_t base = size_t(c) * n_ant;
-          lists[(base + a1) * n_sub + s.sol[d]].push_back(uint32_t(slot << 1));
-          lists[(base + a2) * n_sub + s.sol[d]].push_back(uint32_t(slot << 1) | 1u);
-        }
+        for (uint64_t part = 0; part < parts; ++part)
+          for (uint32_t d = 0; d < n_dir; ++d) {
+            const uint64_t slot = (part * total_runs + n_runs + r) * n_dir + d;
+            if (slot >= (uint64_t(1) << 31))
+              return ctx->Fail(DDSOLVE_E_UNSUPPORTED, "full-Jones: too many runs");
+            const size_t base = size_t(c) * n_ant;
+            lists[(base + a1) * n_sub + s.sol[d]].push_back(uint32_t(slot << 1));
+            lists[(base + a2) * n_sub + s.sol[d]].push_back(uint32_t(slot << 1) | 1u);
+          }
       }
       n_runs += s.R;
       run_start.push_back(uint32_t(n_runs));
@@ -4107,15 +4245,16 @@ int BuildFullJonesPlan(ddsolve_ctx* ctx) {
       (rc = up(ctx->d_fj_list_ent, ent.data(), ent.size() * 4)) != DDSOLVE_OK)
     return rc;
   DDS_CHECK_CUDA(ctx, ctx->d_partials.Reserve(
-                          std::max<uint64_t>(n_runs, 1) * n_dir * kFjSlotFloats * 4));
+                          std::max<uint64_t>(n_runs * parts, 1) * n_dir * kFjSlotFloats * 4));
   const uint32_t n_items = ctx->n_cb * n_ant * n_sub;
-  ctx->fj_blocks = (n_items + kThreads - 1) / kThreads;
+  ctx->fj_blocks = uint32_t((uint64_t(n_items) * 32 + kThreads - 1) / kThreads);  // a warp per item
   DDS_CHECK_CUDA(ctx, ctx->d_block_sum.Reserve(size_t(ctx->fj_blocks) * 8));
   DDS_CHECK_CUDA(ctx, ctx->d_block_cnt.Reserve(size_t(ctx->fj_blocks) * 4));
   // keep the host vectors alive until the copies have been issued from pageable memory
   DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   ctx->fj_n_slabs = uint32_t(descs.size());
   ctx->fj_n_runs = uint32_t(n_runs);
+  ctx->fj_parts = uint32_t(parts);
   ctx->use_pipe = false;
   ctx->plan_dirty = false;
   return DDSOLVE_OK;
@@ -4645,7 +4784,9 @@ int LaunchFullJones(ddsolve_ctx* ctx, bool host_mode, bool use_handle, bool with
   pp.state = ctx->d_state.as<LoopState>();
   pp.use_handle = (use_handle && !host_mode) ? 1 : 0;
   pp.d0 = 0;
-  const uint32_t blocks = std::max<uint32_t>(1, (ctx->fj_n_runs + kFjThreads - 1) / kFjThreads);
+  pp.n_parts = ctx->fj_parts;
+  const uint32_t blocks = std::max<uint32_t>(
+      1, uint32_t((uint64_t(ctx->fj_n_runs) * ctx->fj_parts + kFjThreads - 1) / kFjThreads));
   switch (ctx->n_dir) {
     case 1: fj_pass_kernel<1><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
     case 2: fj_pass_kernel<2><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
@@ -4986,39 +5127,55 @@ static int SetRegularBlock(ddsolve_ctx* ctx, uint32_t cbi, uint32_t n_times,
   if (cbi >= ctx->n_cb) return ctx->Fail(DDSOLVE_E_INVALID, "channel block out of range");
   if (n_times == 0 || n_baselines == 0 || n_channels == 0 || !antenna1 || !antenna2)
     return ctx->Fail(DDSOLVE_E_INVALID, "empty channel block or NULL pointer");
-  for (uint32_t b = 0; b < n_baselines; ++b)
-    if (antenna1[b] >= ctx->n_ant || antenna2[b] >= ctx->n_ant ||
-        antenna1[b] == antenna2[b])
-      return ctx->Fail(DDSOLVE_E_INVALID, "bad antenna pair (or autocorrelation)");
-  cudaSetDevice(ctx->device);
-  ChannelBlockStore& cb = ctx->cbs[cbi];
-  cb.n_vis = uint64_t(n_times) * n_baselines * n_channels;
-  cb.slabs.clear();
   // Runs in cyclic-diagonal order. Each baseline is oriented so that its
   // cyclic distance delta = (a2 - a1) mod n_ant is at most n_ant / 2 (a
   // swapped baseline is stored Hermitian-transposed by the repack, which does
   // not change the normal equations); runs are sorted by (delta, a1). A
   // cyclic diagonal is then a permutation (distinct first and distinct second
   // antennas), so windows of up to n_ant consecutive runs have distinct
-  // antennas on each side: conflict-free shared-memory accumulation.
+  // antennas on each side: conflict-free shared-memory accumulation. The
+  // order depends on the antenna arrays only, so it is computed once for the
+  // channel blocks and intervals that repeat them.
   const uint32_t n_ant = ctx->n_ant;
-  std::vector<uint32_t> o_a1(n_baselines), o_a2(n_baselines), o_delta(n_baselines);
-  std::vector<uint8_t> o_flip(n_baselines);
-  for (uint32_t b = 0; b < n_baselines; ++b) {
-    const uint32_t a = antenna1[b], c = antenna2[b];
-    const uint32_t d = (c + n_ant - a) % n_ant;
-    bool flip = 2 * d > n_ant;
-    if (2 * d == n_ant) flip = a > c;  // half-way diagonal: first antenna < n/2
-    o_flip[b] = flip;
-    o_a1[b] = flip ? c : a;
-    o_a2[b] = flip ? a : c;
-    o_delta[b] = flip ? n_ant - d : d;
+  const bool same_order = ctx->order_a1.size() == n_baselines &&
+                          std::equal(antenna1, antenna1 + n_baselines, ctx->order_a1.begin()) &&
+                          std::equal(antenna2, antenna2 + n_baselines, ctx->order_a2.begin());
+  if (!same_order) {
+    for (uint32_t b = 0; b < n_baselines; ++b)
+      if (antenna1[b] >= n_ant || antenna2[b] >= n_ant || antenna1[b] == antenna2[b])
+        return ctx->Fail(DDSOLVE_E_INVALID, "bad antenna pair (or autocorrelation)");
+    std::vector<uint32_t> o_a1(n_baselines), o_a2(n_baselines), o_delta(n_baselines);
+    std::vector<uint8_t> o_flip(n_baselines);
+    for (uint32_t b = 0; b < n_baselines; ++b) {
+      const uint32_t a = antenna1[b], c = antenna2[b];
+      const uint32_t d = (c + n_ant - a) % n_ant;
+      bool flip = 2 * d > n_ant;
+      if (2 * d == n_ant) flip = a > c;  // half-way diagonal: first antenna < n/2
+      o_flip[b] = flip;
+      o_a1[b] = flip ? c : a;
+      o_a2[b] = flip ? a : c;
+      o_delta[b] = flip ? n_ant - d : d;
+    }
+    std::vector<uint32_t> order(n_baselines);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+      return o_delta[x] != o_delta[y] ? o_delta[x] < o_delta[y] : o_a1[x] < o_a1[y];
+    });
+    ctx->order_a1.assign(antenna1, antenna1 + n_baselines);
+    ctx->order_a2.assign(antenna2, antenna2 + n_baselines);
+    ctx->order_bl = order;
+    ctx->order_ant.resize(n_baselines);
+    ctx->order_flip.resize(n_baselines);
+    for (uint32_t r = 0; r < n_baselines; ++r) {
+      const uint32_t b = order[r];
+      ctx->order_ant[r] = o_a1[b] | (o_a2[b] << 16);
+      ctx->order_flip[r] = o_flip[b];
+    }
   }
-  std::vector<uint32_t> order(n_baselines);
-  std::iota(order.begin(), order.end(), 0u);
-  std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
-    return o_delta[x] != o_delta[y] ? o_delta[x] < o_delta[y] : o_a1[x] < o_a1[y];
-  });
+  cudaSetDevice(ctx->device);
+  ChannelBlockStore& cb = ctx->cbs[cbi];
+  cb.n_vis = uint64_t(n_times) * n_baselines * n_channels;
+  cb.slabs.clear();
   // Run arrays padded to whole 16-byte groups (pipe_kernel bulk-copies
   // them); padding runs have no antennas and no visibilities.
   const size_t n_run_pad = (size_t(n_baselines) + 3) & ~size_t(3);
@@ -5026,10 +5183,9 @@ static int SetRegularBlock(ddsolve_ctx* ctx, uint32_t cbi, uint32_t n_times,
   cb.run_src.assign(n_run_pad, 0u);
   cb.run_len.assign(n_run_pad, 0u);
   for (uint32_t r = 0; r < n_baselines; ++r) {
-    const uint32_t b = order[r];
-    cb.run_ant[r] = o_a1[b] | (o_a2[b] << 16);
-    cb.run_src[r] = b * n_channels;
-    cb.run_len[r] = n_channels | (o_flip[b] ? kRunFlipped : 0u);
+    cb.run_ant[r] = ctx->order_ant[r];
+    cb.run_src[r] = ctx->order_bl[r] * n_channels;
+    cb.run_len[r] = n_channels | (ctx->order_flip[r] ? kRunFlipped : 0u);
   }
   // Solution index per (direction, time), SolveData.cc:102-105,124-125,167.
   std::vector<uint32_t> nsol(ctx->n_dir), start(ctx->n_dir);
@@ -5217,20 +5373,25 @@ int ddsolve_set_interval_buffers(ddsolve_ctx* ctx, const ddsolve_interval_buffer
   return DDSOLVE_OK;
 }
 
-int ddsolve_correct_and_subtract(ddsolve_ctx* ctx, const ddsolve_interval_buffers* in,
-                                 const double* solutions, float* data_out, float* model_out) {
+int ddsolve_correct_and_subtract(ddsolve_ctx* ctx, const ddsolve_subtract_buffers* in,
+                                 const double* solutions, float* data_out,
+                                 float* const* models_out) {
   if (!ctx) return DDSOLVE_E_INVALID;
   if (!in || !in->antenna1 || !in->antenna2 || !solutions || in->n_times == 0 ||
       in->n_baselines == 0 || in->n_channels < ctx->n_cb)
     return ctx->Fail(DDSOLVE_E_INVALID, "correct and subtract: NULL pointer or empty interval");
-  if (!data_out && !model_out) return DDSOLVE_OK;  // neither subtract nor keepmodel
+  if (!data_out && !models_out) return DDSOLVE_OK;  // neither subtract nor keepmodel
   if (data_out && !in->data)
     return ctx->Fail(DDSOLVE_E_INVALID, "correct and subtract: subtracting needs the data");
-  if (!in->model && (!in->sky || !in->frequencies || !in->station_uvw))
+  if (!in->models && (!in->sky || !in->frequencies || !in->station_uvw))
     return ctx->Fail(DDSOLVE_E_INVALID,
                      "correct and subtract: no model and no sky to predict it");
+  const uint32_t n_dir = ctx->n_dir;
+  for (uint32_t d = 0; d < n_dir; ++d)
+    if ((in->models && !in->models[d]) || (models_out && !models_out[d]))
+      return ctx->Fail(DDSOLVE_E_INVALID, "correct and subtract: NULL model pointer");
   // DDECal.cc:1085-1090
-  if (ctx->n_sub != ctx->n_dir)
+  if (ctx->n_sub != n_dir)
     return ctx->Fail(DDSOLVE_E_UNSUPPORTED,
                      "Model correction is not implemented for DDECal with direction "
                      "dependent solution intervals");
@@ -5240,36 +5401,39 @@ int ddsolve_correct_and_subtract(ddsolve_ctx* ctx, const ddsolve_interval_buffer
   cudaSetDevice(ctx->device);
   const uint32_t n_t = in->n_times, n_bl = in->n_baselines, n_ch = in->n_channels;
   const uint64_t n_vis = uint64_t(n_t) * n_bl * n_ch;
-  const size_t b_data = n_vis * 32, b_m = n_vis * 32 * ctx->n_dir;
-  const size_t b_sol = size_t(ctx->n_cb) * ctx->n_ant * ctx->n_dir * ctx->n_pol * 16;
-  const size_t b_a = size_t(n_bl) * 4;
+  const size_t b_data = n_vis * 32, b_dir = n_vis * 32, b_m = b_dir * n_dir;
+  const size_t b_sol = size_t(ctx->n_cb) * ctx->n_ant * n_dir * ctx->n_pol * 16;
+  const size_t b_a = size_t(n_bl) * 4, b_ptr = size_t(n_dir) * 8;
   auto align = [](size_t x) { return (x + 255) / 256 * 256; };
   const size_t o_sol = data_out ? align(b_data) : 0, o_a1 = o_sol + align(b_sol);
-  const size_t o_a2 = o_a1 + align(b_a);
-  DDS_CHECK_CUDA(ctx, ctx->raw_in.Reserve(o_a2 + align(b_a)));
+  const size_t o_a2 = o_a1 + align(b_a), o_pin = o_a2 + align(b_a), o_pout = o_pin + align(b_ptr);
+  DDS_CHECK_CUDA(ctx, ctx->raw_in.Reserve(o_pout + align(b_ptr)));
   DDS_CHECK_CUDA(ctx, ctx->raw_model.Reserve(b_m));
+  char* base = ctx->raw_in.as<char>();
+  char* staged_m = ctx->raw_model.as<char>();
   int rc;
-  const void *d_data = nullptr, *d_m = nullptr, *d_sol = nullptr;
+  const void *d_data = nullptr, *d_sol = nullptr;
   if (data_out && (rc = DeviceView(ctx, in->data, b_data, ctx->raw_in, 0, &d_data)) != DDSOLVE_OK)
     return rc;
   if ((rc = DeviceView(ctx, solutions, b_sol, ctx->raw_in, o_sol, &d_sol)) != DDSOLVE_OK) return rc;
-  char* base = ctx->raw_in.as<char>();
-  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_a1, in->antenna1, b_a, cudaMemcpyHostToDevice,
-                                      ctx->stream));
-  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_a2, in->antenna2, b_a, cudaMemcpyHostToDevice,
-                                      ctx->stream));
-  if (in->model) {
-    if ((rc = DeviceView(ctx, in->model, b_m, ctx->raw_model, 0, &d_m)) != DDSOLVE_OK) return rc;
+  // Every direction's model: used in place when it is device memory, else
+  // staged (or predicted) into direction d's slice of raw_model.
+  std::vector<const void*> m_in(n_dir);
+  if (in->models) {
+    for (uint32_t d = 0; d < n_dir; ++d)
+      if ((rc = DeviceView(ctx, in->models[d], b_dir, ctx->raw_model, d * b_dir, &m_in[d])) !=
+          DDSOLVE_OK)
+        return rc;
   } else {  // the unweighted 4-correlation model of every baseline and channel
     const PredictJob job{n_t, n_bl, n_ch, in->frequencies, in->station_uvw,
                          in->antenna1, in->antenna2, in->sky};
     if ((rc = CheckPredictJob(ctx, job)) != DDSOLVE_OK) return rc;
     if ((rc = LaunchPredict(ctx, job, ctx->raw_model.as<float2>(), 4)) != DDSOLVE_OK) return rc;
-    d_m = ctx->raw_model.ptr;
+    for (uint32_t d = 0; d < n_dir; ++d) m_in[d] = staged_m + d * b_dir;
   }
   // Outputs in device memory are written in place; host outputs go through
-  // device memory of the context (the staged data and model when they were
-  // staged, else cs_out) and one copy back each.
+  // device memory of the context (the staged data or model slice when that
+  // input was staged, else cs_out) and one copy back each.
   auto on_device = [&](const void* ptr) {
     cudaPointerAttributes a{};
     const bool dev = cudaPointerGetAttributes(&a, ptr) == cudaSuccess &&
@@ -5278,25 +5442,24 @@ int ddsolve_correct_and_subtract(ddsolve_ctx* ctx, const ddsolve_interval_buffer
     return dev;
   };
   const bool data_dev = data_out && on_device(data_out);
-  const bool model_dev = model_out && on_device(model_out);
   float4* k_data = nullptr;
-  float4* k_model = nullptr;
-  size_t cs_bytes = 0;
   if (data_out) {
     if (data_dev)
       k_data = reinterpret_cast<float4*>(data_out);
     else if (d_data == base)
       k_data = reinterpret_cast<float4*>(base);
-    else
-      cs_bytes += align(b_data);
   }
-  if (model_out) {
-    if (model_dev)
-      k_model = reinterpret_cast<float4*>(model_out);
-    else if (d_m == ctx->raw_model.ptr)
-      k_model = ctx->raw_model.as<float4>();
+  std::vector<void*> m_out(models_out ? n_dir : 0, nullptr);
+  std::vector<bool> m_out_dev(m_out.size(), false);
+  size_t cs_bytes = (data_out && !k_data) ? align(b_data) : 0;
+  for (size_t d = 0; d < m_out.size(); ++d) {
+    m_out_dev[d] = on_device(models_out[d]);
+    if (m_out_dev[d])
+      m_out[d] = models_out[d];
+    else if (m_in[d] == staged_m + d * b_dir)
+      m_out[d] = staged_m + d * b_dir;
     else
-      cs_bytes += b_m;
+      cs_bytes += b_dir;
   }
   if (cs_bytes) {
     DDS_CHECK_CUDA(ctx, ctx->cs_out.Reserve(cs_bytes));
@@ -5305,13 +5468,27 @@ int ddsolve_correct_and_subtract(ddsolve_ctx* ctx, const ddsolve_interval_buffer
       k_data = ctx->cs_out.as<float4>();
       o = align(b_data);
     }
-    if (model_out && !k_model) k_model = reinterpret_cast<float4*>(ctx->cs_out.as<char>() + o);
+    for (size_t d = 0; d < m_out.size(); ++d)
+      if (!m_out[d]) {
+        m_out[d] = ctx->cs_out.as<char>() + o;
+        o += b_dir;
+      }
   }
+  // antennas and the per-direction pointer tables: one small copy each
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_a1, in->antenna1, b_a, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_a2, in->antenna2, b_a, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_pin, m_in.data(), b_ptr, cudaMemcpyHostToDevice,
+                                      ctx->stream));
+  if (models_out)
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_pout, m_out.data(), b_ptr,
+                                        cudaMemcpyHostToDevice, ctx->stream));
   CorrectParams p;
   p.data = static_cast<const float4*>(d_data);
-  p.model = static_cast<const float4*>(d_m);
+  p.model = reinterpret_cast<const float4* const*>(base + o_pin);
   p.data_out = k_data;
-  p.model_out = k_model;
+  p.model_out = models_out ? reinterpret_cast<float4* const*>(base + o_pout) : nullptr;
   p.solutions = static_cast<const double2*>(d_sol);
   p.a1 = reinterpret_cast<const uint32_t*>(base + o_a1);
   p.a2 = reinterpret_cast<const uint32_t*>(base + o_a2);
@@ -5320,7 +5497,7 @@ int ddsolve_correct_and_subtract(ddsolve_ctx* ctx, const ddsolve_interval_buffer
   p.n_ch = n_ch;
   p.n_cb = ctx->n_cb;
   p.n_ant = ctx->n_ant;
-  p.n_dir = ctx->n_dir;
+  p.n_dir = n_dir;
   const uint32_t blocks =
       uint32_t(std::min<uint64_t>((n_vis + 255) / 256, uint64_t(ctx->n_sm) * 8));
   if (ctx->n_pol == 4)
@@ -5333,9 +5510,10 @@ int ddsolve_correct_and_subtract(ddsolve_ctx* ctx, const ddsolve_interval_buffer
   if (data_out && !data_dev)
     DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(data_out, k_data, b_data, cudaMemcpyDeviceToHost,
                                         ctx->stream));
-  if (model_out && !model_dev)
-    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(model_out, k_model, b_m, cudaMemcpyDeviceToHost,
-                                        ctx->stream));
+  for (size_t d = 0; d < m_out.size(); ++d)
+    if (!m_out_dev[d])
+      DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(models_out[d], m_out[d], b_dir,
+                                          cudaMemcpyDeviceToHost, ctx->stream));
   DDS_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return DDSOLVE_OK;
 }

@@ -158,6 +158,15 @@ class Smoothness(ctypes.Structure):
                 ("antenna_factors", ctypes.c_void_p), ("dd_factors", ctypes.c_void_p)]
 
 
+class SubtractBuffers(ctypes.Structure):
+    """ddsolve_subtract_buffers (include/ddsolve_b200.h)."""
+    _fields_ = [("n_times", ctypes.c_uint32), ("n_baselines", ctypes.c_uint32),
+                ("n_channels", ctypes.c_uint32), ("antenna1", ctypes.c_void_p),
+                ("antenna2", ctypes.c_void_p), ("data", ctypes.c_void_p),
+                ("models", ctypes.c_void_p), ("frequencies", ctypes.c_void_p),
+                ("station_uvw", ctypes.c_void_p), ("sky", ctypes.c_void_p)]
+
+
 class IntervalBuffers(ctypes.Structure):
     """ddsolve_interval_buffers (include/ddsolve_b200.h)."""
     _fields_ = [("n_times", ctypes.c_uint32), ("n_baselines", ctypes.c_uint32),
@@ -170,25 +179,31 @@ class IntervalBuffers(ctypes.Structure):
 
 
 def _interval_struct(antenna1, antenna2, data, model, frequencies, station_uvw, sky,
-                     n_times=None, n_baselines=None, n_channels=None):
-    """ddsolve_interval_buffers of numpy arrays (weights and flags unset)
+                     subtract=False):
+    """ddsolve_interval_buffers (or with subtract=True ddsolve_subtract_buffers,
+    one model pointer per direction) of numpy arrays, weights and flags unset,
     and the arrays it points into."""
     a1 = np.ascontiguousarray(antenna1, dtype=np.uint32)
     a2 = np.ascontiguousarray(antenna2, dtype=np.uint32)
     keep = [a1, a2]
-    ib = IntervalBuffers()
+    ib = SubtractBuffers() if subtract else IntervalBuffers()
     if data is not None:
         n_times, n_baselines, n_channels, _ = data.shape
         keep.append(data)
         ib.data = data.ctypes.data
-    elif model is not None:
+    else:
         _, n_times, n_baselines, n_channels, _ = np.shape(model)
     ib.n_times, ib.n_baselines, ib.n_channels = n_times, n_baselines, n_channels
     ib.antenna1, ib.antenna2 = a1.ctypes.data, a2.ctypes.data
     if model is not None:
         model = np.ascontiguousarray(model, np.complex64)
         keep.append(model)
-        ib.model = model.ctypes.data
+        if subtract:
+            ptrs = (ctypes.c_void_p * len(model))(*[m.ctypes.data for m in model])
+            keep.append(ptrs)
+            ib.models = ctypes.cast(ptrs, ctypes.c_void_p).value
+        else:
+            ib.model = model.ctypes.data
     elif sky is not None:
         freqs = np.ascontiguousarray(frequencies, np.float64)
         uvw = np.ascontiguousarray(station_uvw, np.float64)
@@ -365,28 +380,30 @@ class Context:
 
     def correct_and_subtract(self, antenna1, antenna2, solutions, data=None, model=None,
                              frequencies=None, station_uvw=None, sky=None,
-                             subtract=True, keep_model=False, n_times=None,
-                             n_baselines=None, n_channels=None):
+                             subtract=True, keep_model=False):
         """ddsolve_correct_and_subtract (DDECal::CorrectAndSubtractModels):
         data complex64 [n_t][n_bl][n_ch][4], model complex64
         [n_dir][n_t][n_bl][n_ch][4] or None with frequencies / station_uvw /
         sky to predict it, solutions complex128 [n_cb][n_ant][n_dir][n_pol].
         Returns (data - sum of corrected models or None, corrected models or
         None) as new arrays."""
-        data = None if data is None else np.ascontiguousarray(data, np.complex64)
+        assert data is not None, "the data give the interval's shape"
+        data = np.ascontiguousarray(data, np.complex64)
         ib, keep = _interval_struct(antenna1, antenna2, data, model, frequencies,
-                                    station_uvw, sky, n_times, n_baselines, n_channels)
+                                    station_uvw, sky, subtract=True)
         sol = np.ascontiguousarray(solutions, np.complex128)
-        d_out = np.empty((ib.n_times, ib.n_baselines, ib.n_channels, 4), np.complex64) \
-            if subtract else None
-        m_out = np.empty((self.n_directions, ib.n_times, ib.n_baselines, ib.n_channels, 4),
-                         np.complex64) if keep_model else None
-        assert not subtract or data is not None, "subtracting needs the data"
         assert sol.size == self.n_channel_blocks * self.n_antennas * self.n_directions * \
             self.n_pol
-        self._check(lib().ddsolve_correct_and_subtract(self._h, ctypes.byref(ib), _addr(sol),
-                                                       _addr(d_out), _addr(m_out)),
-                    "ddsolve_correct_and_subtract")
+        d_out = np.empty(data.shape, np.complex64) if subtract else None
+        m_out = np.empty((self.n_directions,) + data.shape, np.complex64) if keep_model else None
+        m_ptrs = None
+        if m_out is not None:
+            m_ptrs = (ctypes.c_void_p * self.n_directions)(*[m.ctypes.data for m in m_out])
+        self._check(lib().ddsolve_correct_and_subtract(
+            self._h, ctypes.byref(ib), _addr(sol), _addr(d_out),
+            ctypes.cast(m_ptrs, ctypes.c_void_p) if m_ptrs is not None else None),
+            "ddsolve_correct_and_subtract")
+        del keep
         return d_out, m_out
 
     def solve(self, solutions, step_magnitudes=None):

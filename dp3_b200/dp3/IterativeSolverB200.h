@@ -174,6 +174,46 @@ class IterativeSolverB200 final : public SolverBase {
     return SolveWithHostConstraints(solutions, time, stat_stream);
   }
 
+  /// The step after the solve on the GPU, for one time step of an interval:
+  /// DDECal::CorrectAndSubtractModels (steps/DDECal.cc:1081-1125) with
+  /// ApplySolutionAndSubtract (:1031-1079) through
+  /// ddsolve_correct_and_subtract. data: the step's DPBuffer data
+  /// [baseline][channel][4]; models: every direction's model buffer of that
+  /// step (DPBuffer::GetData(direction name)), same shape; antenna1 /
+  /// antenna2: DDECal's antennas per baseline (autocorrelations included).
+  /// With subtract, data -= the sum of the corrected models; with
+  /// keep_model_data, each model buffer is replaced by its corrected model.
+  /// Throws as the reference does for direction-dependent intervals.
+  void CorrectAndSubtract(const std::vector<std::vector<DComplex>>& solutions,
+                          size_t n_baselines, size_t n_channels,
+                          const std::vector<uint32_t>& antenna1,
+                          const std::vector<uint32_t>& antenna2, std::complex<float>* data,
+                          const std::vector<std::complex<float>*>& models, bool subtract,
+                          bool keep_model_data) {
+    if (models.size() != n_solutions_per_direction_.size() ||
+        antenna1.size() != n_baselines || antenna2.size() != n_baselines)
+      throw std::runtime_error("B200 solver: CorrectAndSubtract arguments do not match");
+    EnsureContext();
+    const std::vector<double> flat = Flatten(solutions);
+    std::vector<const float*> in(models.size());
+    std::vector<float*> out(models.size());
+    for (size_t d = 0; d != models.size(); ++d) {
+      in[d] = reinterpret_cast<const float*>(models[d]);
+      out[d] = reinterpret_cast<float*>(models[d]);
+    }
+    ddsolve_subtract_buffers b{};
+    b.n_times = 1;
+    b.n_baselines = uint32_t(n_baselines);
+    b.n_channels = uint32_t(n_channels);
+    b.antenna1 = antenna1.data();
+    b.antenna2 = antenna2.data();
+    b.data = reinterpret_cast<const float*>(data);
+    b.models = in.data();
+    Check(ddsolve_correct_and_subtract(ctx_, &b, flat.data(),
+                                       subtract ? reinterpret_cast<float*>(data) : nullptr,
+                                       keep_model_data ? out.data() : nullptr));
+  }
+
  private:
   static constexpr uint32_t kNCorrelations =
       std::is_same_v<VisMatrix, aocommon::MC2x2F>       ? 4
@@ -187,19 +227,22 @@ class IterativeSolverB200 final : public SolverBase {
       throw std::runtime_error(std::string("B200 solver: ") + ddsolve_last_error(ctx_));
   }
 
+  void EnsureContext() {
+    if (ctx_) return;
+    const ddsolve_dims dims{uint32_t(NAntennas()),
+                            uint32_t(n_solutions_per_direction_.size()),
+                            uint32_t(NChannelBlocks()),
+                            kNCorrelations,
+                            uint32_t(NPol),
+                            n_solutions_per_direction_.data()};
+    Check(ddsolve_create(&dims, device_, &ctx_));
+    DP3B200_ADAPTER_TRACE("context created");
+  }
+
   void Upload(const SolveData<VisMatrix>& data) {
     if (data.NChannelBlocks() != NChannelBlocks())
       throw std::runtime_error("B200 solver: SolveData has another channel-block count");
-    if (!ctx_) {
-      const ddsolve_dims dims{uint32_t(NAntennas()),
-                              uint32_t(n_solutions_per_direction_.size()),
-                              uint32_t(NChannelBlocks()),
-                              kNCorrelations,
-                              uint32_t(NPol),
-                              n_solutions_per_direction_.data()};
-      Check(ddsolve_create(&dims, device_, &ctx_));
-      DP3B200_ADAPTER_TRACE("context created");
-    }
+    EnsureContext();
     std::vector<uint32_t> pairs;
     for (size_t cb = 0; cb != data.NChannelBlocks(); ++cb) {
       const typename SolveData<VisMatrix>::ChannelBlockData& block = data.ChannelBlock(cb);

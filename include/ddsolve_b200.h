@@ -167,8 +167,8 @@ typedef struct {
  * smearing and no beam. Only `data` crosses PCIe (host or device memory);
  * frequencies [n_channels] (Hz) are this block's channels, station_uvw
  * [n_times][n_antennas][3] (m) the station UVW per time step, sky one entry
- * per direction. Limit: 3 n_antennas + 8 (sources of one direction) doubles
- * must fit in 200 KiB (DDSOLVE_E_UNSUPPORTED beyond). */
+ * per direction. Limit: at most 3200 sources in one direction
+ * (DDSOLVE_E_UNSUPPORTED beyond). */
 DDSOLVE_API int ddsolve_set_channel_block_regular_sky(
     ddsolve_ctx* ctx, uint32_t channel_block, uint32_t n_times, uint32_t n_baselines,
     uint32_t n_channels, const float* data, const double* frequencies,
@@ -224,38 +224,55 @@ typedef struct {
 DDSOLVE_API int ddsolve_set_interval_buffers(ddsolve_ctx* ctx,
                                              const ddsolve_interval_buffers* buffers);
 
+/* One interval as DDECal holds it for the step after the solve: data
+ * [n_times][n_baselines][n_channels][XX XY YX YY] and one model buffer per
+ * direction (DPBuffer::GetData(direction name) per time step; one call per
+ * time step passes n_times = 1 and that step's buffers). */
+typedef struct {
+  uint32_t n_times;
+  uint32_t n_baselines;     /* all baselines, autocorrelations included */
+  uint32_t n_channels;      /* channel block cb of the context gets channels
+                               [cb n_ch / n_cb, (cb + 1) n_ch / n_cb) */
+  const uint32_t* antenna1; /* [n_baselines], host memory */
+  const uint32_t* antenna2;
+  const float* data;            /* [n_times][n_baselines][n_channels][4][2] */
+  const float* const* models;   /* [n_directions] host array of pointers, each
+                                   [n_times][n_baselines][n_channels][4][2]; or
+                                   NULL: predicted from `sky` */
+  const double* frequencies;        /* [n_channels] Hz (with sky) */
+  const double* station_uvw;        /* [n_times][n_antennas][3] m (with sky) */
+  const ddsolve_sky_direction* sky; /* [n_directions] (with sky) */
+} ddsolve_subtract_buffers;
+
 /* The step after the solve: applies the solutions to every direction's model
  * and subtracts the corrected models from the data. Replaces
  * DDECal::CorrectAndSubtractModels (steps/DDECal.cc:1081-1125) with
  * ApplySolutionAndSubtract and its ApplyFullJones/Diagonal/ScalarSolution
- * helpers (:1004-1079), for one interval in the buffer layout of
- * ddsolve_interval_buffers. Per visibility (autocorrelations included) and
+ * helpers (:1004-1079). Per visibility (autocorrelations included) and
  * direction the corrected model is G_1 M G_2^H in FP64, as the reference's
- * complex<double> arithmetic. Of `buffers` it reads the interval sizes,
- * antenna1 / antenna2, data (when subtracting) and model, or with model ==
- * NULL predicts the unweighted model of every baseline from sky /
- * frequencies / station_uvw first (as ddsolve_set_interval_buffers); weights,
- * flags and linear_weighting are not used (the reference corrects the
- * unweighted buffers and leaves the flags alone). Channel block cb of the
- * context covers channels [cb n_ch / n_cb, (cb + 1) n_ch / n_cb).
- *   solutions: complex float64 [n_channel_blocks][n_antennas][n_directions]
- *              [n_pol] (DDECal's solutions_ of the interval); the context
- *              must have one solution per direction (otherwise
- *              DDSOLVE_E_UNSUPPORTED, as the reference throws).
- *   data_out:  [n_times][n_baselines][n_channels][4][2]: data - sum over
- *              directions of the corrected models ("subtract"); may equal
- *              buffers->data; NULL = no subtraction.
- *   model_out: [n_directions][n_times][n_baselines][n_channels][4][2]: the
- *              corrected models ("keepmodel"); may equal buffers->model;
- *              NULL = not kept.
- * antenna1 / antenna2 are host memory; every other array may be host or
- * device memory of the context's device. The call returns when the outputs
- * are written. Independent of the context's uploaded visibilities and
- * solutions. */
+ * complex<double> arithmetic (products and sums rounded separately); the sum
+ * over directions is subtracted as float(double(data) - sum). With models ==
+ * NULL the unweighted model of every baseline (autocorrelations zero) is
+ * predicted from sky / frequencies / station_uvw first, as
+ * ddsolve_predict_regular. The reference leaves weights and flags alone, and
+ * so does this call.
+ *   solutions:  complex float64 [n_channel_blocks][n_antennas][n_directions]
+ *               [n_pol] (DDECal's solutions_ of the interval); the context
+ *               must have one solution per direction (otherwise
+ *               DDSOLVE_E_UNSUPPORTED, as the reference throws).
+ *   data_out:   [n_times][n_baselines][n_channels][4][2]: data - the sum over
+ *               directions of the corrected models ("subtract"); may equal
+ *               buffers->data; NULL = no subtraction.
+ *   models_out: [n_directions] host array of pointers, each like a model
+ *               buffer: the corrected models ("keepmodel"); each may equal
+ *               its buffers->models[d]; NULL = not kept.
+ * Data, models, solutions and outputs may be host or device memory of the
+ * context's device. The call returns when the outputs are written. It does
+ * not use the context's uploaded visibilities or solutions. */
 DDSOLVE_API int ddsolve_correct_and_subtract(ddsolve_ctx* ctx,
-                                             const ddsolve_interval_buffers* buffers,
+                                             const ddsolve_subtract_buffers* buffers,
                                              const double* solutions, float* data_out,
-                                             float* model_out);
+                                             float* const* models_out);
 
 /* Full iterate-until-converged solve on the device with no host constraints:
  * replaces IterativeDiagonalSolver<V>::Solve

@@ -149,6 +149,65 @@ int Dispatch(int use_b200, int device, const ref_problem& p, const ref_settings&
 
 extern "C" HARNESS_API const char* adapter_last_error(void) { return g_error.c_str(); }
 
+namespace {
+template <typename V, size_t NPol>
+int CorrectAndSubtract(int device, uint32_t n_ant, uint32_t n_dir, uint32_t n_cb,
+                       uint32_t n_times, uint32_t n_bl, uint32_t n_ch, const uint32_t* a1,
+                       const uint32_t* a2, const double* solutions, float* data,
+                       float* models, int subtract, int keep) {
+  dp3::ddecal::IterativeSolverB200<V, NPol> solver(device);
+  solver.Initialize(n_ant, std::vector<size_t>(n_dir, 1), n_cb);
+  const size_t per_cb = size_t(n_ant) * n_dir * NPol;
+  const auto sol = dp3b200_ref::ToVectors(solutions, n_cb, per_cb);
+  const std::vector<uint32_t> ant1(a1, a1 + n_bl), ant2(a2, a2 + n_bl);
+  const size_t per_step = size_t(n_bl) * n_ch * 4;  // complex values of one time step
+  auto* d = reinterpret_cast<std::complex<float>*>(data);
+  auto* m = reinterpret_cast<std::complex<float>*>(models);
+  for (uint32_t t = 0; t < n_times; ++t) {  // one DPBuffer per time step, as DDECal holds them
+    std::vector<std::complex<float>*> step_models(n_dir);
+    for (uint32_t k = 0; k < n_dir; ++k)
+      step_models[k] = m + (size_t(k) * n_times + t) * per_step;
+    solver.CorrectAndSubtract(sol, n_bl, n_ch, ant1, ant2, d + t * per_step, step_models,
+                              subtract != 0, keep != 0);
+  }
+  return 0;
+}
+}  // namespace
+
+// The adapter's CorrectAndSubtract for n_pol 1, 2 or 4 (4-correlation
+// buffers): data [n_times][n_bl][n_ch][4] and models [n_dir][n_times][n_bl]
+// [n_ch][4] (complex float) are corrected in place, one call per time step.
+extern "C" HARNESS_API int adapter_correct_and_subtract(int n_pol, int device, uint32_t n_ant,
+                                                        uint32_t n_dir, uint32_t n_cb,
+                                                        uint32_t n_times, uint32_t n_bl,
+                                                        uint32_t n_ch, const uint32_t* a1,
+                                                        const uint32_t* a2,
+                                                        const double* solutions, float* data,
+                                                        float* models, int subtract, int keep) {
+  try {
+    switch (n_pol) {
+      case 1:
+        return CorrectAndSubtract<aocommon::MC2x2F, 1>(device, n_ant, n_dir, n_cb, n_times, n_bl,
+                                                       n_ch, a1, a2, solutions, data, models,
+                                                       subtract, keep);
+      case 2:
+        return CorrectAndSubtract<aocommon::MC2x2F, 2>(device, n_ant, n_dir, n_cb, n_times, n_bl,
+                                                       n_ch, a1, a2, solutions, data, models,
+                                                       subtract, keep);
+      case 4:
+        return CorrectAndSubtract<aocommon::MC2x2F, 4>(device, n_ant, n_dir, n_cb, n_times, n_bl,
+                                                       n_ch, a1, a2, solutions, data, models,
+                                                       subtract, keep);
+      default:
+        g_error = "n_pol must be 1, 2 or 4";
+        return 1;
+    }
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return 2;
+  }
+}
+
 // kind: REF_* of ref_problem.h; use_b200: 0 = DP3's own solver, 1 = the B200
 // adapter on CUDA device `device` with DP3's constraint classes (a
 // SmoothnessConstraint keeps the loop on the host), 2 = the adapter with its

@@ -105,7 +105,8 @@ def test_gpu_equals_oracle_bitwise(built, npol, subtract, keep):
 @pytest.mark.parametrize("npol", [2, 4])
 def test_gpu_device_buffers_in_place(built, npol):
     """Device-memory buffers through the C ABI, data and models corrected in
-    place (data_out == data, model_out == model)."""
+    place (data_out == data, models_out == models, one buffer per
+    direction)."""
     import torch
     a1, a2, data, model, sol = _interval(n_st=9, n_t=3, n_ch=12, n_dir=4, n_cb=3, npol=npol,
                                          seed=7)
@@ -113,19 +114,23 @@ def test_gpu_device_buffers_in_place(built, npol):
     ctx = _ctx(9, 4, 3, npol)
     dev = torch.device("cuda", 0)
     d_data = torch.from_numpy(data.view(np.float32).copy()).to(dev)
-    d_model = torch.from_numpy(model.view(np.float32).copy()).to(dev)
+    # one separate device buffer per direction, as DDECal keeps them
+    d_models = [torch.from_numpy(m.view(np.float32).copy()).to(dev) for m in model]
     d_sol = torch.from_numpy(sol.view(np.float64).copy()).to(dev)
-    ib = ddsolve.IntervalBuffers()
+    ptrs = (ctypes.c_void_p * len(d_models))(*[m.data_ptr() for m in d_models])
+    ib = ddsolve.SubtractBuffers()
     ib.n_times, ib.n_baselines, ib.n_channels = data.shape[:3]
     ib.antenna1, ib.antenna2 = a1.ctypes.data, a2.ctypes.data
-    ib.data, ib.model = d_data.data_ptr(), d_model.data_ptr()
+    ib.data, ib.models = d_data.data_ptr(), ctypes.cast(ptrs, ctypes.c_void_p).value
     torch.cuda.synchronize()
     rc = ddsolve.lib().ddsolve_correct_and_subtract(ctx._h, ctypes.byref(ib), d_sol.data_ptr(),
-                                                    d_data.data_ptr(), d_model.data_ptr())
+                                                    d_data.data_ptr(),
+                                                    ctypes.cast(ptrs, ctypes.c_void_p))
     assert rc == 0, ddsolve.lib().ddsolve_last_error(ctx._h)
     ctx.close()
     got_d = d_data.cpu().numpy().view(np.complex64).reshape(data.shape)
-    got_m = d_model.cpu().numpy().view(np.complex64).reshape(model.shape)
+    got_m = np.stack([m.cpu().numpy().view(np.complex64).reshape(model.shape[1:])
+                      for m in d_models])
     np.testing.assert_array_equal(got_d.view(np.uint32), want_d.view(np.uint32))
     np.testing.assert_array_equal(got_m.view(np.uint32), want_m.view(np.uint32))
 

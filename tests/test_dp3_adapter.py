@@ -244,3 +244,46 @@ def test_adapter_stall_matches_dp3(built):
     assert rd.iterations < 3000
     assert rg.iterations == rd.iterations
     assert H.max_rel_diff(b, a) < RTOL
+
+
+def _correct_subtract_child(n_pol, n_ant, n_cb, a1, a2, sol, data, model, subtract, keep):
+    L = lib()
+    L.adapter_correct_and_subtract.restype = ctypes.c_int
+    u32 = ctypes.c_uint32
+    n_dir, n_t, n_bl, n_ch, _ = model.shape
+    data, model = data.copy(), model.copy()
+    rc = L.adapter_correct_and_subtract(
+        ctypes.c_int(n_pol), ctypes.c_int(0), u32(n_ant), u32(n_dir), u32(n_cb), u32(n_t),
+        u32(n_bl), u32(n_ch), ctypes.c_void_p(a1.ctypes.data), ctypes.c_void_p(a2.ctypes.data),
+        ctypes.c_void_p(sol.ctypes.data), ctypes.c_void_p(data.ctypes.data),
+        ctypes.c_void_p(model.ctypes.data), ctypes.c_int(int(subtract)), ctypes.c_int(int(keep)))
+    if rc != 0:
+        raise RuntimeError(L.adapter_last_error().decode())
+    return data, model
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n_pol", [1, 2, 4])
+def test_adapter_correct_and_subtract(built, n_pol):
+    """The adapter's CorrectAndSubtract (DDECal::CorrectAndSubtractModels on
+    the GPU, one call per time step as DDECal holds its buffers) equals the
+    restated step (oracle/subtract_oracle.py) bit for bit, data and kept
+    models."""
+    from oracle import subtract_oracle as so
+    rng = np.random.default_rng(n_pol)
+    n_st, n_t, n_ch, n_dir, n_cb = 7, 3, 10, 3, 3
+    a1, a2 = (x.astype(np.uint32) for x in np.triu_indices(n_st, 0))
+    cz = lambda *s: (rng.standard_normal(s) + 1j * rng.standard_normal(s))  # noqa: E731
+    data = cz(n_t, len(a1), n_ch, 4).astype(np.complex64)
+    model = cz(n_dir, n_t, len(a1), n_ch, 4).astype(np.complex64)
+    sol = np.ascontiguousarray(1.0 + 0.3 * cz(n_cb, n_st, n_dir, n_pol))
+    try:
+        got_d, got_m = _pool().submit(_correct_subtract_child, n_pol, n_st, n_cb, a1, a2, sol,
+                                      data, model, True, True).result()
+    except BrokenProcessPool:
+        global _POOL
+        _POOL = None
+        raise RuntimeError("the adapter's child process crashed (see its stderr)")
+    want_d, want_m = so.correct_and_subtract(data, model, sol, a1, a2, True, True)
+    np.testing.assert_array_equal(got_d.view(np.uint32), want_d.view(np.uint32))
+    np.testing.assert_array_equal(got_m.view(np.uint32), want_m.view(np.uint32))
