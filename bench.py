@@ -597,6 +597,47 @@ def run_correct_subtract(args):
     return 0
 
 
+def run_full_jones(args):
+    """The full-Jones pass (IterativeFullJonesSolver's PerformIteration on
+    the GPU: fj_pass_kernel, or fj_chunk_kernel above four directions, and
+    fj_finalize_kernel) on the layout of configuration `args.config` with
+    four correlations and `args.fj_directions` directions (one solution
+    each), seeded random visibilities and unit gains; mean device time of
+    one pass over `args.kernel_launches` launches (CUDA events on the
+    context's stream, ddsolve_time_stream_kernel) and the algorithmic bytes
+    (32 B per visibility for the data and every direction's model)."""
+    from dp3_b200 import build as native_build
+    from dp3_b200 import ddsolve, synth
+    native_build.build_all()
+    cfg = synth.benchmark_configs()[args.config]
+    n_dir = args.fj_directions
+    rng = np.random.default_rng(0)
+    ctx = ddsolve.Context(cfg.n_stations, [1] * n_dir, cfg.n_channel_blocks, 4, 4)
+    a1, a2 = (np.ascontiguousarray(x, np.uint32) for x in np.triu_indices(cfg.n_stations, 1))
+    n_vis = 0
+    for cb, nc in enumerate(cfg.cb_channels):
+        nv = cfg.n_times * cfg.n_baselines * nc
+        d = rng.standard_normal((nv, 4, 2)).astype(np.float32)
+        m = rng.standard_normal((n_dir, nv, 4, 2)).astype(np.float32)
+        ctx.set_channel_block_regular(cb, cfg.n_times, cfg.n_baselines, nc, d, m, a1, a2)
+        n_vis += nv
+    sol = np.zeros((cfg.n_channel_blocks, cfg.n_stations, n_dir, 4), np.complex128)
+    sol[..., 0] = sol[..., 3] = 1.0
+    ctx.perform_iteration(sol)
+    launches = ctx.last_launch_count()
+    ms = ctx.time_stream_kernel(args.kernel_launches)
+    ctx.close()
+    algo = n_vis * 32 * (1 + n_dir)
+    peak, peak_kind = _peaks()
+    print(json.dumps({"config": cfg.name, "solver": "full-Jones (4 correlations, 2x2 gains)",
+                      "n_directions": n_dir, "n_vis": n_vis, "pass_ms": ms,
+                      "launches_per_pass": launches, "algorithmic_bytes": algo,
+                      "achieved_gbs": algo / (ms / 1e3) / 1e9, "peak_gbs": peak,
+                      "peak_kind": peak_kind, "frac": algo / (ms / 1e3) / 1e9 / peak}),
+          flush=True)
+    return 0
+
+
 def run_fp64_check(args):
     """Solution error of the GPU solver against the FP64 oracle on
     configuration `args.config` (a numerical statement, not a timing): one
@@ -1068,6 +1109,9 @@ def main():
                     help="time only the warm-start network's forward pass (for profiling)")
     ap.add_argument("--predict-only", action="store_true",
                     help="time only the GPU point-source predict of --config (for profiling)")
+    ap.add_argument("--full-jones", action="store_true",
+                    help="time only the full-Jones pass on the layout of --config")
+    ap.add_argument("--fj-directions", type=int, default=4)
     ap.add_argument("--correct-subtract", action="store_true",
                     help="time only the GPU CorrectAndSubtractModels step of --config")
     ap.add_argument("--mlp-only", action="store_true",
@@ -1089,6 +1133,8 @@ def main():
         return run_predict_only(args)
     if args.correct_subtract:
         return run_correct_subtract(args)
+    if args.full_jones:
+        return run_full_jones(args)
     if args.fp64_check:
         return run_fp64_check(args)
     if args.batch > 1:

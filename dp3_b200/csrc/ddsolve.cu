@@ -2797,6 +2797,8 @@ struct FjPassParams {
   uint32_t n_slabs, n_runs, n_ant, n_sub, n_dir;
   uint32_t n_parts;           // each run's rows split into this many parts
   uint32_t d0;                // fj_chunk_kernel: first direction of the launch
+  float2* resid;              // more than kFjMaxDirections: the residual, [slab rows][R][4]
+  const uint64_t* resid_off;  // [n_slabs]: first residual element of each slab
   const LoopState* state;
   int32_t use_handle;
 };
@@ -2829,13 +2831,64 @@ __device__ __forceinline__ void FjStoreSlots(float* out, const C22* P1, const C2
   }
 }
 
-// More than kFjMaxDirections directions: the launch for directions
-// [d0, d0 + NC) recomputes each visibility's residual over all n_dir
-// directions, in direction order with the same FP32 operations as
-// fj_pass_kernel (the gains of the other directions are read per visibility
-// from the solutions, which stay in L1), then accumulates its own NC
-// directions. Each launch reads the data and all models once, so a pass of
-// n_dir directions reads the visibilities ceil(n_dir / kFjMaxDirections) times.
+// More than kFjMaxDirections directions: fj_residual_kernel first stores
+// every visibility's residual R = V - sum_d J_1 M_d J_2^H (in direction
+// order, with the same FP32 operations as fj_pass_kernel) in HBM, taking
+// rows in batches of kFjRowBatch so that each direction's gains are loaded
+// once per batch; then one fj_chunk_kernel launch per group of up to
+// kFjMaxDirections directions reads R and its own directions' models and
+// accumulates them. A pass reads the data and every model once for the
+// residual, then R once per group.
+constexpr int kFjRowBatch = 8;
+
+__global__ void __launch_bounds__(kFjThreads) fj_residual_kernel(const FjPassParams p) {
+  if (SolveStopped(p.state, p.use_handle)) return;
+  const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gt >= p.n_runs * p.n_parts) return;
+  const uint32_t gr = gt % p.n_runs, part = gt / p.n_runs;
+  const uint32_t si = FjSlabOf(p, gr);
+  const SlabDesc sl = p.slabs[si];
+  const uint32_t r = gr - p.run_start[si];
+  const uint32_t ap = sl.run_ant[r];
+  const uint32_t a1 = ap & 0xFFFFu, a2 = ap >> 16;
+  const uint32_t nd = p.n_dir;
+  const double2* sol1 = p.solutions + (size_t(sl.cb) * p.n_ant + a1) * p.n_sub * 4;
+  const double2* sol2 = p.solutions + (size_t(sl.cb) * p.n_ant + a2) * p.n_sub * 4;
+  const float2* vis = static_cast<const float2*>(sl.vis);
+  float2* res = p.resid + p.resid_off[si] * 4;
+  const uint64_t rows = uint64_t(sl.T) * sl.L;
+  const uint64_t row_end = rows * (part + 1) / p.n_parts;
+  for (uint64_t rb = rows * part / p.n_parts; rb < row_end; rb += kFjRowBatch) {
+    const uint64_t nb = row_end - rb < uint64_t(kFjRowBatch) ? row_end - rb : kFjRowBatch;
+    C22 R[kFjRowBatch];
+#pragma unroll
+    for (int i = 0; i < kFjRowBatch; ++i)
+      if (uint64_t(i) < nb) R[i] = LoadC22(vis + SlabElem(sl.R, sl.W, nd + 1, rb + i, 0, r) * 4);
+    for (uint32_t e = 0; e < nd; ++e) {
+      const uint32_t s = p.slab_sol[sl.sol_off + e];
+      const C22 J1 = LoadJones(sol1 + size_t(s) * 4), J2 = LoadJones(sol2 + size_t(s) * 4);
+#pragma unroll
+      for (int i = 0; i < kFjRowBatch; ++i) {
+        if (uint64_t(i) < nb) {
+          const C22 M = LoadC22(vis + SlabElem(sl.R, sl.W, nd + 1, rb + i, 1 + e, r) * 4);
+          const C22 t = MulHerm22(Mul22(J1, M), J2);
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            R[i].m[k] = make_float2(R[i].m[k].x - t.m[k].x, R[i].m[k].y - t.m[k].y);
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < kFjRowBatch; ++i) {
+      if (uint64_t(i) < nb) {
+        float4* o = reinterpret_cast<float4*>(res + ((rb + i) * sl.R + r) * 4);
+        o[0] = make_float4(R[i].m[0].x, R[i].m[0].y, R[i].m[1].x, R[i].m[1].y);
+        o[1] = make_float4(R[i].m[2].x, R[i].m[2].y, R[i].m[3].x, R[i].m[3].y);
+      }
+    }
+  }
+}
+
 template <int NC>
 __global__ void __launch_bounds__(kFjThreads) fj_chunk_kernel(const FjPassParams p) {
   if (SolveStopped(p.state, p.use_handle)) return;
@@ -2861,18 +2914,11 @@ __global__ void __launch_bounds__(kFjThreads) fj_chunk_kernel(const FjPassParams
       P1[d].m[k] = D1[d].m[k] = P2[d].m[k] = D2[d].m[k] = make_float2(0.f, 0.f);
   }
   const float2* vis = static_cast<const float2*>(sl.vis);
+  const float2* res = p.resid + p.resid_off[si] * 4;
   const uint64_t rows = uint64_t(sl.T) * sl.L;
   const uint64_t row_end = rows * (part + 1) / p.n_parts;
   for (uint64_t row = rows * part / p.n_parts; row < row_end; ++row) {
-    C22 R = LoadC22(vis + SlabElem(sl.R, sl.W, nd + 1, row, 0, r) * 4);
-    for (uint32_t e = 0; e < nd; ++e) {
-      const uint32_t s = p.slab_sol[sl.sol_off + e];
-      const C22 M = LoadC22(vis + SlabElem(sl.R, sl.W, nd + 1, row, 1 + e, r) * 4);
-      const C22 t = MulHerm22(Mul22(LoadJones(sol1 + size_t(s) * 4), M),
-                              LoadJones(sol2 + size_t(s) * 4));
-#pragma unroll
-      for (int k = 0; k < 4; ++k) R.m[k] = make_float2(R.m[k].x - t.m[k].x, R.m[k].y - t.m[k].y);
-    }
+    const C22 R = LoadC22(res + (row * sl.R + r) * 4);
 #pragma unroll
     for (int d = 0; d < NC; ++d) {
       const C22 M = LoadC22(vis + SlabElem(sl.R, sl.W, nd + 1, row, 1 + p.d0 + d, r) * 4);
@@ -3344,7 +3390,7 @@ struct ddsolve_ctx {
   DevBuf d_cons, d_ref_ant;  // second next-solutions buffer; reference antennas
   // full-Jones plan: first global run of each slab, per (cb, antenna,
   // sub-solution) item the list of its partial slots
-  DevBuf d_fj_run_start, d_fj_list_off, d_fj_list_ent;
+  DevBuf d_fj_run_start, d_fj_list_off, d_fj_list_ent, d_fj_resid, d_fj_resid_off;
   uint32_t fj_n_slabs = 0, fj_n_runs = 0, fj_blocks = 0, fj_parts = 1;
   // independent solution intervals (ddsolve_set_intervals): interval g owns
   // channel blocks [group_first_cb[g], group_first_cb[g + 1])
@@ -4193,7 +4239,8 @@ int BuildFullJonesPlan(ddsolve_ctx* ctx) {
   uint64_t parts = total_runs ? (want_threads + total_runs - 1) / total_runs : 1;
   parts = std::max<uint64_t>(1, std::min<uint64_t>({parts, max_rows / 16, 16}));
   if (total_runs * parts * n_dir >= (uint64_t(1) << 31)) parts = 1;
-  uint64_t n_runs = 0;
+  uint64_t n_runs = 0, n_resid = 0;
+  std::vector<uint64_t> resid_off;
   for (uint32_t c = 0; c < ctx->n_cb; ++c) {
     ChannelBlockStore& cb = ctx->cbs[c];
     for (const HostSlab& s : cb.slabs) {
@@ -4223,6 +4270,8 @@ int BuildFullJonesPlan(ddsolve_ctx* ctx) {
       }
       n_runs += s.R;
       run_start.push_back(uint32_t(n_runs));
+      resid_off.push_back(n_resid);
+      n_resid += uint64_t(s.T) * s.L * s.R;
     }
   }
   std::vector<uint32_t> off(lists.size() + 1, 0), ent;
@@ -4244,6 +4293,11 @@ int BuildFullJonesPlan(ddsolve_ctx* ctx) {
       (rc = up(ctx->d_fj_list_off, off.data(), off.size() * 4)) != DDSOLVE_OK ||
       (rc = up(ctx->d_fj_list_ent, ent.data(), ent.size() * 4)) != DDSOLVE_OK)
     return rc;
+  if (n_dir > uint32_t(kFjMaxDirections)) {  // the residual between the pass launches
+    if ((rc = up(ctx->d_fj_resid_off, resid_off.data(), resid_off.size() * 8)) != DDSOLVE_OK)
+      return rc;
+    DDS_CHECK_CUDA(ctx, ctx->d_fj_resid.Reserve(std::max<uint64_t>(n_resid, 1) * 32));
+  }
   DDS_CHECK_CUDA(ctx, ctx->d_partials.Reserve(
                           std::max<uint64_t>(n_runs * parts, 1) * n_dir * kFjSlotFloats * 4));
   const uint32_t n_items = ctx->n_cb * n_ant * n_sub;
@@ -4755,12 +4809,12 @@ uint32_t ConstraintLaunches(const ddsolve_ctx* ctx) {
 // (assign_kernel, or finalize_kernel again) finishes the iteration.
 // One full-Jones iteration: MakeSolutionsFinite4Pol, the pass, the
 // finalisation (or, in host mode, the next solutions only).
-// Launches of the full-Jones streaming pass: one, or one per group of
-// kFjMaxDirections directions.
+// Launches of the full-Jones streaming pass: one, or the residual and one
+// per group of kFjMaxDirections directions.
 uint32_t FjPassLaunches(const ddsolve_ctx* ctx) {
   return ctx->n_dir <= uint32_t(kFjMaxDirections)
              ? 1u
-             : (ctx->n_dir + kFjMaxDirections - 1) / kFjMaxDirections;
+             : 1u + (ctx->n_dir + kFjMaxDirections - 1) / kFjMaxDirections;
 }
 
 int LaunchFullJones(ddsolve_ctx* ctx, bool host_mode, bool use_handle, bool with_make_finite) {
@@ -4784,6 +4838,8 @@ int LaunchFullJones(ddsolve_ctx* ctx, bool host_mode, bool use_handle, bool with
   pp.state = ctx->d_state.as<LoopState>();
   pp.use_handle = (use_handle && !host_mode) ? 1 : 0;
   pp.d0 = 0;
+  pp.resid = nullptr;
+  pp.resid_off = nullptr;
   pp.n_parts = ctx->fj_parts;
   const uint32_t blocks = std::max<uint32_t>(
       1, uint32_t((uint64_t(ctx->fj_n_runs) * ctx->fj_parts + kFjThreads - 1) / kFjThreads));
@@ -4793,6 +4849,9 @@ int LaunchFullJones(ddsolve_ctx* ctx, bool host_mode, bool use_handle, bool with
     case 3: fj_pass_kernel<3><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
     case 4: fj_pass_kernel<4><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
     default:
+      pp.resid = ctx->d_fj_resid.as<float2>();
+      pp.resid_off = ctx->d_fj_resid_off.as<uint64_t>();
+      fj_residual_kernel<<<blocks, kFjThreads, 0, ctx->stream>>>(pp);
       for (uint32_t d0 = 0; d0 < ctx->n_dir; d0 += kFjMaxDirections) {
         pp.d0 = d0;
         switch (std::min<uint32_t>(kFjMaxDirections, ctx->n_dir - d0)) {
