@@ -639,6 +639,7 @@ __device__ __forceinline__ double2 zconj(double2 a) { return make_double2(a.x, -
 
 template <int NPOL>
 __global__ void __launch_bounds__(256) correct_subtract_kernel(const CorrectParams p) {
+  constexpr int kGroup = 4;  // directions whose models are loaded before their products
   for (uint64_t v = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; v < p.n_vis;
        v += uint64_t(gridDim.x) * blockDim.x) {
     const uint32_t ch = uint32_t(v % p.n_ch);
@@ -647,13 +648,16 @@ __global__ void __launch_bounds__(256) correct_subtract_kernel(const CorrectPara
     const uint32_t cb = uint32_t((uint64_t(ch + 1) * p.n_cb - 1) / p.n_ch);
     const double2* s1 = p.solutions + (size_t(cb) * p.n_ant + p.a1[bl]) * p.n_dir * NPOL;
     const double2* s2 = p.solutions + (size_t(cb) * p.n_ant + p.a2[bl]) * p.n_dir * NPOL;
+    float4 da = make_float4(0.f, 0.f, 0.f, 0.f), db = da;
+    if (p.data_out) {  // issued first, used last
+      da = __ldcs(p.data + v * 2);
+      db = __ldcs(p.data + v * 2 + 1);
+    }
     double2 sum[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) sum[k] = make_double2(0.0, 0.0);
-#pragma unroll 2
-    for (uint32_t d = 0; d < p.n_dir; ++d) {
-      const float4* md = p.model[d] + v * 2;
-      const float4 ma = __ldcs(md), mb = __ldcs(md + 1);
+    // direction d's corrected model from its loaded visibility (ma, mb)
+    auto apply = [&](uint32_t d, const float4 ma, const float4 mb) {
       const double2 m[4] = {make_double2(ma.x, ma.y), make_double2(ma.z, ma.w),
                             make_double2(mb.x, mb.y), make_double2(mb.z, mb.w)};
       double2 c[4];
@@ -689,9 +693,27 @@ __global__ void __launch_bounds__(256) correct_subtract_kernel(const CorrectPara
         __stcs(mo, make_float4(float(c[0].x), float(c[0].y), float(c[1].x), float(c[1].y)));
         __stcs(mo + 1, make_float4(float(c[2].x), float(c[2].y), float(c[3].x), float(c[3].y)));
       }
+    };
+    // Groups of kGroup directions: every model of the group is loaded before
+    // any product or store (a kept model is written only to its own
+    // direction's buffer, so the loads of the group cannot depend on them).
+    uint32_t d = 0;
+    for (; d + kGroup <= p.n_dir; d += kGroup) {
+      float4 ma[kGroup], mb[kGroup];
+#pragma unroll
+      for (int j = 0; j < kGroup; ++j) {
+        const float4* md = p.model[d + j] + v * 2;
+        ma[j] = __ldcs(md);
+        mb[j] = __ldcs(md + 1);
+      }
+#pragma unroll
+      for (int j = 0; j < kGroup; ++j) apply(d + j, ma[j], mb[j]);
+    }
+    for (; d < p.n_dir; ++d) {
+      const float4* md = p.model[d] + v * 2;
+      apply(d, __ldcs(md), __ldcs(md + 1));
     }
     if (p.data_out) {
-      const float4 da = __ldcs(p.data + v * 2), db = __ldcs(p.data + v * 2 + 1);
       __stcs(p.data_out + v * 2,
              make_float4(float(__dsub_rn(da.x, sum[0].x)), float(__dsub_rn(da.y, sum[0].y)),
                          float(__dsub_rn(da.z, sum[1].x)), float(__dsub_rn(da.w, sum[1].y))));
@@ -2816,17 +2838,41 @@ __device__ __forceinline__ uint32_t FjSlabOf(const FjPassParams& p, uint32_t gr)
   return lo;
 }
 
+// A Gram matrix sum X^H X, Hermitian: its real diagonal and the upper
+// element. The products and sums of these three elements are those of
+// AddHermMul22; the lower element is the conjugate of the upper one (as the
+// host's non-fused complex arithmetic gives it) and the diagonal is real.
+struct H22 {
+  float d00, d11;
+  float2 d01;
+};
+__device__ __forceinline__ void ZeroH22(H22& h) {
+  h.d00 = h.d11 = 0.f;
+  h.d01 = make_float2(0.f, 0.f);
+}
+// acc += x^H x
+__device__ __forceinline__ void AddGram22(H22& acc, const C22& x) {
+  acc.d00 = fmaf(x.m[2].x, x.m[2].x,
+                 fmaf(x.m[2].y, x.m[2].y, fmaf(x.m[0].x, x.m[0].x, fmaf(x.m[0].y, x.m[0].y, acc.d00))));
+  acc.d11 = fmaf(x.m[3].x, x.m[3].x,
+                 fmaf(x.m[3].y, x.m[3].y, fmaf(x.m[1].x, x.m[1].x, fmaf(x.m[1].y, x.m[1].y, acc.d11))));
+  acc.d01 = cconj_fma(x.m[2], x.m[3], cconj_fma(x.m[0], x.m[1], acc.d01));
+}
+
 template <int N>
-__device__ __forceinline__ void FjStoreSlots(float* out, const C22* P1, const C22* D1,
-                                             const C22* P2, const C22* D2) {
+__device__ __forceinline__ void FjStoreSlots(float* out, const C22* P1, const H22* D1,
+                                             const C22* P2, const H22* D2) {
 #pragma unroll
   for (int d = 0; d < N; ++d) {
-    const C22* parts[4] = {&P1[d], &D1[d], &P2[d], &D2[d]};
+    const C22* ps[2] = {&P1[d], &P2[d]};
+    const H22* ds[2] = {&D1[d], &D2[d]};
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      float4* o = reinterpret_cast<float4*>(out + d * kFjSlotFloats + q * 8);
-      o[0] = make_float4(parts[q]->m[0].x, parts[q]->m[0].y, parts[q]->m[1].x, parts[q]->m[1].y);
-      o[1] = make_float4(parts[q]->m[2].x, parts[q]->m[2].y, parts[q]->m[3].x, parts[q]->m[3].y);
+    for (int q = 0; q < 2; ++q) {
+      float4* o = reinterpret_cast<float4*>(out + d * kFjSlotFloats + q * 16);
+      o[0] = make_float4(ps[q]->m[0].x, ps[q]->m[0].y, ps[q]->m[1].x, ps[q]->m[1].y);
+      o[1] = make_float4(ps[q]->m[2].x, ps[q]->m[2].y, ps[q]->m[3].x, ps[q]->m[3].y);
+      o[2] = make_float4(ds[q]->d00, 0.f, ds[q]->d01.x, ds[q]->d01.y);
+      o[3] = make_float4(ds[q]->d01.x, -ds[q]->d01.y, ds[q]->d11, 0.f);
     }
   }
 }
@@ -2903,7 +2949,8 @@ __global__ void __launch_bounds__(kFjThreads) fj_chunk_kernel(const FjPassParams
   const uint32_t nd = p.n_dir;
   const double2* sol1 = p.solutions + (size_t(sl.cb) * p.n_ant + a1) * p.n_sub * 4;
   const double2* sol2 = p.solutions + (size_t(sl.cb) * p.n_ant + a2) * p.n_sub * 4;
-  C22 J1[NC], J2[NC], P1[NC], D1[NC], P2[NC], D2[NC];
+  C22 J1[NC], J2[NC], P1[NC], P2[NC];
+  H22 D1[NC], D2[NC];
 #pragma unroll
   for (int d = 0; d < NC; ++d) {
     const uint32_t s = p.slab_sol[sl.sol_off + p.d0 + d];
@@ -2911,7 +2958,9 @@ __global__ void __launch_bounds__(kFjThreads) fj_chunk_kernel(const FjPassParams
     J2[d] = LoadJones(sol2 + size_t(s) * 4);
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-      P1[d].m[k] = D1[d].m[k] = P2[d].m[k] = D2[d].m[k] = make_float2(0.f, 0.f);
+      P1[d].m[k] = P2[d].m[k] = make_float2(0.f, 0.f);
+    ZeroH22(D1[d]);
+    ZeroH22(D2[d]);
   }
   const float2* vis = static_cast<const float2*>(sl.vis);
   const float2* res = p.resid + p.resid_off[si] * 4;
@@ -2925,9 +2974,9 @@ __global__ void __launch_bounds__(kFjThreads) fj_chunk_kernel(const FjPassParams
       const C22 Y = Mul22(J1[d], M);
       const C22 X = MulHerm22(J2[d], M);
       AddMul22(P1[d], R, X);
-      AddHermMul22(D1[d], X, X);
+      AddGram22(D1[d], X);
       AddHermMul22(P2[d], R, Y);
-      AddHermMul22(D2[d], Y, Y);
+      AddGram22(D2[d], Y);
     }
   }
   FjStoreSlots<NC>(p.partials + (size_t(gt) * nd + p.d0) * kFjSlotFloats, P1, D1, P2, D2);
@@ -2945,7 +2994,8 @@ __global__ void __launch_bounds__(kFjThreads) fj_pass_kernel(const FjPassParams 
   const uint32_t ap = sl.run_ant[r];
   const uint32_t a1 = ap & 0xFFFFu, a2 = ap >> 16;
   const size_t cb_off = size_t(sl.cb) * p.n_ant * p.n_sub;
-  C22 J1[ND], J2[ND], P1[ND], D1[ND], P2[ND], D2[ND];
+  C22 J1[ND], J2[ND], P1[ND], P2[ND];
+  H22 D1[ND], D2[ND];
 #pragma unroll
   for (int d = 0; d < ND; ++d) {
     const uint32_t s = p.slab_sol[sl.sol_off + d];
@@ -2953,7 +3003,9 @@ __global__ void __launch_bounds__(kFjThreads) fj_pass_kernel(const FjPassParams 
     J2[d] = LoadJones(p.solutions + (cb_off + size_t(a2) * p.n_sub + s) * 4);
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-      P1[d].m[k] = D1[d].m[k] = P2[d].m[k] = D2[d].m[k] = make_float2(0.f, 0.f);
+      P1[d].m[k] = P2[d].m[k] = make_float2(0.f, 0.f);
+    ZeroH22(D1[d]);
+    ZeroH22(D2[d]);
   }
   const float2* vis = static_cast<const float2*>(sl.vis);
   const uint64_t rows = uint64_t(sl.T) * sl.L;
@@ -2975,9 +3027,9 @@ __global__ void __launch_bounds__(kFjThreads) fj_pass_kernel(const FjPassParams 
     for (int d = 0; d < ND; ++d) {
       const C22 X = MulHerm22(J2[d], M[d]);  // J_2 M^H
       AddMul22(P1[d], R, X);
-      AddHermMul22(D1[d], X, X);
+      AddGram22(D1[d], X);
       AddHermMul22(P2[d], R, Y[d]);
-      AddHermMul22(D2[d], Y[d], Y[d]);
+      AddGram22(D2[d], Y[d]);
     }
   }
   FjStoreSlots<ND>(p.partials + size_t(gt) * ND * kFjSlotFloats, P1, D1, P2, D2);
