@@ -615,11 +615,13 @@ def run_full_jones(args):
     ctx = ddsolve.Context(cfg.n_stations, [1] * n_dir, cfg.n_channel_blocks, 4, 4)
     a1, a2 = (np.ascontiguousarray(x, np.uint32) for x in np.triu_indices(cfg.n_stations, 1))
     n_vis = 0
+    data, model = [], []
     for cb, nc in enumerate(cfg.cb_channels):
         nv = cfg.n_times * cfg.n_baselines * nc
-        d = rng.standard_normal((nv, 4, 2)).astype(np.float32)
-        m = rng.standard_normal((n_dir, nv, 4, 2)).astype(np.float32)
-        ctx.set_channel_block_regular(cb, cfg.n_times, cfg.n_baselines, nc, d, m, a1, a2)
+        data.append(rng.standard_normal((nv, 4, 2)).astype(np.float32))
+        model.append(rng.standard_normal((n_dir, nv, 4, 2)).astype(np.float32))
+        ctx.set_channel_block_regular(cb, cfg.n_times, cfg.n_baselines, nc, data[-1], model[-1],
+                                      a1, a2)
         n_vis += nv
     sol = np.zeros((cfg.n_channel_blocks, cfg.n_stations, n_dir, 4), np.complex128)
     sol[..., 0] = sol[..., 3] = 1.0
@@ -629,12 +631,34 @@ def run_full_jones(args):
     ctx.close()
     algo = n_vis * 32 * (1 + n_dir)
     peak, peak_kind = _peaks()
-    print(json.dumps({"config": cfg.name, "solver": "full-Jones (4 correlations, 2x2 gains)",
-                      "n_directions": n_dir, "n_vis": n_vis, "pass_ms": ms,
-                      "launches_per_pass": launches, "algorithmic_bytes": algo,
-                      "achieved_gbs": algo / (ms / 1e3) / 1e9, "peak_gbs": peak,
-                      "peak_kind": peak_kind, "frac": algo / (ms / 1e3) / 1e9 / peak}),
-          flush=True)
+    out = {"config": cfg.name, "solver": "full-Jones (4 correlations, 2x2 gains)",
+           "n_directions": n_dir, "n_vis": n_vis, "pass_ms": ms,
+           "launches_per_pass": launches, "algorithmic_bytes": algo,
+           "achieved_gbs": algo / (ms / 1e3) / 1e9, "peak_gbs": peak,
+           "peak_kind": peak_kind, "frac": algo / (ms / 1e3) / 1e9 / peak}
+    if not args.no_cpu_baseline:
+        # the reference's own IterativeFullJonesSolver (oracle/_ref) on the
+        # same interval with all host threads: seconds per iteration from a
+        # 3-iteration solve, SolveData packing excluded
+        try:
+            from types import SimpleNamespace
+            from oracle import ref_ffi as rf
+            rcfg = SimpleNamespace(n_stations=cfg.n_stations, n_times=cfg.n_times,
+                                   n_baselines=cfg.n_baselines, cb_channels=cfg.cb_channels,
+                                   nspd=[1] * n_dir)
+            prep = rf.Prepared(rcfg, a1, a2, data, model, 4, 4)
+            threads = os.cpu_count() or 1
+            st = rf.settings(max_iterations=3, accuracy=1e-12, step_size=0.2)
+            s0 = sol.copy()
+            sec = prep.solve(s0, st, threads).seconds_solve
+            prep.close()
+            out["cpu_baseline"] = {"value": sec / 3 * 1e3, "unit": "ms per iteration",
+                                   "cores": threads, "kind": "reference",
+                                   "sample": "DP3's IterativeFullJonesSolver (reference sources "
+                                             "compiled here), 3 iterations of the same interval"}
+        except Exception as e:  # the reference oracle is test infrastructure
+            out["cpu_baseline"] = {"unavailable": str(e)[:200]}
+    print(json.dumps(out), flush=True)
     return 0
 
 
