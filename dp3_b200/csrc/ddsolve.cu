@@ -274,7 +274,8 @@ __global__ void pack_kernel(const PackSlab s, const uint32_t* __restrict__ run_s
                             const uint32_t* __restrict__ run_len,
                             const float2* __restrict__ src_data,
                             const float2* __restrict__ src_model, uint64_t n_vis,
-                            uint32_t n_dir, float2* __restrict__ dst_vis) {
+                            uint32_t n_dir, uint32_t n_models_copied,
+                            float2* __restrict__ dst_vis) {
   const uint64_t tlr = uint64_t(s.T) * s.L * s.R;
   for (uint64_t e = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; e < tlr;
        e += uint64_t(gridDim.x) * blockDim.x) {
@@ -289,7 +290,7 @@ __global__ void pack_kernel(const PackSlab s, const uint32_t* __restrict__ run_s
     float2* dst = dst_vis + (uint64_t(1 + n_dir) * s.dst_elem_off) * NCORR;
     CopyVis<NCORR>(src_data + v * NCORR,
                    dst + SlabElem(s.R, s.W, 1 + n_dir, tl, 0, r) * NCORR, valid, flip);
-    for (uint32_t d = 0; d < n_dir; ++d)
+    for (uint32_t d = 0; d < n_models_copied; ++d)
       CopyVis<NCORR>(src_model + (d * n_vis + v) * NCORR,
                      dst + SlabElem(s.R, s.W, 1 + n_dir, tl, 1 + d, r) * NCORR, valid, flip);
   }
@@ -333,6 +334,16 @@ struct PredictParams {
   float2* model;            // [n_dir][n_times * n_bl * L][NCORR]
   uint32_t n_times, n_bl, L, n_ant, n_dir, max_src, n_slots;
   int uniform;              // channels evenly spaced: chunk starts + step in the table
+  // Packed mode (run_ant non-null): thread bl is run bl of a packed channel
+  // block, between the run's oriented antennas (a flipped baseline's model
+  // is then the conjugate transpose its packing stores), written straight
+  // into the packed layout: element t_elem[t] + SlabElem(n_bl, W, n_dir + 1,
+  // t_row[t] + channel, 1 + d, bl) of vis.
+  const uint32_t* run_ant;
+  float2* vis;
+  const uint64_t* t_elem;   // [n_times]
+  const uint32_t* t_row;    // [n_times]
+  uint32_t W;
 };
 
 struct PhasorParams {
@@ -448,12 +459,34 @@ __global__ void __launch_bounds__(kPredictThreads) predict_kernel(const PredictP
   __syncthreads();
   const uint32_t bl = blockIdx.x * blockDim.x + threadIdx.x;
   if (bl >= p.n_bl) return;
-  const uint32_t ap = p.a1[bl], aq = p.a2[bl];
-  const uint64_t n_vis = uint64_t(p.n_times) * p.n_bl * p.L;
-  const uint64_t v0 = (uint64_t(t) * p.n_bl + bl) * p.L;
-  float2* out = p.model + (uint64_t(d) * n_vis + v0) * NCORR;
+  const bool packed = p.run_ant != nullptr;
+  uint32_t ap, aq;
+  if (packed) {
+    const uint32_t x = p.run_ant[bl];
+    ap = x & 0xFFFFu;
+    aq = x >> 16;
+  } else {
+    ap = p.a1[bl];
+    aq = p.a2[bl];
+  }
+  // channel c's model at out + c * cstride (packed: one slab row per channel)
+  float2* out;
+  uint64_t cstride;
+  if (packed) {
+    const uint64_t row_elems = uint64_t(p.n_bl) * (p.n_dir + 1);
+    out = p.vis + (p.t_elem[t] + SlabElem(p.n_bl, p.W, p.n_dir + 1, p.t_row[t], 1 + d, bl)) *
+                      NCORR;
+    cstride = row_elems * NCORR;
+  } else {
+    const uint64_t n_vis = uint64_t(p.n_times) * p.n_bl * p.L;
+    const uint64_t v0 = (uint64_t(t) * p.n_bl + bl) * p.L;
+    out = p.model + (uint64_t(d) * n_vis + v0) * NCORR;
+    cstride = NCORR;
+  }
+  auto at = [&](uint32_t c) -> float2* { return out + c * cstride; };
   if (ap == aq) {  // autocorrelations stay zero (Simulator.cc:162-163)
-    for (uint32_t i = 0; i < p.L * NCORR; ++i) out[i] = make_float2(0.f, 0.f);
+    for (uint32_t c = 0; c < p.L; ++c)
+      for (int k = 0; k < NCORR; ++k) at(c)[k] = make_float2(0.f, 0.f);
     return;
   }
   // this (time, direction)'s table: [source][station][slot]
@@ -501,11 +534,11 @@ __global__ void __launch_bounds__(kPredictThreads) predict_kernel(const PredictP
     }
 #pragma unroll
     for (int c = 0; c < CH; ++c)
-      if (c < int(nc))
+      if (c < int(nc)) {
+        float2* o = at(c0 + c);
 #pragma unroll
-        for (int k = 0; k < NCORR; ++k)
-          out[uint64_t(c0 + c) * NCORR + k] =
-              make_float2(float(acc[c][k].x), float(acc[c][k].y));
+        for (int k = 0; k < NCORR; ++k) o[k] = make_float2(float(acc[c][k].x), float(acc[c][k].y));
+      }
   }
 }
 
@@ -3395,6 +3428,20 @@ struct ddsolve_ctx {
   void* predict_host = nullptr;
   size_t predict_host_bytes = 0;
   cudaEvent_t predict_copied = nullptr;
+  // Pinned image of the small inputs of a synchronous call
+  // (ddsolve_correct_and_subtract), free again when the call returns.
+  void* small_host = nullptr;
+  size_t small_host_bytes = 0;
+  // Per channel block, for the sky path (ddsolve_set_channel_block_regular_sky),
+  // whose uploads overlap a solve of another context: the predict's device
+  // inputs and their pinned image (consecutive blocks do not wait for each
+  // other's copies), and the data's staging buffer, filled on copy_stream so
+  // that the copies run while the kernels of the upload wait for the solve.
+  cudaStream_t copy_stream = nullptr;
+  std::vector<DevBuf> blk_predict_in, blk_data_stage;
+  std::vector<void*> blk_predict_host;
+  std::vector<size_t> blk_predict_host_bytes;
+  std::vector<cudaEvent_t> blk_predict_copied, blk_data_copied, blk_packed;
   DevBuf raw_in;      // DP3-layout interval buffers (ddsolve_set_interval_buffers)
   DevBuf raw_model;   // the 4-correlation predicted model of one block
   DevBuf cs_out;      // outputs of ddsolve_correct_and_subtract bound for the host
@@ -3480,6 +3527,44 @@ struct ddsolve_ctx {
     if (h_stage) cudaFreeHost(h_stage);
     if (predict_copied) cudaEventDestroy(predict_copied);
     if (predict_host) cudaFreeHost(predict_host);
+    if (small_host) cudaFreeHost(small_host);
+    for (void* h : blk_predict_host)
+      if (h) cudaFreeHost(h);
+    for (auto* evs : {&blk_predict_copied, &blk_data_copied, &blk_packed})
+      for (cudaEvent_t ev : *evs)
+        if (ev) cudaEventDestroy(ev);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+  }
+  // A pinned image of at least n bytes that is free to overwrite: the copy
+  // recorded in `ev` (created on first use) has run.
+  static cudaError_t ReservePinned(void*& buf, size_t& bytes, cudaEvent_t& ev, size_t n) {
+    if (ev) {
+      const cudaError_t e = cudaEventSynchronize(ev);
+      if (e != cudaSuccess) return e;
+    } else {
+      const cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+      if (e != cudaSuccess) return e;
+    }
+    if (buf && n <= bytes) return cudaSuccess;
+    if (buf) cudaFreeHost(buf);
+    buf = nullptr;
+    bytes = 0;
+    const cudaError_t e = cudaMallocHost(&buf, std::max<size_t>(n, 1 << 16));
+    if (e == cudaSuccess) bytes = std::max<size_t>(n, 1 << 16);
+    return e;
+  }
+  static cudaError_t EnsureEvent(cudaEvent_t& ev) {
+    return ev ? cudaSuccess : cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+  }
+  // The pinned image of small inputs, at least n bytes.
+  cudaError_t ReserveSmallHost(size_t n) {
+    if (small_host && n <= small_host_bytes) return cudaSuccess;
+    if (small_host) cudaFreeHost(small_host);
+    small_host = nullptr;
+    small_host_bytes = 0;
+    const cudaError_t e = cudaMallocHost(&small_host, std::max<size_t>(n, 1 << 16));
+    if (e == cudaSuccess) small_host_bytes = std::max<size_t>(n, 1 << 16);
+    return e;
   }
   // The pinned predict image, at least n bytes, free to overwrite.
   cudaError_t ReservePredictHost(size_t n) {
@@ -3722,10 +3807,23 @@ int CheckPredictJob(ddsolve_ctx* ctx, const PredictJob& j) {
   return DDSOLVE_OK;
 }
 
+// A packed channel block the predict writes into directly (predict_kernel's
+// packed mode): its runs' oriented antennas on the device, its packed
+// visibilities, and per time step the slab element and row of the step.
+struct PackedTarget {
+  const uint32_t* run_ant;
+  float2* vis;
+  std::vector<uint64_t> t_elem;
+  std::vector<uint32_t> t_row;
+  uint32_t W;
+};
+
 // Uploads the job's inputs and launches predict_kernel into `model` (device
-// memory, [n_dir][n_times * n_bl * L][n_corr]) on the context stream; n_corr
-// is the context's unless n_corr_out (1, 2 or 4) is given.
-int LaunchPredict(ddsolve_ctx* ctx, const PredictJob& j, float2* model, uint32_t n_corr_out = 0) {
+// memory, [n_dir][n_times * n_bl * L][n_corr]) on the context stream, or
+// into the packed block `packed`; n_corr is the context's unless n_corr_out
+// (1, 2 or 4) is given.
+int LaunchPredict(ddsolve_ctx* ctx, const PredictJob& j, float2* model, uint32_t n_corr_out = 0,
+                  const PackedTarget* packed = nullptr, int blk = -1) {
   const uint32_t nc = n_corr_out ? n_corr_out : ctx->n_corr;
   uint32_t n_src = 0, max_src = 0;
   std::vector<uint32_t> off(ctx->n_dir + 1, 0);
@@ -3753,9 +3851,15 @@ int LaunchPredict(ddsolve_ctx* ctx, const PredictJob& j, float2* model, uint32_t
   const size_t b_uvw = size_t(j.n_times) * ctx->n_ant * 3 * 8, b_src = src.size() * 8 + 8;
   const size_t b_off = off.size() * 4, b_f = size_t(j.L) * 8, b_a = size_t(j.n_bl) * 4;
   const size_t o_src = align(b_uvw), o_off = o_src + align(b_src), o_f = o_off + align(b_off);
-  const size_t o_a1 = o_f + align(b_f), o_a2 = o_a1 + align(b_a), total = o_a2 + align(b_a);
-  DDS_CHECK_CUDA(ctx, ctx->predict_in.Reserve(total));
-  char* base = ctx->predict_in.as<char>();
+  const size_t b_te = packed ? size_t(j.n_times) * 8 : 0, b_tr = packed ? size_t(j.n_times) * 4 : 0;
+  const size_t o_a1 = o_f + align(b_f), o_a2 = o_a1 + align(b_a), o_te = o_a2 + align(b_a);
+  const size_t o_tr = o_te + align(b_te), total = o_tr + align(b_tr);
+  // the device inputs and their pinned image: the context's, or channel
+  // block blk's own (blocks then do not wait for each other's copies)
+  DevBuf& pin = blk >= 0 ? ctx->blk_predict_in[blk] : ctx->predict_in;
+  cudaEvent_t& copied = blk >= 0 ? ctx->blk_predict_copied[blk] : ctx->predict_copied;
+  DDS_CHECK_CUDA(ctx, pin.Reserve(total));
+  char* base = pin.as<char>();
   // Host inputs go through one pinned image and one copy (each small copy
   // from pageable memory costs a staged transfer of its own); inputs in
   // device memory are copied device to device.
@@ -3767,24 +3871,33 @@ int LaunchPredict(ddsolve_ctx* ctx, const PredictJob& j, float2* model, uint32_t
     }
     return a.type == cudaMemoryTypeUnregistered || a.type == cudaMemoryTypeHost;
   };
-  DDS_CHECK_CUDA(ctx, ctx->ReservePredictHost(total));
-  char* host = static_cast<char*>(ctx->predict_host);
+  if (blk >= 0)
+    DDS_CHECK_CUDA(ctx, ddsolve_ctx::ReservePinned(ctx->blk_predict_host[blk],
+                                                   ctx->blk_predict_host_bytes[blk], copied,
+                                                   total));
+  else
+    DDS_CHECK_CUDA(ctx, ctx->ReservePredictHost(total));
+  char* host = static_cast<char*>(blk >= 0 ? ctx->blk_predict_host[blk] : ctx->predict_host);
   struct Piece {
     const void* src;
     size_t off, bytes;
   };
-  const Piece pieces[6] = {{j.uvw, 0, b_uvw},           {src.data(), o_src, src.size() * 8},
-                           {off.data(), o_off, b_off},  {j.freq, o_f, b_f},
-                           {j.a1, o_a1, b_a},           {j.a2, o_a2, b_a}};
-  bool device_piece[6];
-  for (int k = 0; k < 6; ++k) {
+  constexpr int kPieces = 8;
+  const Piece pieces[kPieces] = {
+      {j.uvw, 0, b_uvw},          {src.data(), o_src, src.size() * 8},
+      {off.data(), o_off, b_off}, {j.freq, o_f, b_f},
+      {j.a1, o_a1, b_a},          {j.a2, o_a2, b_a},
+      {packed ? static_cast<const void*>(packed->t_elem.data()) : nullptr, o_te, b_te},
+      {packed ? static_cast<const void*>(packed->t_row.data()) : nullptr, o_tr, b_tr}};
+  bool device_piece[kPieces];
+  for (int k = 0; k < kPieces; ++k) {
     const Piece& pc = pieces[k];
     device_piece[k] = pc.bytes > 0 && !on_host(pc.src);
     if (pc.bytes > 0 && !device_piece[k]) std::memcpy(host + pc.off, pc.src, pc.bytes);
   }
   DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base, host, total, cudaMemcpyHostToDevice, ctx->stream));
-  DDS_CHECK_CUDA(ctx, cudaEventRecord(ctx->predict_copied, ctx->stream));
-  for (int k = 0; k < 6; ++k)  // after the image, which they overwrite
+  DDS_CHECK_CUDA(ctx, cudaEventRecord(copied, ctx->stream));
+  for (int k = 0; k < kPieces; ++k)  // after the image, which they overwrite
     if (device_piece[k])
       DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + pieces[k].off, pieces[k].src, pieces[k].bytes,
                                           cudaMemcpyDeviceToDevice, ctx->stream));
@@ -3830,6 +3943,11 @@ int LaunchPredict(ddsolve_ctx* ctx, const PredictJob& j, float2* model, uint32_t
   p.max_src = max_src;
   p.n_slots = n_slots;
   p.uniform = uniform;
+  p.run_ant = packed ? packed->run_ant : nullptr;
+  p.vis = packed ? packed->vis : nullptr;
+  p.t_elem = reinterpret_cast<const uint64_t*>(base + o_te);
+  p.t_row = reinterpret_cast<const uint32_t*>(base + o_tr);
+  p.W = packed ? packed->W : 0;
   const size_t smem = size_t(max_src) * 8 * sizeof(double);
   const dim3 grid((j.n_bl + kPredictThreads - 1) / kPredictThreads, j.n_times, ctx->n_dir);
   const void* fn = nc == 1   ? reinterpret_cast<const void*>(predict_kernel<1>)
@@ -3852,10 +3970,11 @@ using StageFn = std::function<int(char* staging)>;
 // block into the staging buffer: copies of host or device arrays
 // (StageCopy), a copy of the data plus the GPU predict of the model, or the
 // GPU weighting of raw buffers.
-int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const StageFn& stage) {
+int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const StageFn& stage,
+                  bool models_in_place = false, int blk = -1) {
   const size_t E = ctx->elem_bytes;
   const size_t src_bytes = size_t(cb.n_vis) * E * (1 + ctx->n_dir);
-  DDS_CHECK_CUDA(ctx, ctx->staging.Reserve(src_bytes));
+  if (blk < 0) DDS_CHECK_CUDA(ctx, ctx->staging.Reserve(src_bytes));  // else the block's own
   cb.vis.realloc_flag = cb.run_ant_dev.realloc_flag = false;
   DDS_CHECK_CUDA(ctx, cb.vis.Reserve(cb.n_elems * E * (1 + ctx->n_dir)));
   DDS_CHECK_CUDA(ctx, cb.run_ant_dev.Reserve(cb.run_ant.size() * 4));
@@ -3868,19 +3987,20 @@ int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const StageFn& stage)
     ps[i] = PackSlab{s.elem_off, s.src_base, s.tstride, s.T, s.L, s.R, s.run_off, s.W};
   }
   char* st = ctx->staging.as<char>();
-  if (cb.n_vis) {
-    const int rc = stage(st);
-    if (rc != DDSOLVE_OK) return rc;
-  }
   // The run arrays are copied only when they changed: a copy from pageable
   // memory waits for the stream, which would hold this host thread behind
   // the kernels already queued (the previous block's predict and pack, or a
   // solve of the other context). Consecutive blocks and intervals of one
-  // layout repeat them.
+  // layout repeat them. The run antennas go first: a stage that writes the
+  // packed block directly reads them.
   if (cb.run_ant_dev.realloc_flag || !cb.set || cb.run_ant != cb.prev_run_ant)
     DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(cb.run_ant_dev.ptr, cb.run_ant.data(),
                                         cb.run_ant.size() * 4,
                                         cudaMemcpyHostToDevice, ctx->stream));
+  if (cb.n_vis) {
+    const int rc = stage(st);
+    if (rc != DDSOLVE_OK) return rc;
+  }
   if (ctx->run_src_dev.realloc_flag || ctx->run_len_dev.realloc_flag ||
       cb.run_src != ctx->staged_run_src || cb.run_len != ctx->staged_run_len) {
     DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ctx->run_src_dev.ptr, cb.run_src.data(),
@@ -3898,22 +4018,31 @@ int UploadAndPack(ddsolve_ctx* ctx, ChannelBlockStore& cb, const StageFn& stage)
     if (tlr == 0) continue;
     const uint32_t blocks =
         uint32_t(std::min<uint64_t>((tlr + 255) / 256, uint64_t(ctx->n_sm) * 8));
-    const float2* src_d = reinterpret_cast<const float2*>(st);
+    // the sky path stages the data in the block's own buffer (StagePredict)
+    const float2* src_d = blk >= 0 ? ctx->blk_data_stage[blk].as<float2>()
+                                   : reinterpret_cast<const float2*>(st);
     const float2* src_m = reinterpret_cast<const float2*>(st + size_t(cb.n_vis) * E);
     float2* dst = cb.vis.as<float2>();
     if (E == 8)
       pack_kernel<1><<<blocks, 256, 0, ctx->stream>>>(
           ps[i], ctx->run_src_dev.as<uint32_t>(),
-          ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir, dst);
+          ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir,
+          models_in_place ? 0u : ctx->n_dir, dst);
     else if (E == 16)
       pack_kernel<2><<<blocks, 256, 0, ctx->stream>>>(
           ps[i], ctx->run_src_dev.as<uint32_t>(),
-          ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir, dst);
+          ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir,
+          models_in_place ? 0u : ctx->n_dir, dst);
     else
       pack_kernel<4><<<blocks, 256, 0, ctx->stream>>>(
           ps[i], ctx->run_src_dev.as<uint32_t>(),
-          ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir, dst);
+          ctx->run_len_dev.as<uint32_t>(), src_d, src_m, cb.n_vis, ctx->n_dir,
+          models_in_place ? 0u : ctx->n_dir, dst);
     DDS_CHECK_CUDA(ctx, cudaGetLastError());
+  }
+  if (blk >= 0) {  // the block's data staging may be refilled after these packs
+    DDS_CHECK_CUDA(ctx, ddsolve_ctx::EnsureEvent(ctx->blk_packed[blk]));
+    DDS_CHECK_CUDA(ctx, cudaEventRecord(ctx->blk_packed[blk], ctx->stream));
   }
   // The staging and run arrays are reused by the next upload: keep the
   // stream order (a later upload's copies follow these kernels).
@@ -3942,13 +4071,43 @@ StageFn StageCopy(ddsolve_ctx* ctx, const ChannelBlockStore& cb, const float* da
   };
 }
 
-// Stager of the data array plus the GPU predict of the model.
+// Stager of the data array plus the GPU predict of the model, written
+// straight into the block's packed layout (UploadAndPack then packs the data
+// only): every slab of a regular block holds all its runs for a range of
+// time steps.
 StageFn StagePredict(ddsolve_ctx* ctx, const ChannelBlockStore& cb, const float* data,
-                     const PredictJob& job) {
+                     const PredictJob& job, uint32_t cbi) {
   const size_t n = size_t(cb.n_vis) * ctx->elem_bytes;
-  return [ctx, n, data, job](char* st) {
-    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(st, data, n, cudaMemcpyDefault, ctx->stream));
-    return LaunchPredict(ctx, job, reinterpret_cast<float2*>(st + n));
+  return [ctx, n, data, job, &cb, cbi](char*) {
+    // the data into the block's own staging on the copy stream, after the
+    // previous pack of this block has read it; the context stream waits for
+    // the copy before the pack
+    DevBuf& ds = ctx->blk_data_stage[cbi];
+    DDS_CHECK_CUDA(ctx, ds.Reserve(n));
+    if (ctx->blk_packed[cbi])
+      DDS_CHECK_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->blk_packed[cbi], 0));
+    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(ds.ptr, data, n, cudaMemcpyDefault, ctx->copy_stream));
+    DDS_CHECK_CUDA(ctx, ddsolve_ctx::EnsureEvent(ctx->blk_data_copied[cbi]));
+    DDS_CHECK_CUDA(ctx, cudaEventRecord(ctx->blk_data_copied[cbi], ctx->copy_stream));
+    DDS_CHECK_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->blk_data_copied[cbi], 0));
+    PackedTarget t;
+    t.run_ant = cb.run_ant_dev.as<uint32_t>();
+    t.vis = cb.vis.as<float2>();
+    t.W = cb.slabs.empty() ? 0u : cb.slabs.front().W;
+    t.t_elem.resize(job.n_times);
+    t.t_row.resize(job.n_times);
+    uint32_t t0 = 0;
+    for (const HostSlab& s : cb.slabs) {
+      if (s.R != job.n_bl || s.L != job.L || s.W != t.W || s.run_off != 0)
+        return ctx->Fail(DDSOLVE_E_INVALID, "predict: block is not a regular layout");
+      for (uint32_t k = 0; k < s.T && t0 + k < job.n_times; ++k) {
+        t.t_elem[t0 + k] = uint64_t(1 + ctx->n_dir) * s.elem_off;
+        t.t_row[t0 + k] = k * s.L;
+      }
+      t0 += s.T;
+    }
+    if (t0 != job.n_times) return ctx->Fail(DDSOLVE_E_INVALID, "predict: time steps do not match");
+    return LaunchPredict(ctx, job, nullptr, 0, &t, int(cbi));
   };
 }
 
@@ -5166,10 +5325,18 @@ int ddsolve_create(const ddsolve_dims* dims, int device, ddsolve_ctx** out) {
   ctx->cbs.resize(ctx->n_cb);
   ddsolve_default_settings(&ctx->settings);
   e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     g_last_error = std::string("ddsolve_create: ") + cudaGetErrorString(e);
     return DDSOLVE_E_CUDA;
   }
+  ctx->blk_predict_in.resize(ctx->n_cb);
+  ctx->blk_data_stage.resize(ctx->n_cb);
+  ctx->blk_predict_host.assign(ctx->n_cb, nullptr);
+  ctx->blk_predict_host_bytes.assign(ctx->n_cb, 0);
+  ctx->blk_predict_copied.assign(ctx->n_cb, nullptr);
+  ctx->blk_data_copied.assign(ctx->n_cb, nullptr);
+  ctx->blk_packed.assign(ctx->n_cb, nullptr);
   const int rc = EnsureSolutionsBuffers(ctx.get());
   if (rc != DDSOLVE_OK) {
     g_last_error = ctx->err;
@@ -5233,7 +5400,8 @@ uint64_t ddsolve_last_launch_count(const ddsolve_ctx* ctx) {
 static int SetRegularBlock(ddsolve_ctx* ctx, uint32_t cbi, uint32_t n_times,
                            uint32_t n_baselines, uint32_t n_channels,
                            const uint32_t* antenna1, const uint32_t* antenna2,
-                           const std::function<StageFn(const ChannelBlockStore&)>& make_stage) {
+                           const std::function<StageFn(const ChannelBlockStore&)>& make_stage,
+                           bool models_in_place = false) {
   if (!ctx) return DDSOLVE_E_INVALID;
   if (cbi >= ctx->n_cb) return ctx->Fail(DDSOLVE_E_INVALID, "channel block out of range");
   if (n_times == 0 || n_baselines == 0 || n_channels == 0 || !antenna1 || !antenna2)
@@ -5338,7 +5506,8 @@ static int SetRegularBlock(ddsolve_ctx* ctx, uint32_t cbi, uint32_t n_times,
     t0 = t1;
   }
   cb.n_elems = off;
-  return UploadAndPack(ctx, cb, make_stage(cb));
+  return UploadAndPack(ctx, cb, make_stage(cb), models_in_place,
+                       models_in_place ? int(cbi) : -1);
 }
 
 int ddsolve_set_channel_block_regular(ddsolve_ctx* ctx, uint32_t cbi, uint32_t n_times,
@@ -5367,8 +5536,9 @@ int ddsolve_set_channel_block_regular_sky(ddsolve_ctx* ctx, uint32_t cbi, uint32
   if (rc != DDSOLVE_OK) return rc;
   return SetRegularBlock(ctx, cbi, n_times, n_baselines, n_channels, antenna1, antenna2,
                          [&](const ChannelBlockStore& cb) {
-                           return StagePredict(ctx, cb, data, job);
-                         });
+                           return StagePredict(ctx, cb, data, job, cbi);
+                         },
+                         true);
 }
 
 // A device address for a host-or-device input: device memory of the
@@ -5523,10 +5693,19 @@ int ddsolve_correct_and_subtract(ddsolve_ctx* ctx, const ddsolve_subtract_buffer
   char* base = ctx->raw_in.as<char>();
   char* staged_m = ctx->raw_model.as<char>();
   int rc;
-  const void *d_data = nullptr, *d_sol = nullptr;
+  auto on_device = [&](const void* ptr) {
+    cudaPointerAttributes a{};
+    const bool dev = cudaPointerGetAttributes(&a, ptr) == cudaSuccess &&
+                     a.type == cudaMemoryTypeDevice && a.device == ctx->device;
+    cudaGetLastError();
+    return dev;
+  };
+  const void* d_data = nullptr;
   if (data_out && (rc = DeviceView(ctx, in->data, b_data, ctx->raw_in, 0, &d_data)) != DDSOLVE_OK)
     return rc;
-  if ((rc = DeviceView(ctx, solutions, b_sol, ctx->raw_in, o_sol, &d_sol)) != DDSOLVE_OK) return rc;
+  // host solutions travel in the pinned image of the small inputs below
+  const bool sol_on_device = on_device(solutions);
+  const void* d_sol = sol_on_device ? static_cast<const void*>(solutions) : base + o_sol;
   // Every direction's model: used in place when it is device memory, else
   // staged (or predicted) into direction d's slice of raw_model.
   std::vector<const void*> m_in(n_dir);
@@ -5545,13 +5724,6 @@ int ddsolve_correct_and_subtract(ddsolve_ctx* ctx, const ddsolve_subtract_buffer
   // Outputs in device memory are written in place; host outputs go through
   // device memory of the context (the staged data or model slice when that
   // input was staged, else cs_out) and one copy back each.
-  auto on_device = [&](const void* ptr) {
-    cudaPointerAttributes a{};
-    const bool dev = cudaPointerGetAttributes(&a, ptr) == cudaSuccess &&
-                     a.type == cudaMemoryTypeDevice && a.device == ctx->device;
-    cudaGetLastError();
-    return dev;
-  };
   const bool data_dev = data_out && on_device(data_out);
   float4* k_data = nullptr;
   if (data_out) {
@@ -5585,16 +5757,19 @@ int ddsolve_correct_and_subtract(ddsolve_ctx* ctx, const ddsolve_subtract_buffer
         o += b_dir;
       }
   }
-  // antennas and the per-direction pointer tables: one small copy each
-  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_a1, in->antenna1, b_a, cudaMemcpyHostToDevice,
-                                      ctx->stream));
-  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_a2, in->antenna2, b_a, cudaMemcpyHostToDevice,
-                                      ctx->stream));
-  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_pin, m_in.data(), b_ptr, cudaMemcpyHostToDevice,
-                                      ctx->stream));
-  if (models_out)
-    DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + o_pout, m_out.data(), b_ptr,
-                                        cudaMemcpyHostToDevice, ctx->stream));
+  // The small inputs (host solutions, antennas, the per-direction pointer
+  // tables) in one pinned image and one copy; the call synchronises before
+  // it returns, so the image is free again for the next call.
+  const size_t img_lo = sol_on_device ? o_a1 : o_sol, img_hi = o_pout + align(b_ptr);
+  DDS_CHECK_CUDA(ctx, ctx->ReserveSmallHost(img_hi - img_lo));
+  char* img = static_cast<char*>(ctx->small_host) - img_lo;
+  if (!sol_on_device) std::memcpy(img + o_sol, solutions, b_sol);
+  std::memcpy(img + o_a1, in->antenna1, b_a);
+  std::memcpy(img + o_a2, in->antenna2, b_a);
+  std::memcpy(img + o_pin, m_in.data(), b_ptr);
+  if (models_out) std::memcpy(img + o_pout, m_out.data(), b_ptr);
+  DDS_CHECK_CUDA(ctx, cudaMemcpyAsync(base + img_lo, img + img_lo, img_hi - img_lo,
+                                      cudaMemcpyHostToDevice, ctx->stream));
   CorrectParams p;
   p.data = static_cast<const float4*>(d_data);
   p.model = reinterpret_cast<const float4* const*>(base + o_pin);
