@@ -344,6 +344,7 @@ struct PredictParams {
   const uint64_t* t_elem;   // [n_times]
   const uint32_t* t_row;    // [n_times]
   uint32_t W;
+  const uint32_t* unpol;    // [n_dir]: nonzero when all the direction's sources have Q = U = V = 0
 };
 
 struct PhasorParams {
@@ -448,6 +449,71 @@ struct PredictSource {
   }
 };
 
+// The channel chunks of one (time, baseline, direction): NA accumulators,
+// NCORR, or one for a direction whose sources are all unpolarized (Stokes Q =
+// U = V = 0: XX = YY = the same sum of I terms, XY = YX = 0, so one sum gives
+// every correlation with the same products and additions).
+template <int NCORR, int NA>
+__device__ __forceinline__ void PredictChunks(const PredictParams& p, const double* src,
+                                              uint32_t ns, const double2* tp0, const double2* tq0,
+                                              size_t src_stride, float2* out, uint64_t cstride) {
+  constexpr int CH = kPredictChunk / NCORR;
+  for (uint32_t c0 = 0; c0 < p.L; c0 += CH) {
+    const uint32_t nc = min(uint32_t(CH), p.L - c0);
+    double2 acc[CH][NA];
+#pragma unroll
+    for (int c = 0; c < CH; ++c)
+#pragma unroll
+      for (int k = 0; k < NA; ++k) acc[c][k] = make_double2(0.0, 0.0);
+    // Two sources at a time: their phasor chains are independent, so the
+    // FP64 rotations of one fill the latency of the other's. Per channel the
+    // sources are still added in order.
+    uint32_t s = 0;
+    for (; s + 2 <= ns; s += 2) {
+      PredictSource<NA, CH> a, b;
+      a.Start(src + s * 8, tp0 + s * src_stride, tq0 + s * src_stride, p, c0);
+      b.Start(src + (s + 1) * 8, tp0 + (s + 1) * src_stride, tq0 + (s + 1) * src_stride, p, c0);
+#pragma unroll
+      for (int c = 0; c < CH; ++c) {
+        if (c < int(nc)) {
+          if (c > 0) {
+            a.Advance(p, c0 + c);
+            b.Advance(p, c0 + c);
+          }
+          a.AddTo(acc[c]);
+          b.AddTo(acc[c]);
+        }
+      }
+    }
+    if (s < ns) {
+      PredictSource<NA, CH> a;
+      a.Start(src + s * 8, tp0 + s * src_stride, tq0 + s * src_stride, p, c0);
+#pragma unroll
+      for (int c = 0; c < CH; ++c) {
+        if (c < int(nc)) {
+          if (c > 0) a.Advance(p, c0 + c);
+          a.AddTo(acc[c]);
+        }
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < CH; ++c)
+      if (c < int(nc)) {
+        float2* o = out + uint64_t(c0 + c) * cstride;
+#pragma unroll
+        for (int k = 0; k < NCORR; ++k) {
+          if (NA == NCORR) {
+            o[k] = make_float2(float(acc[c][k].x), float(acc[c][k].y));
+          } else {
+            const bool diag = k == 0 || k == NCORR - 1;
+            o[k] = diag ? make_float2(float(acc[c][0].x), float(acc[c][0].y))
+                        : make_float2(0.f, 0.f);
+          }
+        }
+      }
+  }
+}
+
 template <int NCORR>
 __global__ void __launch_bounds__(kPredictThreads) predict_kernel(const PredictParams p) {
   constexpr int CH = kPredictChunk / NCORR;
@@ -494,52 +560,10 @@ __global__ void __launch_bounds__(kPredictThreads) predict_kernel(const PredictP
   const double2* tab = p.table + (size_t(t) * p.n_dir + d) * p.max_src * src_stride;
   const double2* tp0 = tab + size_t(ap) * p.n_slots;
   const double2* tq0 = tab + size_t(aq) * p.n_slots;
-  for (uint32_t c0 = 0; c0 < p.L; c0 += CH) {
-    const uint32_t nc = min(uint32_t(CH), p.L - c0);
-    double2 acc[CH][NCORR];
-#pragma unroll
-    for (int c = 0; c < CH; ++c)
-#pragma unroll
-      for (int k = 0; k < NCORR; ++k) acc[c][k] = make_double2(0.0, 0.0);
-    // Two sources at a time: their phasor chains are independent, so the
-    // FP64 rotations of one fill the latency of the other's. Per channel the
-    // sources are still added in order.
-    uint32_t s = 0;
-    for (; s + 2 <= ns; s += 2) {
-      PredictSource<NCORR, CH> a, b;
-      a.Start(src + s * 8, tp0 + s * src_stride, tq0 + s * src_stride, p, c0);
-      b.Start(src + (s + 1) * 8, tp0 + (s + 1) * src_stride, tq0 + (s + 1) * src_stride, p, c0);
-#pragma unroll
-      for (int c = 0; c < CH; ++c) {
-        if (c < int(nc)) {
-          if (c > 0) {
-            a.Advance(p, c0 + c);
-            b.Advance(p, c0 + c);
-          }
-          a.AddTo(acc[c]);
-          b.AddTo(acc[c]);
-        }
-      }
-    }
-    if (s < ns) {
-      PredictSource<NCORR, CH> a;
-      a.Start(src + s * 8, tp0 + s * src_stride, tq0 + s * src_stride, p, c0);
-#pragma unroll
-      for (int c = 0; c < CH; ++c) {
-        if (c < int(nc)) {
-          if (c > 0) a.Advance(p, c0 + c);
-          a.AddTo(acc[c]);
-        }
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < CH; ++c)
-      if (c < int(nc)) {
-        float2* o = at(c0 + c);
-#pragma unroll
-        for (int k = 0; k < NCORR; ++k) o[k] = make_float2(float(acc[c][k].x), float(acc[c][k].y));
-      }
-  }
+  if (NCORR == 1 || p.unpol[d])
+    PredictChunks<NCORR, 1>(p, src, ns, tp0, tq0, src_stride, out, cstride);
+  else
+    PredictChunks<NCORR, NCORR>(p, src, ns, tp0, tq0, src_stride, out, cstride);
 }
 
 // ---------------------------------------------------------------------------
@@ -3853,7 +3877,13 @@ int LaunchPredict(ddsolve_ctx* ctx, const PredictJob& j, float2* model, uint32_t
   const size_t o_src = align(b_uvw), o_off = o_src + align(b_src), o_f = o_off + align(b_off);
   const size_t b_te = packed ? size_t(j.n_times) * 8 : 0, b_tr = packed ? size_t(j.n_times) * 4 : 0;
   const size_t o_a1 = o_f + align(b_f), o_a2 = o_a1 + align(b_a), o_te = o_a2 + align(b_a);
-  const size_t o_tr = o_te + align(b_te), total = o_tr + align(b_tr);
+  const size_t o_tr = o_te + align(b_te), o_up = o_tr + align(b_tr);
+  const size_t b_up = size_t(ctx->n_dir) * 4, total = o_up + align(b_up);
+  std::vector<uint32_t> unpol(ctx->n_dir, 1u);
+  for (uint32_t d = 0; d < ctx->n_dir; ++d)
+    for (uint32_t s = 0; s < j.sky[d].n_sources && unpol[d]; ++s)
+      for (int k = 1; k < 4; ++k)
+        if (j.sky[d].stokes[4 * s + k] != 0.0) unpol[d] = 0u;
   // the device inputs and their pinned image: the context's, or channel
   // block blk's own (blocks then do not wait for each other's copies)
   DevBuf& pin = blk >= 0 ? ctx->blk_predict_in[blk] : ctx->predict_in;
@@ -3882,13 +3912,14 @@ int LaunchPredict(ddsolve_ctx* ctx, const PredictJob& j, float2* model, uint32_t
     const void* src;
     size_t off, bytes;
   };
-  constexpr int kPieces = 8;
+  constexpr int kPieces = 9;
   const Piece pieces[kPieces] = {
       {j.uvw, 0, b_uvw},          {src.data(), o_src, src.size() * 8},
       {off.data(), o_off, b_off}, {j.freq, o_f, b_f},
       {j.a1, o_a1, b_a},          {j.a2, o_a2, b_a},
       {packed ? static_cast<const void*>(packed->t_elem.data()) : nullptr, o_te, b_te},
-      {packed ? static_cast<const void*>(packed->t_row.data()) : nullptr, o_tr, b_tr}};
+      {packed ? static_cast<const void*>(packed->t_row.data()) : nullptr, o_tr, b_tr},
+      {unpol.data(), o_up, b_up}};
   bool device_piece[kPieces];
   for (int k = 0; k < kPieces; ++k) {
     const Piece& pc = pieces[k];
@@ -3948,6 +3979,7 @@ int LaunchPredict(ddsolve_ctx* ctx, const PredictJob& j, float2* model, uint32_t
   p.t_elem = reinterpret_cast<const uint64_t*>(base + o_te);
   p.t_row = reinterpret_cast<const uint32_t*>(base + o_tr);
   p.W = packed ? packed->W : 0;
+  p.unpol = reinterpret_cast<const uint32_t*>(base + o_up);
   const size_t smem = size_t(max_src) * 8 * sizeof(double);
   const dim3 grid((j.n_bl + kPredictThreads - 1) / kPredictThreads, j.n_times, ctx->n_dir);
   const void* fn = nc == 1   ? reinterpret_cast<const void*>(predict_kernel<1>)
