@@ -404,13 +404,33 @@ struct PredictSource {
   const double2* tp;
   const double2* tq;
   double re[NCORR], im[NCORR];
+  // the four station phasors a Start needs: the chunk's first channel and
+  // the step (evenly spaced channels) of both stations
+  struct Loads {
+    double2 q, p, qs, ps;
+  };
+  static __device__ __forceinline__ Loads Load(const double2* tp_, const double2* tq_,
+                                               const PredictParams& p, uint32_t c0) {
+    const uint32_t k = p.uniform ? c0 / CH : c0;
+    Loads l;
+    l.q = __ldg(tq_ + k);
+    l.p = __ldg(tp_ + k);
+    if (p.uniform) {
+      l.qs = __ldg(tq_ + p.n_slots - 1);
+      l.ps = __ldg(tp_ + p.n_slots - 1);
+    }
+    return l;
+  }
   __device__ __forceinline__ void Start(const double* q, const double2* tp_, const double2* tq_,
                                         const PredictParams& p, uint32_t c0) {
+    Start(q, tp_, tq_, p, Load(tp_, tq_, p, c0));
+  }
+  __device__ __forceinline__ void Start(const double* q, const double2* tp_, const double2* tq_,
+                                        const PredictParams& p, const Loads& l) {
     tp = tp_;
     tq = tq_;
-    const uint32_t k = p.uniform ? c0 / CH : c0;
-    PhasorProduct(__ldg(tq + k), __ldg(tp + k), zc, zs);
-    if (p.uniform) PhasorProduct(__ldg(tq + p.n_slots - 1), __ldg(tp + p.n_slots - 1), sc, ss);
+    PhasorProduct(l.q, l.p, zc, zs);
+    if (p.uniform) PhasorProduct(l.qs, l.ps, sc, ss);
     if (NCORR == 1) {
       re[0] = q[3];
     } else if (NCORR == 2) {
@@ -468,11 +488,23 @@ __device__ __forceinline__ void PredictChunks(const PredictParams& p, const doub
     // Two sources at a time: their phasor chains are independent, so the
     // FP64 rotations of one fill the latency of the other's. Per channel the
     // sources are still added in order.
+    // The next pair's table phasors are loaded before this pair's channel
+    // work, so that their latency hides under it.
+    using Src = PredictSource<NA, CH>;
     uint32_t s = 0;
+    typename Src::Loads la, lb;
+    if (ns >= 2) {
+      la = Src::Load(tp0, tq0, p, c0);
+      lb = Src::Load(tp0 + src_stride, tq0 + src_stride, p, c0);
+    }
     for (; s + 2 <= ns; s += 2) {
-      PredictSource<NA, CH> a, b;
-      a.Start(src + s * 8, tp0 + s * src_stride, tq0 + s * src_stride, p, c0);
-      b.Start(src + (s + 1) * 8, tp0 + (s + 1) * src_stride, tq0 + (s + 1) * src_stride, p, c0);
+      Src a, b;
+      a.Start(src + s * 8, tp0 + s * src_stride, tq0 + s * src_stride, p, la);
+      b.Start(src + (s + 1) * 8, tp0 + (s + 1) * src_stride, tq0 + (s + 1) * src_stride, p, lb);
+      if (s + 4 <= ns) {
+        la = Src::Load(tp0 + (s + 2) * src_stride, tq0 + (s + 2) * src_stride, p, c0);
+        lb = Src::Load(tp0 + (s + 3) * src_stride, tq0 + (s + 3) * src_stride, p, c0);
+      }
 #pragma unroll
       for (int c = 0; c < CH; ++c) {
         if (c < int(nc)) {
@@ -514,7 +546,9 @@ __device__ __forceinline__ void PredictChunks(const PredictParams& p, const doub
   }
 }
 
-template <int NCORR>
+// ALL_UNPOL: every direction of the launch is unpolarized (one accumulator
+// per channel throughout, so the kernel's registers are those of that path).
+template <int NCORR, bool ALL_UNPOL>
 __global__ void __launch_bounds__(kPredictThreads) predict_kernel(const PredictParams p) {
   constexpr int CH = kPredictChunk / NCORR;
   extern __shared__ double predict_smem[];
@@ -560,7 +594,9 @@ __global__ void __launch_bounds__(kPredictThreads) predict_kernel(const PredictP
   const double2* tab = p.table + (size_t(t) * p.n_dir + d) * p.max_src * src_stride;
   const double2* tp0 = tab + size_t(ap) * p.n_slots;
   const double2* tq0 = tab + size_t(aq) * p.n_slots;
-  if (NCORR == 1 || p.unpol[d])
+  if (ALL_UNPOL || NCORR == 1)
+    PredictChunks<NCORR, 1>(p, src, ns, tp0, tq0, src_stride, out, cstride);
+  else if (p.unpol[d])
     PredictChunks<NCORR, 1>(p, src, ns, tp0, tq0, src_stride, out, cstride);
   else
     PredictChunks<NCORR, NCORR>(p, src, ns, tp0, tq0, src_stride, out, cstride);
@@ -3982,9 +4018,14 @@ int LaunchPredict(ddsolve_ctx* ctx, const PredictJob& j, float2* model, uint32_t
   p.unpol = reinterpret_cast<const uint32_t*>(base + o_up);
   const size_t smem = size_t(max_src) * 8 * sizeof(double);
   const dim3 grid((j.n_bl + kPredictThreads - 1) / kPredictThreads, j.n_times, ctx->n_dir);
-  const void* fn = nc == 1   ? reinterpret_cast<const void*>(predict_kernel<1>)
-                   : nc == 2 ? reinterpret_cast<const void*>(predict_kernel<2>)
-                             : reinterpret_cast<const void*>(predict_kernel<4>);
+  const bool all_unpol = std::all_of(unpol.begin(), unpol.end(), [](uint32_t u) { return u != 0; });
+  const void* fn =
+      nc == 1 ? reinterpret_cast<const void*>(predict_kernel<1, true>)
+      : nc == 2
+          ? (all_unpol ? reinterpret_cast<const void*>(predict_kernel<2, true>)
+                       : reinterpret_cast<const void*>(predict_kernel<2, false>))
+          : (all_unpol ? reinterpret_cast<const void*>(predict_kernel<4, true>)
+                       : reinterpret_cast<const void*>(predict_kernel<4, false>));
   DDS_CHECK_CUDA(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            int(kPredictMaxSmem)));
   void* args[] = {&p};
