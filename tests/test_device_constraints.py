@@ -8,7 +8,7 @@ AssignSolutions (IterativeDiagonalSolver.cc:77-83).
 
 GPU: the whole constrained loop runs on the device (one CUDA graph); the
 iteration count equals the reference's and the solutions agree to 1e-4
-relative after phase referencing to antenna 0, on
+relative after phase referencing to antenna 0 (the parity tolerance), on
 the pipelined path (2 and 4 correlations) and on the streaming path
 (1 correlation), diagonal and scalar. CPU: the reference-oracle side of the
 new constraint options.

@@ -11,7 +11,7 @@ through DP3's own SolverBase::ApplyConstraints between device passes.
 CPU: the library loads and DP3's own path through the harness reproduces the
 reference-code oracle bit for bit. GPU: the adapter against DP3's own solver
 on the same inputs: identical iteration counts and <= 1e-4 relative after
-phase referencing to antenna 0, with and without
+phase referencing to antenna 0 (the parity tolerance), with and without
 constraints, including a solve that DP3's stall detection stops.
 """
 import ctypes

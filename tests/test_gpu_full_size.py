@@ -3,7 +3,7 @@
 The reference here is DP3's own IterativeDiagonalSolver / IterativeScalarSolver
 compiled from the reference sources (oracle/_ref, oracle/ref_ffi.py), run with
 one thread per channel block (a fixed FP32 summation order). The bar is the
-north star's: identical iteration counts at tolerance 1e-5 and solutions
+parity contract's: identical iteration counts at tolerance 1e-5 and solutions
 within 1e-4 relative after phase referencing to antenna 0. Cases:
 
 * benchmark configurations from unit solutions (51 iterations, capped): c1

@@ -1,6 +1,6 @@
 """GPU parity of the CUDA solver against the CPU oracle, through the C ABI.
 
-Tolerances (stated by the north-star contract):
+Tolerances (the parity contract of this path):
   * one direction-iterative pass (next_solutions before the step): relative
     difference <= 1e-4 per element vs the FP64 oracle;
   * full solves: identical iteration counts and max relative difference
