@@ -3128,6 +3128,82 @@ __global__ void __launch_bounds__(kFjThreads) fj_pass_kernel(const FjPassParams 
   FjStoreSlots<ND>(p.partials + size_t(gt) * ND * kFjSlotFloats, P1, D1, P2, D2);
 }
 
+// Two directions (NL = 2): NL lanes per part of a run, lane l owning
+// direction l (lanes past n_dir idle). Per row every lane loads its own
+// direction's model and the data, forms its term J_1 M J_2^H, gathers the
+// terms of the run's lanes by shuffles and subtracts them from the data in
+// direction order, which gives every lane the residual of fj_pass_kernel (the
+// same FP32 operations in the same order), and accumulates its own
+// direction. A lane holds one direction's gains and sums instead of all of
+// them, so an SM keeps several times as many warps in flight.
+template <int NL>
+__global__ void __launch_bounds__(kFjThreads) fj_lane_kernel(const FjPassParams p) {
+  if (SolveStopped(p.state, p.use_handle)) return;
+  const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t unit = gl / NL, l = gl % NL;  // unit: part * n_runs + global run
+  if (unit >= p.n_runs * p.n_parts) return;    // the whole group of NL lanes
+  const uint32_t lane = threadIdx.x & 31u;
+  const unsigned group = ((1u << NL) - 1u) << (lane & ~uint32_t(NL - 1));
+  const uint32_t first = lane & ~uint32_t(NL - 1);
+  const uint32_t gr = unit % p.n_runs, part = unit / p.n_runs;
+  const uint32_t si = FjSlabOf(p, gr);
+  const SlabDesc sl = p.slabs[si];
+  const uint32_t r = gr - p.run_start[si];
+  const uint32_t ap = sl.run_ant[r];
+  const uint32_t a1 = ap & 0xFFFFu, a2 = ap >> 16;
+  const uint32_t nd = p.n_dir;
+  const bool own = l < nd;
+  C22 J1, J2, P1, P2;
+  H22 D1, D2;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    J1.m[k] = J2.m[k] = P1.m[k] = P2.m[k] = make_float2(0.f, 0.f);
+  }
+  ZeroH22(D1);
+  ZeroH22(D2);
+  if (own) {
+    const size_t cb_off = size_t(sl.cb) * p.n_ant * p.n_sub;
+    const uint32_t s = p.slab_sol[sl.sol_off + l];
+    J1 = LoadJones(p.solutions + (cb_off + size_t(a1) * p.n_sub + s) * 4);
+    J2 = LoadJones(p.solutions + (cb_off + size_t(a2) * p.n_sub + s) * 4);
+  }
+  const float2* vis = static_cast<const float2*>(sl.vis);
+  const uint64_t rows = uint64_t(sl.T) * sl.L;
+  const uint64_t row_end = rows * (part + 1) / p.n_parts;
+  for (uint64_t row = rows * part / p.n_parts; row < row_end; ++row) {
+    C22 M;
+    if (own) {
+      M = LoadC22(vis + SlabElem(sl.R, sl.W, nd + 1, row, 1 + l, r) * 4);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) M.m[k] = make_float2(0.f, 0.f);
+    }
+    C22 R = LoadC22(vis + SlabElem(sl.R, sl.W, nd + 1, row, 0, r) * 4);
+    const C22 Y = Mul22(J1, M);
+    const C22 t = MulHerm22(Y, J2);  // J_1 M J_2^H of this lane's direction
+#pragma unroll
+    for (int e = 0; e < NL; ++e) {
+      C22 te;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        te.m[k].x = __shfl_sync(group, t.m[k].x, first + e);
+        te.m[k].y = __shfl_sync(group, t.m[k].y, first + e);
+      }
+      if (uint32_t(e) < nd) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          R.m[k] = make_float2(R.m[k].x - te.m[k].x, R.m[k].y - te.m[k].y);
+      }
+    }
+    const C22 X = MulHerm22(J2, M);  // J_2 M^H
+    AddMul22(P1, R, X);
+    AddGram22(D1, X);
+    AddHermMul22(P2, R, Y);
+    AddGram22(D2, Y);
+  }
+  if (own) FjStoreSlots<1>(p.partials + (size_t(unit) * nd + l) * kFjSlotFloats, &P1, &D1, &P2, &D2);
+}
+
 struct D22 {
   double2 m[4];
 };
@@ -4519,7 +4595,9 @@ int BuildFullJonesPlan(ddsolve_ctx* ctx) {
       total_runs += s.R;
       max_rows = std::max<uint64_t>(max_rows, uint64_t(s.T) * s.L);
     }
-  const uint64_t want_threads = uint64_t(std::max(ctx->n_sm, 1)) * 256 * 4;
+  // (two directions: two lanes per part, so fewer parts give the same waves)
+  const uint64_t lanes = n_dir == 2 ? 2 : 1;
+  const uint64_t want_threads = uint64_t(std::max(ctx->n_sm, 1)) * 256 * 4 / lanes;
   uint64_t parts = total_runs ? (want_threads + total_runs - 1) / total_runs : 1;
   parts = std::max<uint64_t>(1, std::min<uint64_t>({parts, max_rows / 16, 16}));
   if (total_runs * parts * n_dir >= (uint64_t(1) << 31)) parts = 1;
@@ -5127,9 +5205,14 @@ int LaunchFullJones(ddsolve_ctx* ctx, bool host_mode, bool use_handle, bool with
   pp.n_parts = ctx->fj_parts;
   const uint32_t blocks = std::max<uint32_t>(
       1, uint32_t((uint64_t(ctx->fj_n_runs) * ctx->fj_parts + kFjThreads - 1) / kFjThreads));
+  const uint64_t units = uint64_t(ctx->fj_n_runs) * ctx->fj_parts;
+  const uint32_t blocks2 = uint32_t(std::max<uint64_t>(1, (units * 2 + kFjThreads - 1) / kFjThreads));
+  // two directions: two lanes per part (measured faster than one thread per
+  // part); three or four: one thread per part (the four-lane form's extra
+  // loads and shuffles measured slower than its higher occupancy gains)
   switch (ctx->n_dir) {
     case 1: fj_pass_kernel<1><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
-    case 2: fj_pass_kernel<2><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
+    case 2: fj_lane_kernel<2><<<blocks2, kFjThreads, 0, ctx->stream>>>(pp); break;
     case 3: fj_pass_kernel<3><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
     case 4: fj_pass_kernel<4><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
     default:
