@@ -3128,15 +3128,16 @@ __global__ void __launch_bounds__(kFjThreads) fj_pass_kernel(const FjPassParams 
   FjStoreSlots<ND>(p.partials + size_t(gt) * ND * kFjSlotFloats, P1, D1, P2, D2);
 }
 
-// Two directions (NL = 2): NL lanes per part of a run, lane l owning
-// direction l (lanes past n_dir idle). Per row every lane loads its own
-// direction's model and the data, forms its term J_1 M J_2^H, gathers the
-// terms of the run's lanes by shuffles and subtracts them from the data in
-// direction order, which gives every lane the residual of fj_pass_kernel (the
-// same FP32 operations in the same order), and accumulates its own
-// direction. A lane holds one direction's gains and sums instead of all of
-// them, so an SM keeps several times as many warps in flight.
-template <int NL>
+// NL lanes per part of a run (used for two directions: NL = 2, DPL = 1),
+// lane l owning directions l * DPL .. l * DPL + DPL - 1 (those past n_dir
+// idle). Per row
+// every lane loads its own directions' models and the data, forms their
+// terms J_1 M J_2^H, gathers the terms of the run's lanes by shuffles and
+// subtracts them from the data in direction order, which gives every lane
+// the residual of fj_pass_kernel (the same FP32 operations in the same
+// order), and accumulates its own directions. A lane holds DPL directions'
+// gains and sums instead of all of them, so an SM keeps more warps in flight.
+template <int NL, int DPL>
 __global__ void __launch_bounds__(kFjThreads) fj_lane_kernel(const FjPassParams p) {
   if (SolveStopped(p.state, p.use_handle)) return;
   const uint32_t gl = blockIdx.x * blockDim.x + threadIdx.x;
@@ -3152,56 +3153,73 @@ __global__ void __launch_bounds__(kFjThreads) fj_lane_kernel(const FjPassParams 
   const uint32_t ap = sl.run_ant[r];
   const uint32_t a1 = ap & 0xFFFFu, a2 = ap >> 16;
   const uint32_t nd = p.n_dir;
-  const bool own = l < nd;
-  C22 J1, J2, P1, P2;
-  H22 D1, D2;
+  C22 J1[DPL], J2[DPL], P1[DPL], P2[DPL];
+  H22 D1[DPL], D2[DPL];
+  const size_t cb_off = size_t(sl.cb) * p.n_ant * p.n_sub;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    J1.m[k] = J2.m[k] = P1.m[k] = P2.m[k] = make_float2(0.f, 0.f);
-  }
-  ZeroH22(D1);
-  ZeroH22(D2);
-  if (own) {
-    const size_t cb_off = size_t(sl.cb) * p.n_ant * p.n_sub;
-    const uint32_t s = p.slab_sol[sl.sol_off + l];
-    J1 = LoadJones(p.solutions + (cb_off + size_t(a1) * p.n_sub + s) * 4);
-    J2 = LoadJones(p.solutions + (cb_off + size_t(a2) * p.n_sub + s) * 4);
+  for (int k = 0; k < DPL; ++k) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      J1[k].m[q] = J2[k].m[q] = P1[k].m[q] = P2[k].m[q] = make_float2(0.f, 0.f);
+    ZeroH22(D1[k]);
+    ZeroH22(D2[k]);
+    const uint32_t d = l * DPL + k;
+    if (d < nd) {
+      const uint32_t s = p.slab_sol[sl.sol_off + d];
+      J1[k] = LoadJones(p.solutions + (cb_off + size_t(a1) * p.n_sub + s) * 4);
+      J2[k] = LoadJones(p.solutions + (cb_off + size_t(a2) * p.n_sub + s) * 4);
+    }
   }
   const float2* vis = static_cast<const float2*>(sl.vis);
   const uint64_t rows = uint64_t(sl.T) * sl.L;
   const uint64_t row_end = rows * (part + 1) / p.n_parts;
   for (uint64_t row = rows * part / p.n_parts; row < row_end; ++row) {
-    C22 M;
-    if (own) {
-      M = LoadC22(vis + SlabElem(sl.R, sl.W, nd + 1, row, 1 + l, r) * 4);
-    } else {
+    C22 M[DPL], Y[DPL], t[DPL];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) M.m[k] = make_float2(0.f, 0.f);
+    for (int k = 0; k < DPL; ++k) {
+      const uint32_t d = l * DPL + k;
+      if (d < nd) {
+        M[k] = LoadC22(vis + SlabElem(sl.R, sl.W, nd + 1, row, 1 + d, r) * 4);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) M[k].m[q] = make_float2(0.f, 0.f);
+      }
+      Y[k] = Mul22(J1[k], M[k]);
+      t[k] = MulHerm22(Y[k], J2[k]);  // J_1 M J_2^H of direction d
     }
     C22 R = LoadC22(vis + SlabElem(sl.R, sl.W, nd + 1, row, 0, r) * 4);
-    const C22 Y = Mul22(J1, M);
-    const C22 t = MulHerm22(Y, J2);  // J_1 M J_2^H of this lane's direction
 #pragma unroll
-    for (int e = 0; e < NL; ++e) {
-      C22 te;
+    for (int e = 0; e < NL; ++e)
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        te.m[k].x = __shfl_sync(group, t.m[k].x, first + e);
-        te.m[k].y = __shfl_sync(group, t.m[k].y, first + e);
+      for (int k = 0; k < DPL; ++k) {
+        C22 te;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          te.m[q].x = __shfl_sync(group, t[k].m[q].x, first + e);
+          te.m[q].y = __shfl_sync(group, t[k].m[q].y, first + e);
+        }
+        if (uint32_t(e * DPL + k) < nd) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            R.m[q] = make_float2(R.m[q].x - te.m[q].x, R.m[q].y - te.m[q].y);
+        }
       }
-      if (uint32_t(e) < nd) {
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
-          R.m[k] = make_float2(R.m[k].x - te.m[k].x, R.m[k].y - te.m[k].y);
-      }
+    for (int k = 0; k < DPL; ++k) {
+      const C22 X = MulHerm22(J2[k], M[k]);  // J_2 M^H
+      AddMul22(P1[k], R, X);
+      AddGram22(D1[k], X);
+      AddHermMul22(P2[k], R, Y[k]);
+      AddGram22(D2[k], Y[k]);
     }
-    const C22 X = MulHerm22(J2, M);  // J_2 M^H
-    AddMul22(P1, R, X);
-    AddGram22(D1, X);
-    AddHermMul22(P2, R, Y);
-    AddGram22(D2, Y);
   }
-  if (own) FjStoreSlots<1>(p.partials + (size_t(unit) * nd + l) * kFjSlotFloats, &P1, &D1, &P2, &D2);
+#pragma unroll
+  for (int k = 0; k < DPL; ++k) {
+    const uint32_t d = l * DPL + k;
+    if (d < nd)
+      FjStoreSlots<1>(p.partials + (size_t(unit) * nd + d) * kFjSlotFloats, &P1[k], &D1[k],
+                      &P2[k], &D2[k]);
+  }
 }
 
 struct D22 {
@@ -5208,11 +5226,12 @@ int LaunchFullJones(ddsolve_ctx* ctx, bool host_mode, bool use_handle, bool with
   const uint64_t units = uint64_t(ctx->fj_n_runs) * ctx->fj_parts;
   const uint32_t blocks2 = uint32_t(std::max<uint64_t>(1, (units * 2 + kFjThreads - 1) / kFjThreads));
   // two directions: two lanes per part (measured faster than one thread per
-  // part); three or four: one thread per part (the four-lane form's extra
-  // loads and shuffles measured slower than its higher occupancy gains)
+  // part); three or four: one thread per part (two lanes of two directions
+  // and four lanes of one direction each measured slower: their extra loads
+  // and shuffles cost more than their occupancy gives)
   switch (ctx->n_dir) {
     case 1: fj_pass_kernel<1><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
-    case 2: fj_lane_kernel<2><<<blocks2, kFjThreads, 0, ctx->stream>>>(pp); break;
+    case 2: fj_lane_kernel<2, 1><<<blocks2, kFjThreads, 0, ctx->stream>>>(pp); break;
     case 3: fj_pass_kernel<3><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
     case 4: fj_pass_kernel<4><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
     default:
