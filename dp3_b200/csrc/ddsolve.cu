@@ -2898,8 +2898,8 @@ __device__ __forceinline__ C22 LoadJones(const double2* s) {  // FP32, as MC2x2F
 
 constexpr int kFjThreads = 128;
 // Directions whose gains and sums one thread holds in registers: up to this
-// many, fj_pass_kernel does everything in one read of the visibilities; more
-// directions go through fj_chunk_kernel, one launch per group of this many.
+// many, one pass kernel does everything in one read of the visibilities; more
+// directions go through fj_residual_kernel and fj_accumulate_kernel.
 constexpr int kFjMaxDirections = 4;
 constexpr uint32_t kFjSlotFloats = 32;  // per run and direction: P and den of both sides
 
@@ -2911,7 +2911,6 @@ struct FjPassParams {
   float* partials;            // [part][global run][direction][kFjSlotFloats]
   uint32_t n_slabs, n_runs, n_ant, n_sub, n_dir;
   uint32_t n_parts;           // each run's rows split into this many parts
-  uint32_t d0;                // fj_chunk_kernel: first direction of the launch
   float2* resid;              // more than kFjMaxDirections: the residual, [slab rows][R][4]
   const uint64_t* resid_off;  // [n_slabs]: first residual element of each slab
   const LoopState* state;
@@ -2974,10 +2973,9 @@ __device__ __forceinline__ void FjStoreSlots(float* out, const C22* P1, const H2
 // every visibility's residual R = V - sum_d J_1 M_d J_2^H (in direction
 // order, with the same FP32 operations as fj_pass_kernel) in HBM, taking
 // rows in batches of kFjRowBatch so that each direction's gains are loaded
-// once per batch; then one fj_chunk_kernel launch per group of up to
-// kFjMaxDirections directions reads R and its own directions' models and
-// accumulates them. A pass reads the data and every model once for the
-// residual, then R once per group.
+// once per batch; then fj_accumulate_kernel reads R and each direction's
+// model and accumulates the directions. A pass reads the data and every
+// model once for the residual, then R once more.
 constexpr int kFjRowBatch = 8;
 
 __global__ void __launch_bounds__(kFjThreads) fj_residual_kernel(const FjPassParams p) {
@@ -3028,52 +3026,52 @@ __global__ void __launch_bounds__(kFjThreads) fj_residual_kernel(const FjPassPar
   }
 }
 
-template <int NC>
-__global__ void __launch_bounds__(kFjThreads) fj_chunk_kernel(const FjPassParams p) {
+// More than kFjMaxDirections directions, after fj_residual_kernel: one
+// thread per (part of a run, direction), the directions of a part on
+// consecutive threads (so the part's residual is read once from HBM and then
+// from cache), each reading R and its direction's model and accumulating
+// that direction alone: a thread holds one direction's gains and sums, so
+// the grid runs at high occupancy, in one launch for every direction.
+__global__ void __launch_bounds__(kFjThreads) fj_accumulate_kernel(const FjPassParams p) {
   if (SolveStopped(p.state, p.use_handle)) return;
-  const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gt >= p.n_runs * p.n_parts) return;
-  const uint32_t gr = gt % p.n_runs, part = gt / p.n_runs;
+  const uint32_t nd = p.n_dir;
+  const uint64_t gl = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x;
+  const uint64_t unit = gl / nd;  // part * n_runs + global run
+  const uint32_t d = uint32_t(gl % nd);
+  if (unit >= uint64_t(p.n_runs) * p.n_parts) return;
+  const uint32_t gr = uint32_t(unit % p.n_runs), part = uint32_t(unit / p.n_runs);
   const uint32_t si = FjSlabOf(p, gr);
   const SlabDesc sl = p.slabs[si];
   const uint32_t r = gr - p.run_start[si];
   const uint32_t ap = sl.run_ant[r];
   const uint32_t a1 = ap & 0xFFFFu, a2 = ap >> 16;
-  const uint32_t nd = p.n_dir;
-  const double2* sol1 = p.solutions + (size_t(sl.cb) * p.n_ant + a1) * p.n_sub * 4;
-  const double2* sol2 = p.solutions + (size_t(sl.cb) * p.n_ant + a2) * p.n_sub * 4;
-  C22 J1[NC], J2[NC], P1[NC], P2[NC];
-  H22 D1[NC], D2[NC];
+  const size_t cb_off = size_t(sl.cb) * p.n_ant * p.n_sub;
+  const uint32_t s = p.slab_sol[sl.sol_off + d];
+  const C22 J1 = LoadJones(p.solutions + (cb_off + size_t(a1) * p.n_sub + s) * 4);
+  const C22 J2 = LoadJones(p.solutions + (cb_off + size_t(a2) * p.n_sub + s) * 4);
+  C22 P1, P2;
+  H22 D1, D2;
 #pragma unroll
-  for (int d = 0; d < NC; ++d) {
-    const uint32_t s = p.slab_sol[sl.sol_off + p.d0 + d];
-    J1[d] = LoadJones(sol1 + size_t(s) * 4);
-    J2[d] = LoadJones(sol2 + size_t(s) * 4);
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-      P1[d].m[k] = P2[d].m[k] = make_float2(0.f, 0.f);
-    ZeroH22(D1[d]);
-    ZeroH22(D2[d]);
-  }
+  for (int k = 0; k < 4; ++k) P1.m[k] = P2.m[k] = make_float2(0.f, 0.f);
+  ZeroH22(D1);
+  ZeroH22(D2);
   const float2* vis = static_cast<const float2*>(sl.vis);
   const float2* res = p.resid + p.resid_off[si] * 4;
   const uint64_t rows = uint64_t(sl.T) * sl.L;
   const uint64_t row_end = rows * (part + 1) / p.n_parts;
   for (uint64_t row = rows * part / p.n_parts; row < row_end; ++row) {
     const C22 R = LoadC22(res + (row * sl.R + r) * 4);
-#pragma unroll
-    for (int d = 0; d < NC; ++d) {
-      const C22 M = LoadC22(vis + SlabElem(sl.R, sl.W, nd + 1, row, 1 + p.d0 + d, r) * 4);
-      const C22 Y = Mul22(J1[d], M);
-      const C22 X = MulHerm22(J2[d], M);
-      AddMul22(P1[d], R, X);
-      AddGram22(D1[d], X);
-      AddHermMul22(P2[d], R, Y);
-      AddGram22(D2[d], Y);
-    }
+    const C22 M = LoadC22(vis + SlabElem(sl.R, sl.W, nd + 1, row, 1 + d, r) * 4);
+    const C22 Y = Mul22(J1, M);
+    const C22 X = MulHerm22(J2, M);
+    AddMul22(P1, R, X);
+    AddGram22(D1, X);
+    AddHermMul22(P2, R, Y);
+    AddGram22(D2, Y);
   }
-  FjStoreSlots<NC>(p.partials + (size_t(gt) * nd + p.d0) * kFjSlotFloats, P1, D1, P2, D2);
+  FjStoreSlots<1>(p.partials + (unit * nd + d) * kFjSlotFloats, &P1, &D1, &P2, &D2);
 }
+
 
 template <int ND>
 __global__ void __launch_bounds__(kFjThreads) fj_pass_kernel(const FjPassParams p) {
@@ -3644,7 +3642,7 @@ struct ddsolve_ctx {
   // full-Jones plan: first global run of each slab, per (cb, antenna,
   // sub-solution) item the list of its partial slots
   DevBuf d_fj_run_start, d_fj_list_off, d_fj_list_ent, d_fj_resid, d_fj_resid_off;
-  uint32_t fj_n_slabs = 0, fj_n_runs = 0, fj_blocks = 0, fj_parts = 1;
+  uint32_t fj_n_slabs = 0, fj_n_runs = 0, fj_blocks = 0, fj_parts = 1, fj_resid_parts = 1;
   // independent solution intervals (ddsolve_set_intervals): interval g owns
   // channel blocks [group_first_cb[g], group_first_cb[g + 1])
   uint32_t n_groups = 1;
@@ -4613,8 +4611,9 @@ int BuildFullJonesPlan(ddsolve_ctx* ctx) {
       total_runs += s.R;
       max_rows = std::max<uint64_t>(max_rows, uint64_t(s.T) * s.L);
     }
-  // (two directions: two lanes per part, so fewer parts give the same waves)
-  const uint64_t lanes = n_dir == 2 ? 2 : 1;
+  // (two directions: two lanes per part, more than four: a thread per part
+  // and direction in the accumulation, so fewer parts give the same waves)
+  const uint64_t lanes = n_dir == 2 ? 2 : n_dir > uint32_t(kFjMaxDirections) ? n_dir : 1;
   const uint64_t want_threads = uint64_t(std::max(ctx->n_sm, 1)) * 256 * 4 / lanes;
   uint64_t parts = total_runs ? (want_threads + total_runs - 1) / total_runs : 1;
   parts = std::max<uint64_t>(1, std::min<uint64_t>({parts, max_rows / 16, 16}));
@@ -4689,6 +4688,15 @@ int BuildFullJonesPlan(ddsolve_ctx* ctx) {
   ctx->fj_n_slabs = uint32_t(descs.size());
   ctx->fj_n_runs = uint32_t(n_runs);
   ctx->fj_parts = uint32_t(parts);
+  // The residual kernel stores R per row, so its row split costs no partial
+  // slots: about four waves of its threads (3 blocks of kFjThreads per SM),
+  // at least 8 rows each.
+  {
+    const uint64_t want_resid = uint64_t(std::max(ctx->n_sm, 1)) * 3 * kFjThreads * 4;
+    uint64_t rp = total_runs ? (want_resid + total_runs - 1) / total_runs : 1;
+    rp = std::max<uint64_t>(1, std::min<uint64_t>({rp, max_rows / 8, 16}));
+    ctx->fj_resid_parts = uint32_t(rp);
+  }
   ctx->use_pipe = false;
   ctx->plan_dirty = false;
   return DDSOLVE_OK;
@@ -5189,12 +5197,10 @@ uint32_t ConstraintLaunches(const ddsolve_ctx* ctx) {
 // (assign_kernel, or finalize_kernel again) finishes the iteration.
 // One full-Jones iteration: MakeSolutionsFinite4Pol, the pass, the
 // finalisation (or, in host mode, the next solutions only).
-// Launches of the full-Jones streaming pass: one, or the residual and one
-// per group of kFjMaxDirections directions.
+// Launches of the full-Jones streaming pass: one, or the residual and the
+// accumulation.
 uint32_t FjPassLaunches(const ddsolve_ctx* ctx) {
-  return ctx->n_dir <= uint32_t(kFjMaxDirections)
-             ? 1u
-             : 1u + (ctx->n_dir + kFjMaxDirections - 1) / kFjMaxDirections;
+  return ctx->n_dir <= uint32_t(kFjMaxDirections) ? 1u : 2u;
 }
 
 int LaunchFullJones(ddsolve_ctx* ctx, bool host_mode, bool use_handle, bool with_make_finite) {
@@ -5217,7 +5223,6 @@ int LaunchFullJones(ddsolve_ctx* ctx, bool host_mode, bool use_handle, bool with
   pp.n_dir = ctx->n_dir;
   pp.state = ctx->d_state.as<LoopState>();
   pp.use_handle = (use_handle && !host_mode) ? 1 : 0;
-  pp.d0 = 0;
   pp.resid = nullptr;
   pp.resid_off = nullptr;
   pp.n_parts = ctx->fj_parts;
@@ -5237,15 +5242,19 @@ int LaunchFullJones(ddsolve_ctx* ctx, bool host_mode, bool use_handle, bool with
     default:
       pp.resid = ctx->d_fj_resid.as<float2>();
       pp.resid_off = ctx->d_fj_resid_off.as<uint64_t>();
-      fj_residual_kernel<<<blocks, kFjThreads, 0, ctx->stream>>>(pp);
-      for (uint32_t d0 = 0; d0 < ctx->n_dir; d0 += kFjMaxDirections) {
-        pp.d0 = d0;
-        switch (std::min<uint32_t>(kFjMaxDirections, ctx->n_dir - d0)) {
-          case 1: fj_chunk_kernel<1><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
-          case 2: fj_chunk_kernel<2><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
-          case 3: fj_chunk_kernel<3><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
-          default: fj_chunk_kernel<4><<<blocks, kFjThreads, 0, ctx->stream>>>(pp); break;
-        }
+      {  // its own row split (R is stored per row)
+        FjPassParams rp = pp;
+        rp.n_parts = ctx->fj_resid_parts;
+        const uint64_t rthreads = uint64_t(ctx->fj_n_runs) * rp.n_parts;
+        const uint32_t rblocks =
+            uint32_t(std::max<uint64_t>(1, (rthreads + kFjThreads - 1) / kFjThreads));
+        fj_residual_kernel<<<rblocks, kFjThreads, 0, ctx->stream>>>(rp);
+      }
+      {
+        const uint64_t threads = units * ctx->n_dir;
+        const uint32_t blocks_acc =
+            uint32_t(std::max<uint64_t>(1, (threads + kFjThreads - 1) / kFjThreads));
+        fj_accumulate_kernel<<<blocks_acc, kFjThreads, 0, ctx->stream>>>(pp);
       }
   }
   DDS_CHECK_CUDA(ctx, cudaGetLastError());
