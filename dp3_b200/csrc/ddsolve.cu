@@ -732,7 +732,6 @@ __device__ __forceinline__ double2 zconj(double2 a) { return make_double2(a.x, -
 
 template <int NPOL>
 __global__ void __launch_bounds__(256) correct_subtract_kernel(const CorrectParams p) {
-  constexpr int kGroup = 4;  // directions whose models are loaded before their products
   for (uint64_t v = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; v < p.n_vis;
        v += uint64_t(gridDim.x) * blockDim.x) {
     const uint32_t ch = uint32_t(v % p.n_ch);
@@ -741,16 +740,13 @@ __global__ void __launch_bounds__(256) correct_subtract_kernel(const CorrectPara
     const uint32_t cb = uint32_t((uint64_t(ch + 1) * p.n_cb - 1) / p.n_ch);
     const double2* s1 = p.solutions + (size_t(cb) * p.n_ant + p.a1[bl]) * p.n_dir * NPOL;
     const double2* s2 = p.solutions + (size_t(cb) * p.n_ant + p.a2[bl]) * p.n_dir * NPOL;
-    float4 da = make_float4(0.f, 0.f, 0.f, 0.f), db = da;
-    if (p.data_out) {  // issued first, used last
-      da = __ldcs(p.data + v * 2);
-      db = __ldcs(p.data + v * 2 + 1);
-    }
     double2 sum[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) sum[k] = make_double2(0.0, 0.0);
-    // direction d's corrected model from its loaded visibility (ma, mb)
-    auto apply = [&](uint32_t d, const float4 ma, const float4 mb) {
+#pragma unroll 2
+    for (uint32_t d = 0; d < p.n_dir; ++d) {
+      const float4* md = p.model[d] + v * 2;
+      const float4 ma = __ldcs(md), mb = __ldcs(md + 1);
       const double2 m[4] = {make_double2(ma.x, ma.y), make_double2(ma.z, ma.w),
                             make_double2(mb.x, mb.y), make_double2(mb.z, mb.w)};
       double2 c[4];
@@ -786,27 +782,9 @@ __global__ void __launch_bounds__(256) correct_subtract_kernel(const CorrectPara
         __stcs(mo, make_float4(float(c[0].x), float(c[0].y), float(c[1].x), float(c[1].y)));
         __stcs(mo + 1, make_float4(float(c[2].x), float(c[2].y), float(c[3].x), float(c[3].y)));
       }
-    };
-    // Groups of kGroup directions: every model of the group is loaded before
-    // any product or store (a kept model is written only to its own
-    // direction's buffer, so the loads of the group cannot depend on them).
-    uint32_t d = 0;
-    for (; d + kGroup <= p.n_dir; d += kGroup) {
-      float4 ma[kGroup], mb[kGroup];
-#pragma unroll
-      for (int j = 0; j < kGroup; ++j) {
-        const float4* md = p.model[d + j] + v * 2;
-        ma[j] = __ldcs(md);
-        mb[j] = __ldcs(md + 1);
-      }
-#pragma unroll
-      for (int j = 0; j < kGroup; ++j) apply(d + j, ma[j], mb[j]);
-    }
-    for (; d < p.n_dir; ++d) {
-      const float4* md = p.model[d] + v * 2;
-      apply(d, __ldcs(md), __ldcs(md + 1));
     }
     if (p.data_out) {
+      const float4 da = __ldcs(p.data + v * 2), db = __ldcs(p.data + v * 2 + 1);
       __stcs(p.data_out + v * 2,
              make_float4(float(__dsub_rn(da.x, sum[0].x)), float(__dsub_rn(da.y, sum[0].y)),
                          float(__dsub_rn(da.z, sum[1].x)), float(__dsub_rn(da.w, sum[1].y))));
